@@ -1,0 +1,342 @@
+"""Benchmark of the batched PT-RMC hot path on one node.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the batched plain-sampler configuration): fcc Fe50Ni50, 10x10x10
+conventional cells (4,000 atoms), a0 = 3.59 A, single scattering to 5.0 A (42
+neighbours), exact 3-/4-leg multiple scattering to 5.5 A (25 classes, 3,204
+paths per site), 2 K edges, 241 k points, k^1/k^2/k^3 Kaiser-windowed complex
+chi(R) fitted on 1.4-5.0 A; 16 sample positions (seeded noise) x 32 PT rungs =
+512 replicas per GPU, advanced together, FP32 transcendentals with FP64 phase
+reduction and accumulation, FP64 re-anchoring every 1,000 accepted moves.
+
+One bench "step" is one exchange period: 25 sampler steps of every replica
+(one fused launch each) and one device replica exchange, replayed as a CUDA
+graph. value = swap attempts per second over all ranks. With --gpus N every
+rank runs its own 16 ladders (weak scaling, no collective in the timed loop).
+
+--impl reference times the CPU restatement of the reference sampler (oracle/,
+the reference itself is CuPy and cannot run here) on the host cores, one
+process per ladder.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PT-RMC GPU-s to plain's R-factor: learned+batched vs plain GPU; chi err vs FP64"
+UNIT = "swap attempts/s"
+NPOS, NREP, EXCH = 16, 32, 25
+
+
+def workload_config():
+    return {"workload": "batched plain PT-RMC, fcc Fe50Ni50 4000 atoms (10x10x10, a0 3.59 A), "
+                        "SS to 5.0 A + exact 3/4-leg MS to 5.5 A, 2 edges, 241 k, "
+                        "k^1/k^2/k^3 Kaiser complex chi(R) 1.4-5.0 A",
+            "positions": NPOS, "rungs": NREP, "replicas_per_gpu": NPOS * NREP,
+            "steps_per_bench_step": EXCH, "precision": "FP32 terms/transform, FP64 phase+accum",
+            "l2": "inputs larger than L2 (MS incidence records 205 MB per supercell)"}
+
+
+def build_problem():
+    from chimera_b200.configs import Problem
+    return Problem(ncell=(10, 10, 10), rmax=5.0, ms=True)
+
+
+def make_sampler(prob, rank=0):
+    from chimera_b200.sampler import BatchedSampler, LadderSpec
+    specs = []
+    for p in range(NPOS):
+        pos = prob.position(rank * NPOS + p)
+        specs.append(LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R, nrep=NREP,
+                                tmin=1e-4, tmax=1e-1, seed=1000 * rank + p, swap_frac=1.0,
+                                disp_sigma=0.012, max_disp=0.10, ms_library=prob.ms))
+    return BatchedSampler(specs, precision=1, exchange_every=EXCH, reanchor_every=1000)
+
+
+class Clocks:
+    """nvidia-smi samples while the timed region runs."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def step_bytes(prob):
+    """Algorithmic bytes one replica's swap attempt reads or writes: the MS
+    incidence records of both sites, the affected pairs' topology, the
+    endpoint species, and the replica's chi row."""
+    z = prob.top.ncoord
+    M = prob.ms.M if prob.ms is not None else 0
+    nsp, nk = prob.nsp, prob.k.size
+    return 2 * M * 16 + 4 * z * 45 + 2 * z * 4 + 8 * z * 4 + nsp * nk * 8
+
+
+def time_graph(fn, reps):
+    import torch
+    s = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(reps):
+        fn()
+    b.record(s)
+    b.synchronize()
+    return a.elapsed_time(b) / 1e3
+
+
+def cpu_baseline(prob, nsteps=40, nrep=NREP):
+    """The oracle's plain sampler on one ladder of this workload, one core."""
+    from oracle import sampler as OS
+    st = prob.position(0)
+    chans = []
+    for c, f in enumerate(prob.ft.fts):
+        chans.append(OS.Channel(f._idx, f._frac, f._inside, f._w, f.nfft, f._norm,
+                                int(prob.ft.chan_edge[c])))
+    ms = prob.ms
+    msd = None
+    if ms is not None:
+        P = ms.paths
+        msd = dict(p_abs=P.p_abs, p_cls=P.p_cls, p_slot=P.p_slot, inc=P.inc, cls_off=P.cls_off,
+                   nblk=P.nblk, T=ms.T.cpu().numpy())
+    pr = OS.Problem(prob.cell.ideal, prob.top.i, prob.top.j, prob.top.shift, prob.top.shell,
+                    prob.top.sigma2, prob.k, prob.tables.f, prob.tables.delta, prob.tables.lam,
+                    prob.tables.s02, chans, st.target, st.mask, st.sigma_R, prob.nsp, ms=msd)
+    smp = OS.PlainSampler(pr, nrep, 1e-4, 1e-1, 0, 1.0, 0.012, 0.10)
+    smp.init_state(prob.random_config(0), prob.cell.ideal)
+    smp.step()
+    t0 = time.perf_counter()
+    for it in range(nsteps):
+        smp.step()
+        if (it + 1) % EXCH == 0:
+            smp.replica_exchange()
+    dt = time.perf_counter() - t0
+    return {"value": nsteps * nrep / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle plain sampler (C kernels + NumPy FFT), one ladder of {nrep} "
+                      f"replicas on the 4,000-atom workload, {nsteps} steps after 1 warm-up"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement, one process per ladder."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    prob = build_problem()
+    ncores = os.cpu_count() or 1
+    nproc = max(1, min(NPOS, ncores))
+    steps = max(1, args.steps) * 4
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_ref_worker, [(p, steps) for p in range(nproc)])
+    wall = time.perf_counter() - t0
+    attempts = sum(r["attempts"] for r in res)
+    busy = max(r["seconds"] for r in res)
+    val = attempts / busy
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0,
+            "steps": steps, "warmup": 1, "ms_per_step": busy / steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": workload_config(),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": nproc, "kind": "port",
+                             "sample": f"{nproc} ladders x {NREP} replicas x {steps} steps, one "
+                                       f"process per ladder (oracle C kernels + NumPy FFT)"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _ref_worker(arg):
+    p, steps = arg
+    sys.path.insert(0, ROOT)
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    prob = build_problem()
+    r = cpu_baseline(prob, nsteps=steps)
+    return {"attempts": steps * NREP, "seconds": steps * NREP / r["value"]}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=30)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from chimera_b200 import _native as N
+    N.lib()
+    prob = build_problem()
+    smp = make_sampler(prob, rank)
+    rng = np.random.default_rng(rank)
+    sp0 = [prob.random_config(int(rng.integers(1 << 30))) for _ in range(NPOS)]
+    smp.init_state(sp0, prob.cell.ideal)
+    smp.capture()
+    smp.run_blocks(max(3, args.warmup))
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident inputs
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(s)
+        smp.run_blocks(args.steps)
+        ev1.record(s)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    dt = ev0.elapsed_time(ev1) / 1e3
+    if world > 1:
+        t = torch.tensor([dt], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = float(t)
+        dist.barrier()
+    attempts = smp.nslots * EXCH * args.steps * world
+    value = attempts / dt
+
+    # ---- dominant kernel: the fused step, timed alone as a graph of 25 launches
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for _ in range(EXCH):
+            smp.lad.step()
+    g.replay()
+    torch.cuda.synchronize()
+    reps = 20
+    t_steps = time_graph(g.replay, reps)
+    per_launch = t_steps / (reps * EXCH)
+    hbm, src = peaks()
+    achieved = step_bytes(prob) * smp.nslots / per_launch / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "step_traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get("bytes_per_launch")
+
+    # ---- end to end through the public API with host buffers
+    torch.cuda.synchronize()
+    e2e_blocks = max(4, args.steps // 4)
+    t0 = time.perf_counter()
+    smp2 = make_sampler(prob, rank)
+    smp2.init_state(sp0, prob.cell.ideal)
+    smp2.run_blocks(e2e_blocks)
+    best = [smp2.best(li) for li in range(NPOS)]
+    torch.cuda.synchronize()
+    e2e_dt = time.perf_counter() - t0
+    h2d = smp2.nslots * prob.cell.natoms * (4 + 24)
+    d2h = NPOS * (prob.cell.natoms * 4 + 8)
+    e2e_val = smp2.nslots * EXCH * (e2e_blocks + 1) / e2e_dt
+    err = smp.lad.device_error()
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu:
+            cpu = cpu_baseline(prob, nsteps=args.cpu_steps)
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic", "config": workload_config(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "peak_source": src, "kernel": "k_step (fused sampler step)",
+                         "launch_us": per_launch * 1e6,
+                         "bytes_per_launch": step_bytes(prob) * smp.nslots},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d / (e2e_blocks + 1),
+                    "d2h_bytes_per_step": d2h / (e2e_blocks + 1),
+                    "note": "fresh sampler from host arrays: upload, init, run, best configs "
+                            "back; bytes amortised over the run's bench steps"},
+            "gpu_launches": args.steps * (EXCH + 1),
+            "clocks": clocks,
+            "device_error": err,
+            "reanchors": smp.reanchors,
+            "best_chi2_min": min(b[1] for b in best),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,170 @@
+"""ctypes binding of libchimera_b200.so (include/chimera_b200.h).
+
+The library is the product's only compute path. Loading it fails loudly if it
+is missing or cannot be built; there is no fallback. `call(name, *args)`
+invokes an entry point and raises `ChxError` with the library's message on a
+non-zero status. Device buffers are torch CUDA tensors passed by pointer;
+`stream()` is torch's current CUDA stream, so every launch orders with torch's
+own work and is captured by torch CUDA graphs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_LIB = None
+
+
+class ChxError(RuntimeError):
+    pass
+
+
+c_p = C.c_void_p
+c_i = C.c_int
+c_d = C.c_double
+c_u64 = C.c_uint64
+c_i64 = C.c_int64
+
+
+class Pairs(C.Structure):
+    """chx_pairs_t"""
+    _fields_ = [("natoms", c_i), ("ncoord", c_i), ("npairs", c_i), ("nsp", c_i), ("nk", c_i),
+                ("nshell", c_i),
+                ("iidx", c_p), ("jidx", c_p), ("shift", c_p), ("shell", c_p), ("sig2", c_p),
+                ("ftab", c_p), ("dtab", c_p), ("lamtab", c_p), ("ktab", c_p), ("drtab", c_p),
+                ("c3tab", c_p), ("s2tab", c_p), ("s02", c_d)]
+
+
+class Ladder(C.Structure):
+    """chx_ladder_t"""
+    _fields_ = [
+        ("natoms", c_i), ("ncoord", c_i), ("npairs", c_i), ("nshell", c_i), ("nsp", c_i),
+        ("nk", c_i),
+        ("iidx", c_p), ("jidx", c_p), ("rev", c_p), ("shift", c_p), ("shell", c_p),
+        ("sig2", c_p), ("pair_tab", c_p), ("ideal", c_p),
+        ("ftab", c_p), ("dtab", c_p), ("lamtab", c_p), ("ktab", c_p), ("drtab", c_p),
+        ("c3tab", c_p), ("s2tab", c_p), ("s02", c_d), ("sstab", c_p),
+        ("ms_nblk", c_i), ("ms_M", c_i), ("ms_inc", c_p), ("ms_cls_off", c_p), ("ms_T", c_p),
+        ("etab", c_p), ("energy_beta", c_d),
+        ("nchan", c_i), ("nkw", c_i), ("nwin", c_i), ("nfft", c_i), ("ncoef", c_i),
+        ("ft_n0", c_p), ("ft_idx", c_p), ("ft_frac", c_p), ("ft_w", c_p), ("win_bin", c_p),
+        ("chi_extra", c_p), ("tw64", c_p), ("ft_norm", c_d),
+        ("tm_re", c_p), ("tm_im", c_p), ("sm", c_p), ("cplx", c_i), ("profile", c_i),
+        ("nfit", c_d),
+        ("seed", c_u64), ("swap_frac", c_d), ("disp_sigma", c_d), ("max_disp", c_d),
+        ("nrep", c_i), ("slot0", c_i), ("beta_rung", c_p), ("u_stream", c_p),
+        ("u_steps", c_i64),
+        ("species", c_p), ("pos", c_p), ("moved", c_p), ("chi", c_p), ("chi2", c_p),
+        ("count", c_p), ("rung_of", c_p), ("slot_of", c_p), ("best_chi2", c_p),
+        ("best_sp", c_p), ("best_pos", c_p), ("ms_C", c_p), ("acc_rung", c_p), ("n_acc", c_p),
+        ("exch_att", c_p), ("exch_acc", c_p)]
+
+
+# argument types of every entry point, in header order
+_SIGS = {
+    "chx_version": ([], c_i),
+    "chx_struct_size": ([c_i], c_i64),
+    "chx_last_error": ([C.c_char_p, c_i], c_i),
+    "chx_compute_r": ([c_p] * 6 + [c_i] * 3 + [c_p], c_i),
+    "chx_build_ptype": ([c_p] * 4 + [c_i] * 4 + [c_p], c_i),
+    "chx_chi_forward": ([c_p] * 12 + [c_i] * 3 + [c_d, c_i, c_p], c_i),
+    "chx_chi_delta": ([c_p] * 15 + [c_i] * 4 + [c_d, c_i, c_p], c_i),
+    "chx_commit_move": ([c_p] * 6 + [c_i] * 3 + [c_p], c_i),
+    "chx_propose_select": ([c_p] * 9 + [c_i, c_i, c_u64, c_u64, c_d, c_d, c_d, c_p], c_i),
+    "chx_propose_build": ([c_p] * 15 + [c_i] * 6 + [c_p], c_i),
+    "chx_commit_state": ([c_p] * 9 + [c_i, c_i, c_p], c_i),
+    "chx_chi_full_scratch_bytes": ([c_p, c_i], c_i64),
+    "chx_chi_full": ([c_p, c_p, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),
+    "chx_ms_counts": ([c_p, c_i, c_i, c_p, c_i64, c_p, c_i, c_i, c_p, c_p], c_i),
+    "chx_ms_delta": ([c_p, c_i, c_i, c_p, c_i, c_p, c_i, c_i, c_p, c_p, c_p, c_p, c_p, c_p], c_i),
+    "chx_eval_chi2": ([c_p, c_p, c_i, c_p, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
+    "chx_ms_chi_of": ([c_p, c_p, c_i, c_i, c_i, c_i, c_p, c_p], c_i),
+    "chx_sampler_smem_bytes": ([c_p, c_i, c_i], c_i),
+    "chx_shell_table": ([c_p, c_p, c_p, c_p, c_p], c_i),
+    "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
+    "chx_replica_exchange": ([c_p, c_i, c_p, c_p], c_i),
+    "chx_apply_exchange": ([c_p, c_i, c_p, c_p], c_i),
+    "chx_ft_batch": ([c_p, c_i, c_i, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),
+    "chx_ft_batch_scratch_bytes": ([c_i, c_i, c_i, c_i], c_i64),
+}
+
+# entry points declared in include/chimera_b200.h (checked by the tests)
+EXPORTS = tuple(_SIGS)
+
+
+def lib():
+    """Load (building first if needed) the in-tree libchimera_b200.so."""
+    global _LIB
+    if _LIB is None:
+        path = _build.LIB
+        if _build.stale():
+            try:
+                path = _build.build()
+            except Exception as e:          # no nvcc, or a compile error
+                if not os.path.exists(path):
+                    raise ChxError(f"libchimera_b200.so is missing and could not be built: {e}")
+        L = C.CDLL(path)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _LIB = L
+        _check_abi(L)
+    return _LIB
+
+
+def _check_abi(L):
+    got = (L.chx_struct_size(0), L.chx_struct_size(1), L.chx_struct_size(2),
+           L.chx_struct_size(3))
+    want = (C.sizeof(Pairs), C.sizeof(Ladder), Ladder.exch_acc.offset, Ladder.seed.offset)
+    if got != want:
+        raise ChxError(f"ABI mismatch between chimera_b200.h and the binding: {got} != {want}")
+
+
+def last_error():
+    buf = C.create_string_buffer(512)
+    lib().chx_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def call(name, *args):
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        raise ChxError(f"{name} failed ({rc}): {last_error()}")
+    return rc
+
+
+def stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def ptr(t):
+    """Device pointer of a torch tensor (None -> NULL)."""
+    if t is None:
+        return None
+    assert t.is_cuda and t.is_contiguous(), "device buffers must be contiguous CUDA tensors"
+    return C.c_void_p(t.data_ptr())
+
+
+def dptr(t):
+    """Integer device address (for ctypes struct fields)."""
+    return 0 if t is None else int(t.data_ptr())
+
+
+def require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise ChxError("chimera_b200 needs a CUDA device (sm_100a); none is visible")
+    lib()
+
+
+def to_dev(a, dtype=None):
+    """numpy -> contiguous CUDA tensor (dtype kept unless given)."""
+    import torch
+    a = np.ascontiguousarray(a if dtype is None else np.asarray(a, dtype=dtype))
+    return torch.from_numpy(a).to("cuda")

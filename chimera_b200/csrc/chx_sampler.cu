@@ -1,0 +1,731 @@
+// chx_sampler.cu -- the fused parallel-tempering RMC step (A3-A7), the
+// replica exchange (A8) and the ideal-shell term table.
+//
+// One CTA per replica slot runs the whole step of methods/method_a_rmc.py
+// (RMCSampler.step, :250-308) for its replica:
+//   1. propose: the reference's splitmix64 stream keyed (seed, step, rung),
+//      bit-identical (exafs_gpu/kernels.py:362-423);
+//   2. the affected directed pairs: both directions of every bond of a, and of
+//      b with the pairs through a dropped (kernels.py:425-488); old and new
+//      (r, type) of each, r recomputed from the positions;
+//   3. delta chi(k) of those pairs (kernels.py:243-325). In CHX_FP32C a pair
+//      whose two atoms sit on their ideal sites takes its term from the
+//      (shell, pair type) table, so a swap costs a count of type changes
+//      instead of transcendentals; displaced pairs and CHX_FP64 evaluate the
+//      term directly. The MS paths through a and b are re-counted from their
+//      incidence records (chimera/mslibrary.py:466-486) and contracted with
+//      the entry table;
+//   4. the trial chi, normalised per absorber and shifted by chi_extra, is
+//      resampled, windowed and transformed on the fit-window R bins only
+//      (exafs_gpu/fourier.py:69-80, chimera/multift.py:58-63) by a direct
+//      transform against a twiddle table in shared memory;
+//   5. profiled-scale chi^2 (method_a_rmc.py:190-227), Metropolis with the
+//      energy prior (method_a_rmc.py:280-285, 310-320);
+//   6. commit of species, position, chi, chi^2, MS counts and best state
+//      (kernels.py:328-346, 490-511; method_a_rmc.py:298-307).
+// The last CTA to finish advances the step counter, so a sequence of steps is
+// a sequence of identical launches (CUDA-graph capturable).
+#include <algorithm>
+#include "chx_device.cuh"
+
+namespace chx {
+
+constexpr int kStepThreads = 256;
+constexpr int kMaxCoord = 256;
+
+struct DirRec {      // one directly evaluated term: a PairRec plus its sign
+    PairRec r;
+    int neg;
+    int pad[3];
+};
+
+// Shared-memory carve-up of one step CTA (all offsets 16-byte aligned).
+struct StepSmem {
+    size_t tw, u, x, tr, dchi, dir, dirv, hist, dn, list, total;
+};
+
+template <typename T>
+static inline size_t al16(size_t n) { return ((n * sizeof(T)) + 15) / 16 * 16; }
+
+static StepSmem step_smem(const chx_ladder_t &L, int precision) {
+    StepSmem s;
+    bool f64 = precision == CHX_FP64;
+    size_t o = 0;
+    int maxaff = 4 * L.ncoord;
+    int nent = L.ms_nblk ? L.nsp * L.ms_nblk : 0;
+    int ndn = L.nshell * L.nsp * L.nsp;
+    s.tw = o; o += f64 ? al16<double2>(L.nfft) : al16<float2>(L.nfft);
+    s.u = o; o += f64 ? al16<double>((size_t)L.nchan * L.ncoef) : al16<float>((size_t)L.nchan * L.ncoef);
+    s.x = o; o += f64 ? al16<double2>((size_t)L.nchan * L.nwin) : al16<float2>((size_t)L.nchan * L.nwin);
+    s.tr = o; o += al16<double>((size_t)L.nsp * L.nk);
+    s.dchi = o; o += al16<double>((size_t)L.nsp * L.nk);
+    s.dir = o; o += al16<DirRec>((size_t)2 * maxaff);
+    s.dirv = o; o += al16<int>((size_t)2 * maxaff);
+    s.hist = o; o += al16<int>((size_t)std::max(nent, 1));
+    s.dn = o; o += al16<int>((size_t)std::max(ndn, 1));
+    s.list = o; o += al16<int>((size_t)(2 * maxaff + ndn + nent + 32));
+    s.total = o;
+    return s;
+}
+
+// Deterministic in-order compaction by one warp: writes the indices i < n
+// with flag(i) into out, returns the count (valid in lane 0's view for all).
+template <typename F>
+__device__ __forceinline__ int warp_compact(int n, F flag, int *out) {
+    int lane = threadIdx.x & 31, cnt = 0;
+    for (int i0 = 0; i0 < n; i0 += 32) {
+        int i = i0 + lane;
+        bool f = i < n && flag(i);
+        unsigned m = __ballot_sync(0xffffffffu, f);
+        if (f) out[cnt + __popc(m & ((1u << lane) - 1))] = i;
+        cnt += __popc(m);
+    }
+    return cnt;
+}
+
+__device__ __forceinline__ int ms_entry_new(const int *S, int4 rc, const int *cls_off, int nsp,
+                                            int nblk, int a, int b, int nsa, int nsb) {
+    auto sp = [&](int site) { return site == a ? nsa : (site == b ? nsb : S[site]); };
+    int ab = rc.x & 0xFFFFF, cl = rc.x >> 20;
+    int e = sp(ab) * nblk + cls_off[cl];
+    int pw = 1;
+    if (rc.y >= 0) e += sp(rc.y) * pw;
+    pw *= nsp;
+    if (rc.z >= 0) e += sp(rc.z) * pw;
+    pw *= nsp;
+    if (rc.w >= 0) e += sp(rc.w) * pw;
+    return e;
+}
+__device__ __forceinline__ int ms_entry_old(const int *S, int4 rc, const int *cls_off, int nsp,
+                                            int nblk) {
+    return ms_entry_new(S, rc, cls_off, nsp, nblk, -1, -1, 0, 0);
+}
+
+// Steps 4-5 of the step (and the whole of k_eval_chi2): resample x window x
+// k^w the normalised trial chi s_tr (nsp, nk), transform it on the window
+// bins against the twiddles s_tw, and reduce the profiled chi^2 into s_c2.
+template <int NSP, int PREC>
+__device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr,
+                        const typename std::conditional<PREC == CHX_FP64, double2, float2>::type *s_tw,
+                        typename std::conditional<PREC == CHX_FP64, double, float>::type *s_u,
+                        typename std::conditional<PREC == CHX_FP64, double2, float2>::type *s_x,
+                        double *s_num, double *s_den, double *s_sq, double *s_scale,
+                        double *s_c2) {
+    typedef typename std::conditional<PREC == CHX_FP64, double, float>::type real;
+    typedef typename std::conditional<PREC == CHX_FP64, double2, float2>::type real2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nk = L.nk;
+    const int nchan = L.nchan, ncoef = L.ncoef, nwin = L.nwin, nkw = L.nkw;
+    for (int q = tid; q < nchan * ncoef; q += blockDim.x) {
+        int ch = q / ncoef, e = ch / nkw;
+        int id = L.ft_idx[q];
+        double va = s_tr[e * nk + id], vb = s_tr[e * nk + id + 1];
+        s_u[q] = (real)((va + (vb - va) * L.ft_frac[q]) * L.ft_w[q]);
+    }
+    __syncthreads();
+    const int fmask = L.nfft - 1;
+    for (int o = tid; o < nchan * nwin; o += blockDim.x) {
+        int ch = o / nwin, q = o - ch * nwin;
+        int m = L.win_bin[q];
+        int idx = (int)(((long)L.ft_n0[ch] * m) & fmask), stp = m & fmask;
+        const real *u = s_u + (long)ch * ncoef;
+        real sr = 0, si = 0;
+        for (int j = 0; j < ncoef; ++j) {
+            real2 w = s_tw[idx];
+            real uj = u[j];
+            sr = fma(uj, w.x, sr);
+            si = fma(uj, w.y, si);
+            idx = (idx + stp) & fmask;
+        }
+        s_x[o] = real2{(real)(sr * L.ft_norm), (real)(si * L.ft_norm)};
+    }
+    __syncthreads();
+
+    // ---- 5. profiled chi^2
+    for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
+        double nu = 0.0, dn = 0.0;
+        for (int q = lane; q < nwin; q += 32) {
+            real2 m = s_x[ch * nwin + q];
+            double tr = L.tm_re[ch * nwin + q];
+            if (L.cplx) {
+                double ti = L.tm_im[ch * nwin + q];
+                nu += (double)m.x * tr + (double)m.y * ti;
+                dn += (double)m.x * m.x + (double)m.y * m.y;
+            } else {
+                double mag = sqrt((double)m.x * m.x + (double)m.y * m.y);
+                nu += mag * tr;
+                dn += mag * mag;
+            }
+        }
+        nu = warp_sum(nu);
+        dn = warp_sum(dn);
+        if (lane == 0) {
+            s_num[ch] = nu;
+            s_den[ch] = dn;
+        }
+    }
+    __syncthreads();
+    if (tid < NSP) {
+        double s = 1.0;
+        if (L.profile) {
+            double nu = 0.0, dn = 0.0;
+            for (int q = 0; q < nkw; ++q) {
+                nu += s_num[tid * nkw + q];
+                dn += s_den[tid * nkw + q];
+            }
+            s = nu / fmax(dn, 1e-30);
+        }
+        s_scale[tid] = s;
+    }
+    __syncthreads();
+    for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
+        double s = s_scale[ch / nkw], acc = 0.0;
+        for (int q = lane; q < nwin; q += 32) {
+            real2 m = s_x[ch * nwin + q];
+            long g = (long)ch * nwin + q;
+            double sg = L.sm[g];
+            if (L.cplx) {
+                double dr = ((double)m.x * s - L.tm_re[g]) / sg;
+                double di = ((double)m.y * s - L.tm_im[g]) / sg;
+                acc += dr * dr + di * di;
+            } else {
+                double mag = sqrt((double)m.x * m.x + (double)m.y * m.y);
+                double dr = (mag * s - L.tm_re[g]) / sg;
+                acc += dr * dr;
+            }
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) s_sq[ch] = acc;
+    }
+    __syncthreads();
+
+    if (tid == 0) {
+        double tot = 0.0;
+        for (int ch = 0; ch < L.nchan; ++ch) tot += s_sq[ch];
+        *s_c2 = tot / L.nfit;
+    }
+    __syncthreads();
+}
+
+template <int NSP, int PREC>
+__global__ void __launch_bounds__(kStepThreads) k_step(const chx_ladder_t *__restrict__ Ls,
+                                                      const int *__restrict__ slot_ladder,
+                                                      int nslots, StepSmem so,
+                                                      uint64_t *__restrict__ stepc,
+                                                      int *__restrict__ ticket,
+                                                      int *__restrict__ err) {
+    typedef typename std::conditional<PREC == CHX_FP64, double, float>::type real;
+    typedef typename std::conditional<PREC == CHX_FP64, double2, float2>::type real2;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ chx_ladder_t L;
+    __shared__ Proposal prop;
+    __shared__ uint64_t s_step;
+    __shared__ int s_rung, s_ndir, s_ndn, s_nhist, s_acc;
+    __shared__ double s_num[32], s_den[32], s_sq[32], s_scale[8], s_de[kStepThreads / 32];
+    __shared__ double s_c2;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int slot = blockIdx.x;
+    {
+        const int *src = (const int *)&Ls[slot_ladder[slot]];
+        int *dst = (int *)&L;
+        for (int q = tid; q < (int)(sizeof(chx_ladder_t) / 4); q += blockDim.x) dst[q] = src[q];
+    }
+    __syncthreads();
+    const int c = slot - L.slot0;
+    const int natoms = L.natoms, z = L.ncoord, nk = L.nk, nn = NSP * NSP;
+    const int maxaff = 4 * z;
+    const int nent = L.ms_nblk ? NSP * L.ms_nblk : 0;
+    const int ndn = L.nshell * nn;
+    const int *S = L.species + (long)c * natoms;
+    const double *P = L.pos + (long)c * natoms * 3;
+    const uint8_t *MV = L.moved + (long)c * natoms;
+
+    real2 *s_tw = (real2 *)(smem + so.tw);
+    real *s_u = (real *)(smem + so.u);
+    real2 *s_x = (real2 *)(smem + so.x);
+    double *s_tr = (double *)(smem + so.tr);
+    double *s_dchi = (double *)(smem + so.dchi);
+    DirRec *s_dir = (DirRec *)(smem + so.dir);
+    int *s_dirv = (int *)(smem + so.dirv);
+    int *s_hist = (int *)(smem + so.hist);
+    int *s_dn = (int *)(smem + so.dn);
+    int *s_list = (int *)(smem + so.list);
+
+    // ---- 1. proposal (one thread) while the others stage the twiddles
+    if (tid == 0) {
+        s_step = *(volatile uint64_t *)stepc + 1;
+        int rung = L.rung_of[c];
+        s_rung = rung;
+        prop = propose_one(S, P, L.ideal, natoms, L.seed, s_step, rung, L.swap_frac,
+                           L.disp_sigma, L.max_disp);
+    }
+    for (int j = tid; j < L.nfft; j += blockDim.x) {
+        double2 t = ((const double2 *)L.tw64)[j];
+        s_tw[j] = real2{(real)t.x, (real)t.y};
+    }
+    for (int e = tid; e < nent; e += blockDim.x) s_hist[e] = 0;
+    for (int e = tid; e < ndn; e += blockDim.x) s_dn[e] = 0;
+    __syncthreads();
+    const int a = prop.a, b = prop.b, nsa = prop.nsa, nsb = prop.nsb, swp = prop.swap;
+    const bool use_tab = (PREC != CHX_FP64) && L.sstab != nullptr;
+
+    // ---- 2. affected pairs: old/new terms, table counts or direct records
+    double de = 0.0;
+    for (int q = tid; q < maxaff; q += blockDim.x) {
+        int blk = q / z, o = q - (q / z) * z;
+        int site = (blk < 2) ? a : b;
+        int p = site * z + o;
+        if (blk & 1) p = L.rev[p];
+        int i = -1, j = -1;
+        if ((unsigned)p < (unsigned)L.npairs) {
+            i = L.iidx[p];
+            j = L.jidx[p];
+        }
+        if ((unsigned)i >= (unsigned)natoms || (unsigned)j >= (unsigned)natoms) {
+            atomicOr(err, CHX_DEVERR_INDEX);
+            p = -1;
+        }
+        if (blk >= 2 && p >= 0 && (b == a || ((blk == 2) ? j : i) == a)) p = -1;
+        s_dirv[2 * q] = 0;
+        s_dirv[2 * q + 1] = 0;
+        if (p < 0) continue;
+        const double *sh3 = L.shift + 3 * (long)p;
+        const double *pi = P + 3 * (long)i, *pj = P + 3 * (long)j;
+        double dx = pj[0] + sh3[0] - pi[0], dy = pj[1] + sh3[1] - pi[1], dz = pj[2] + sh3[2] - pi[2];
+        double r_old = sqrt(dx * dx + dy * dy + dz * dz);
+        double r_new = r_old;
+        if (!swp) {  // a displacement: atom a moves to prop.np
+            const double *ni = (i == a) ? prop.np : pi, *nj = (j == a) ? prop.np : pj;
+            dx = nj[0] + sh3[0] - ni[0];
+            dy = nj[1] + sh3[1] - ni[1];
+            dz = nj[2] + sh3[2] - ni[2];
+            r_new = sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        int si = S[i], sj = S[j];
+        int t_old = si * NSP + sj;
+        int ni_ = (i == a) ? nsa : ((i == b) ? nsb : si);
+        int nj_ = (j == a) ? nsa : ((j == b) ? nsb : sj);
+        int t_new = ni_ * NSP + nj_;
+        int sh = L.shell[p];
+        if (L.etab) de += L.etab[sh * nn + t_new] - L.etab[sh * nn + t_old];
+        bool tab_ok = use_tab && L.pair_tab[p] && !MV[i] && !MV[j];
+        bool tab_new = tab_ok && swp;  // a displaced atom leaves its site
+        double s2 = L.sig2[p];
+        auto make = [&](double r, int t, int neg) {
+            DirRec d;
+            double reff = r + L.drtab[sh * nn + t];
+            d.r.reff = reff;
+            d.r.s2 = s2 + L.s2tab[sh * nn + t];
+            d.r.c3 = L.c3tab[sh];
+            d.r.inv_r2 = (float)(1.0 / (reff * reff));
+            d.r.t = t;
+            d.neg = neg;
+            return d;
+        };
+        if (tab_ok) atomicSub(&s_dn[sh * nn + t_old], 1);
+        else { s_dir[2 * q] = make(r_old, t_old, 1); s_dirv[2 * q] = 1; }
+        if (tab_new) atomicAdd(&s_dn[sh * nn + t_new], 1);
+        else { s_dir[2 * q + 1] = make(r_new, t_new, 0); s_dirv[2 * q + 1] = 1; }
+    }
+    if (L.etab) {
+        de = warp_sum(de);
+        if (lane == 0) s_de[warp] = de;
+    }
+    // ---- MS entry changes along the paths through a and b
+    if (nent && swp) {
+        const int M = L.ms_M;
+        const int4 *inc = (const int4 *)L.ms_inc;
+        for (int m = tid; m < 2 * M; m += blockDim.x) {
+            int half = m >= M;
+            int site = half ? b : a;
+            int4 rc = __ldg(&inc[(long)site * M + (m - half * M)]);
+            if (rc.x < 0) continue;
+            if (half) {
+                int ab = rc.x & 0xFFFFF;
+                if (ab == a || rc.y == a || rc.z == a || rc.w == a) continue;
+            }
+            int eo = ms_entry_old(S, rc, L.ms_cls_off, NSP, L.ms_nblk);
+            int en = ms_entry_new(S, rc, L.ms_cls_off, NSP, L.ms_nblk, a, b, nsa, nsb);
+            if (eo != en) {
+                atomicAdd(&s_hist[en], 1);
+                atomicSub(&s_hist[eo], 1);
+            }
+        }
+    }
+    __syncthreads();
+    // compact: warp 0 the direct records, warp 1 the table counts, warp 2 the MS entries
+    int *l_dir = s_list, *l_dn = s_list + 2 * maxaff, *l_ms = l_dn + ndn;
+    if (warp == 0) {
+        int n = warp_compact(2 * maxaff, [&](int i) { return s_dirv[i] != 0; }, l_dir);
+        if (lane == 0) s_ndir = n;
+    } else if (warp == 1) {
+        int n = warp_compact(ndn, [&](int i) { return s_dn[i] != 0; }, l_dn);
+        if (lane == 0) s_ndn = n;
+    } else if (warp == 2) {
+        int n = (nent && swp) ? warp_compact(nent, [&](int i) { return s_hist[i] != 0; }, l_ms) : 0;
+        if (lane == 0) s_nhist = n;
+    }
+    __syncthreads();
+
+    // ---- 3. delta chi(k): thread per k
+    const int ndir = s_ndir, ndnz = s_ndn, nms = s_nhist;
+    const double *CH = L.chi + (long)c * NSP * nk;
+    const double *CNT = L.count + (long)c * NSP;
+    for (int ik = tid; ik < nk; ik += blockDim.x) {
+        double acc[NSP];
+#pragma unroll
+        for (int s = 0; s < NSP; ++s) acc[s] = 0.0;
+        if (ndir) {
+            KConst<NSP> kc;
+            load_kconst<NSP>(kc, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, ik);
+            for (int q = 0; q < ndir; ++q) {
+                const DirRec &d = s_dir[l_dir[q]];
+                double v = rec_term<NSP, PREC>(d.r, kc);
+                add_by_species<NSP>(acc, d.r.t / NSP, d.neg ? -v : v);
+            }
+        }
+        for (int q = 0; q < ndnz; ++q) {
+            int jt = l_dn[q];
+            add_by_species<NSP>(acc, (jt % nn) / NSP, (double)s_dn[jt] * L.sstab[(long)jt * nk + ik]);
+        }
+        for (int q = 0; q < nms; ++q) {
+            int e = l_ms[q];
+            add_by_species<NSP>(acc, e / L.ms_nblk, (double)s_hist[e] * L.ms_T[(long)e * nk + ik]);
+        }
+#pragma unroll
+        for (int s = 0; s < NSP; ++s) {
+            s_dchi[s * nk + ik] = acc[s];
+            double v = (CH[s * nk + ik] + acc[s]) / fmax(CNT[s], 1.0);
+            if (L.chi_extra) v += L.chi_extra[s * nk + ik];
+            s_tr[s * nk + ik] = v;
+        }
+    }
+    __syncthreads();
+
+    // ---- 4-5. trial chi(R) on the window and its profiled chi^2
+    ft_chi2<NSP, PREC>(L, s_tr, s_tw, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
+
+    // ---- 6. Metropolis
+    if (tid == 0) {
+        double c2 = s_c2;
+        int rung = s_rung;
+        double x = L.beta_rung[rung] * (c2 - L.chi2[c]) * L.nfit;
+        if (L.etab) {
+            double d = 0.0;
+            for (int w = 0; w < (int)(blockDim.x / 32); ++w) d += s_de[w];
+            x += L.energy_beta * d;
+        }
+        double u;
+        long ui = (long)(s_step - 1);
+        if (L.u_stream && ui < L.u_steps) {
+            u = L.u_stream[ui * L.nrep + rung];
+        } else {
+            if (L.u_stream) atomicOr(err, CHX_DEVERR_INDEX);
+            uint64_t h = splitmix64(splitmix64(L.seed ^ 0xD1B54A32D192ED03ULL) ^
+                                    (s_step * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)rung << 32));
+            u = u01(splitmix64(h));
+        }
+        int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
+        s_acc = acc;
+        L.acc_rung[rung] = (uint8_t)acc;
+    }
+    __syncthreads();
+
+    // ---- 7. commit
+    if (s_acc) {
+        int *Sw = L.species + (long)c * natoms;
+        double *Pw = L.pos + (long)c * natoms * 3;
+        double *CHw = L.chi + (long)c * NSP * nk;
+        for (int q = tid; q < NSP * nk; q += blockDim.x) CHw[q] += s_dchi[q];
+        if (nent && swp) {
+            int *C = L.ms_C + (long)c * nent;
+            for (int q = tid; q < nms; q += blockDim.x) C[l_ms[q]] += s_hist[l_ms[q]];
+        }
+        if (tid == 0) {
+            Sw[a] = nsa;
+            Sw[b] = nsb;
+            if (!swp) {
+                Pw[3 * a] = prop.np[0];
+                Pw[3 * a + 1] = prop.np[1];
+                Pw[3 * a + 2] = prop.np[2];
+                L.moved[(long)c * natoms + a] = 1;
+            }
+            L.chi2[c] = s_c2;
+            L.n_acc[c] += 1;
+        }
+        __syncthreads();
+        if (s_c2 < L.best_chi2[c]) {
+            int *B = L.best_sp + (long)c * natoms;
+            double *BP = L.best_pos + (long)c * natoms * 3;
+            for (int q = tid; q < natoms; q += blockDim.x) B[q] = Sw[q];
+            for (int q = tid; q < 3 * natoms; q += blockDim.x) BP[q] = Pw[q];
+            __syncthreads();
+            if (tid == 0) L.best_chi2[c] = s_c2;
+        }
+    }
+
+    // ---- the last CTA of the launch advances the step counter
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        int t = atomicAdd(ticket, 1);
+        if (t == nslots - 1) {
+            *ticket = 0;
+            *(volatile uint64_t *)stepc = s_step;
+            __threadfence();
+        }
+    }
+}
+
+
+// chi^2 of each slot's chi (or of chi_in, same layout) without a move: the
+// state's initial and end-of-run chi^2 (method_a_rmc.py:180, 437, 448).
+template <int NSP, int PREC>
+__global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *__restrict__ Ls,
+                                                           const int *__restrict__ slot_ladder,
+                                                           StepSmem so,
+                                                           const double *__restrict__ chi_in,
+                                                           const double *__restrict__ count_in,
+                                                           double *__restrict__ out) {
+    typedef typename std::conditional<PREC == CHX_FP64, double, float>::type real;
+    typedef typename std::conditional<PREC == CHX_FP64, double2, float2>::type real2;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ chx_ladder_t L;
+    __shared__ double s_num[32], s_den[32], s_sq[32], s_scale[8], s_c2;
+    const int tid = threadIdx.x, slot = blockIdx.x;
+    {
+        const int *src = (const int *)&Ls[slot_ladder[slot]];
+        int *dst = (int *)&L;
+        for (int q = tid; q < (int)(sizeof(chx_ladder_t) / 4); q += blockDim.x) dst[q] = src[q];
+    }
+    __syncthreads();
+    const int c = slot - L.slot0, nk = L.nk;
+    real2 *s_tw = (real2 *)(smem + so.tw);
+    real *s_u = (real *)(smem + so.u);
+    real2 *s_x = (real2 *)(smem + so.x);
+    double *s_tr = (double *)(smem + so.tr);
+    for (int j = tid; j < L.nfft; j += blockDim.x) {
+        double2 t = ((const double2 *)L.tw64)[j];
+        s_tw[j] = real2{(real)t.x, (real)t.y};
+    }
+    const double *CH = chi_in ? chi_in + (long)slot * NSP * nk : L.chi + (long)c * NSP * nk;
+    const double *CNT = count_in ? count_in + (long)slot * NSP : L.count + (long)c * NSP;
+    for (int q = tid; q < NSP * nk; q += blockDim.x) {
+        double v = CH[q] / fmax(CNT[q / nk], 1.0);
+        if (L.chi_extra) v += L.chi_extra[q];
+        s_tr[q] = v;
+    }
+    __syncthreads();
+    ft_chi2<NSP, PREC>(L, s_tr, s_tw, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
+    if (tid == 0) out[slot] = s_c2;
+}
+
+// ------------------------------------------------------- replica exchange
+// One thread per ladder (method_a_rmc.py:332-373 with the uniforms from a
+// counter stream): rung pairs (i, i+1) from a random parity, d >= 0 or
+// u < exp(max(d, -60)); an accepted pair swaps which slots the two rungs hold.
+__global__ void k_exchange(const chx_ladder_t *__restrict__ Ls, int nladders,
+                           const uint64_t *__restrict__ round_key) {
+    int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= nladders) return;
+    uint64_t round = *(volatile const uint64_t *)round_key;
+    const chx_ladder_t &L = Ls[li];
+    uint64_t h = splitmix64(splitmix64(L.seed ^ 0x5851F42D4C957F2DULL) ^ (round * 0x9E3779B97F4A7C15ULL));
+    h = splitmix64(h);
+    int start = (u01(h) < 0.5) ? 0 : 1;
+    for (int i = start; i < L.nrep - 1; i += 2) {
+        int si = L.slot_of[i], sj = L.slot_of[i + 1];
+        double d = (L.beta_rung[i] - L.beta_rung[i + 1]) * (L.chi2[si] - L.chi2[sj]) * L.nfit;
+        bool ok = d >= 0.0;
+        if (!ok) {
+            h = splitmix64(h);
+            ok = u01(h) < exp(fmax(d, -60.0));
+        }
+        L.exch_att[i] += 1;
+        if (ok) {
+            L.exch_acc[i] += 1;
+            L.slot_of[i] = sj;
+            L.slot_of[i + 1] = si;
+            L.rung_of[sj] = i;
+            L.rung_of[si] = i + 1;
+        }
+    }
+}
+
+// A host-decided permutation: rung i takes the state rung order[i] held.
+__global__ void k_apply_exchange(const chx_ladder_t *__restrict__ Ls, int ladder,
+                                 const int *__restrict__ order) {
+    const chx_ladder_t &L = Ls[ladder];
+    if (threadIdx.x != 0) return;
+    int tmp[1024];
+    int n = min(L.nrep, 1024);
+    for (int i = 0; i < n; ++i) {
+        int o = order[i];
+        tmp[i] = ((unsigned)o < (unsigned)n) ? L.slot_of[o] : L.slot_of[i];
+    }
+    for (int i = 0; i < n; ++i) {
+        L.slot_of[i] = tmp[i];
+        L.rung_of[tmp[i]] = i;
+    }
+}
+
+// sstab[(sh*nn + t)][k] = the term of an ideal pair of shell sh and type t
+template <int NSP>
+__global__ void k_shell_table(chx_ladder_t L, const double *__restrict__ rshell,
+                              const double *__restrict__ s2shell, double *__restrict__ sstab) {
+    int jt = blockIdx.x, nn = NSP * NSP;
+    int sh = jt / nn, t = jt % nn;
+    for (int ik = threadIdx.x; ik < L.nk; ik += blockDim.x) {
+        KPoint kp{L.ktab[ik], L.lamtab[ik]};
+        sstab[(long)jt * L.nk + ik] = term64(rshell[sh], t, sh, s2shell[sh], ik, L.nk, NSP, kp,
+                                             L.ftab, L.dtab, L.drtab, L.c3tab, L.s2tab, L.s02);
+    }
+}
+
+}  // namespace chx
+
+using namespace chx;
+
+extern "C" {
+
+int chx_sampler_smem_bytes(const chx_ladder_t *host_ladders, int nladders, int precision) {
+    if (!host_ladders || nladders <= 0) return CHX_ERR_ARG;
+    size_t m = 0;
+    for (int i = 0; i < nladders; ++i) m = std::max(m, step_smem(host_ladders[i], precision).total);
+    return (int)m;
+}
+
+int chx_shell_table(const chx_ladder_t *L, const double *rshell, const double *s2shell,
+                    double *sstab, void *stream) {
+    CHX_REQUIRE(L && rshell && s2shell && sstab, "shell_table: bad arguments");
+    int n = L->nshell * L->nsp * L->nsp;
+    cudaStream_t st = as_stream(stream);
+    switch (L->nsp) {
+        case 2: k_shell_table<2><<<n, 256, 0, st>>>(*L, rshell, s2shell, sstab); break;
+        case 3: k_shell_table<3><<<n, 256, 0, st>>>(*L, rshell, s2shell, sstab); break;
+        case 4: k_shell_table<4><<<n, 256, 0, st>>>(*L, rshell, s2shell, sstab); break;
+        default: set_error("shell_table: nsp %d not built", L->nsp); return CHX_ERR_UNSUPPORTED;
+    }
+    CHX_CHECK_LAUNCH("shell_table");
+    return CHX_OK;
+}
+
+int chx_sampler_step(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                     int nladders, const int *slot_ladder, int nslots, int precision,
+                     uint64_t *d_stepc, int *d_ticket, int *d_err, void *stream) {
+    CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && d_stepc && d_ticket && d_err &&
+                    nladders > 0 && nslots > 0,
+                "sampler_step: bad arguments");
+    CHX_REQUIRE(precision == CHX_FP64 || precision == CHX_FP32C, "sampler_step: bad precision");
+    int nsp = host_ladders[0].nsp;
+    size_t smem = 0;
+    StepSmem so{};
+    for (int i = 0; i < nladders; ++i) {
+        const chx_ladder_t &L = host_ladders[i];
+        CHX_REQUIRE(L.nsp == nsp, "sampler_step: one launch needs one species count");
+        CHX_REQUIRE(L.ncoord > 0 && L.ncoord <= kMaxCoord && L.nk > 0 && L.nchan <= 32 &&
+                        L.nchan == L.nsp * L.nkw && (L.nfft & (L.nfft - 1)) == 0 &&
+                        L.natoms < (1 << 20),
+                    "sampler_step: ladder %d outside the built limits", i);
+        StepSmem s = step_smem(L, precision);
+        if (s.total > smem) {
+            smem = s.total;
+            so = s;
+        }
+    }
+    // every ladder must share one carve-up: lay out for the largest of each field
+    for (int i = 0; i < nladders; ++i) {
+        StepSmem s = step_smem(host_ladders[i], precision);
+        CHX_REQUIRE(s.tw <= so.tw && s.u <= so.u && s.x <= so.x && s.tr <= so.tr &&
+                        s.dchi <= so.dchi && s.dir <= so.dir && s.hist <= so.hist &&
+                        s.dn <= so.dn && s.list <= so.list,
+                    "sampler_step: ladders of one launch need matching shapes");
+    }
+    CHX_REQUIRE(smem <= 220 * 1024, "sampler_step: %zu bytes of shared memory needed", smem);
+    cudaStream_t st = as_stream(stream);
+#define CHX_STEP(N, PR)                                                                         \
+    do {                                                                                        \
+        cudaFuncSetAttribute(k_step<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
+                             (int)smem);                                                        \
+        k_step<N, PR><<<nslots, kStepThreads, smem, st>>>(d_ladders, slot_ladder, nslots, so,    \
+                                                          d_stepc, d_ticket, d_err);            \
+    } while (0)
+    if (precision == CHX_FP64) {
+        switch (nsp) {
+            case 2: CHX_STEP(2, CHX_FP64); break;
+            case 3: CHX_STEP(3, CHX_FP64); break;
+            case 4: CHX_STEP(4, CHX_FP64); break;
+            default: set_error("sampler_step: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+        }
+    } else {
+        switch (nsp) {
+            case 2: CHX_STEP(2, CHX_FP32C); break;
+            case 3: CHX_STEP(3, CHX_FP32C); break;
+            case 4: CHX_STEP(4, CHX_FP32C); break;
+            default: set_error("sampler_step: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+        }
+    }
+#undef CHX_STEP
+    CHX_CHECK_LAUNCH("sampler_step");
+    return CHX_OK;
+}
+
+int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders, int nladders,
+                  const int *slot_ladder, int nslots, int precision, const double *chi_in,
+                  const double *count_in, double *out, void *stream) {
+    CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && out && nladders > 0 && nslots > 0,
+                "eval_chi2: bad arguments");
+    int nsp = host_ladders[0].nsp;
+    StepSmem so{};
+    size_t smem = 0;
+    for (int i = 0; i < nladders; ++i) {
+        StepSmem s = step_smem(host_ladders[i], precision);
+        if (s.total > smem) { smem = s.total; so = s; }
+    }
+    cudaStream_t st = as_stream(stream);
+#define CHX_EV(N, PR)                                                                          \
+    do {                                                                                       \
+        cudaFuncSetAttribute(k_eval_chi2<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                             (int)smem);                                                       \
+        k_eval_chi2<N, PR><<<nslots, kStepThreads, smem, st>>>(d_ladders, slot_ladder, so,      \
+                                                               chi_in, count_in, out);         \
+    } while (0)
+    if (precision == CHX_FP64) {
+        switch (nsp) {
+            case 2: CHX_EV(2, CHX_FP64); break;
+            case 3: CHX_EV(3, CHX_FP64); break;
+            case 4: CHX_EV(4, CHX_FP64); break;
+            default: set_error("eval_chi2: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+        }
+    } else {
+        switch (nsp) {
+            case 2: CHX_EV(2, CHX_FP32C); break;
+            case 3: CHX_EV(3, CHX_FP32C); break;
+            case 4: CHX_EV(4, CHX_FP32C); break;
+            default: set_error("eval_chi2: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+        }
+    }
+#undef CHX_EV
+    CHX_CHECK_LAUNCH("eval_chi2");
+    return CHX_OK;
+}
+
+int chx_replica_exchange(const chx_ladder_t *d_ladders, int nladders, const uint64_t *round_key,
+                         void *stream) {
+    CHX_REQUIRE(d_ladders && round_key && nladders > 0, "replica_exchange: bad arguments");
+    k_exchange<<<(nladders + 63) / 64, 64, 0, as_stream(stream)>>>(d_ladders, nladders,
+                                                                    round_key);
+    CHX_CHECK_LAUNCH("replica_exchange");
+    return CHX_OK;
+}
+
+int chx_apply_exchange(const chx_ladder_t *d_ladders, int ladder, const int *order,
+                       void *stream) {
+    CHX_REQUIRE(d_ladders && order && ladder >= 0, "apply_exchange: bad arguments");
+    k_apply_exchange<<<1, 32, 0, as_stream(stream)>>>(d_ladders, ladder, order);
+    CHX_CHECK_LAUNCH("apply_exchange");
+    return CHX_OK;
+}
+
+}  // extern "C"

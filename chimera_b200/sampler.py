@@ -1,0 +1,656 @@
+"""Parallel-tempering RMC on the device (methods/method_a_rmc.py).
+
+`Ladders` owns the device state of a batch of independent temperature
+ladders that share a species count: per ladder its supercell topology, tables,
+transform, target and rungs; per replica slot its species, positions, chi(k),
+chi^2, MS entry counts and best state. One `chx_sampler_step` launch advances
+every slot of every ladder by one proposal; temperatures are exchanged by
+permuting the rung <-> slot maps.
+
+`RMCSampler` is the reference class's interface (constructor keywords,
+init_state / step / replica_exchange / adapt / run / best / posterior_wc and
+the attributes fitrun reads) on one ladder. With `reproduce=True` (default)
+it consumes the reference's random streams: the proposal splitmix64 keyed
+(seed, step, rung) on the device, the acceptance uniforms of
+numpy PCG64(seed).random per step (the reference's `cp_rng`), and the
+replica exchange decided on the host with a second PCG64(seed) exactly as
+method_a_rmc.py:332-373 draws it. With `reproduce=False` the exchange is
+decided on the device and whole blocks of steps replay as CUDA graphs.
+
+`BatchedSampler` runs many ladders (sample positions, series points, uneven
+supercells) in one launch per step under CUDA graphs, with periodic FP64
+re-anchoring of the running chi (every `reanchor_every` accepted moves).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _native as N
+from .forward import FP64, FP32C
+
+KB_EV = 8.617333262e-5
+
+
+def _host(x):
+    try:
+        import torch
+        if isinstance(x, torch.Tensor):
+            return x.detach().cpu().numpy()
+    except ImportError:
+        pass
+    return np.asarray(x)
+
+
+def _ft_setup(ft, nsp):
+    """Per-channel window coefficients of a MultiEdgeFT-like object (or one
+    FourierTransform): n0, idx, frac, w padded to a common length."""
+    fts = getattr(ft, "fts", None) or [ft]
+    chan_edge = np.asarray(getattr(ft, "chan_edge", np.arange(len(fts))), np.int32)
+    nkw = len(fts) // nsp
+    assert nkw * nsp == len(fts), f"{len(fts)} channels do not divide into {nsp} edges"
+    assert np.array_equal(chan_edge, np.repeat(np.arange(nsp), nkw)), \
+        "channels must be ordered edge-major"
+    rows = []
+    for f in fts:
+        idx, frac = _host(f._idx), _host(f._frac)
+        wt = _host(f._w) * _host(f._inside)
+        nz = np.nonzero(wt)[0]
+        n0, n1 = (int(nz[0]), int(nz[-1]) + 1) if nz.size else (0, 1)
+        rows.append((n0, idx[n0:n1].astype(np.int32), frac[n0:n1], wt[n0:n1]))
+    ncoef = max(r[1].size for r in rows)
+    n0 = np.array([r[0] for r in rows], np.int32)
+    I = np.zeros((len(rows), ncoef), np.int32)
+    F = np.zeros((len(rows), ncoef))
+    W = np.zeros((len(rows), ncoef))
+    for c, (_, i, fr, w) in enumerate(rows):
+        I[c, :i.size], F[c, :i.size], W[c, :i.size] = i, fr, w
+    nfft = int(fts[0].nfft)
+    norm = float(fts[0]._norm)
+    extra = getattr(ft, "chi_extra", None)
+    return dict(nchan=len(fts), nkw=nkw, n0=n0, idx=I, frac=F, w=W, ncoef=ncoef, nfft=nfft,
+                norm=norm, extra=None if extra is None else _host(extra))
+
+
+def _twiddles(nfft):
+    j = np.arange(nfft)
+    ang = 2.0 * np.pi * j / nfft
+    return np.ascontiguousarray(np.stack([np.cos(ang), -np.sin(ang)], axis=1))
+
+
+class LadderSpec:
+    """Inputs of one temperature ladder (everything RMCSampler takes)."""
+
+    def __init__(self, fm, ft, target, mask, sigma_R, nrep=48, tmin=0.02, tmax=5.0, seed=0,
+                 swap_frac=0.75, disp_sigma=0.015, max_disp=0.30, profile_scale=True,
+                 energy_prior=None, ms_library=None):
+        self.fm, self.ft = fm, ft
+        self.target = np.asarray(target)
+        self.mask = np.asarray(mask, bool)
+        self.sigma_R = np.asarray(sigma_R, float)
+        self.nrep, self.tmin, self.tmax, self.seed = int(nrep), tmin, tmax, int(seed)
+        self.swap_frac, self.disp_sigma, self.max_disp = swap_frac, disp_sigma, max_disp
+        self.profile_scale = bool(profile_scale)
+        self.energy_prior = energy_prior
+        self.ms = ms_library
+
+
+class Ladders:
+    """Device state and descriptors of a batch of ladders (see module doc)."""
+
+    def __init__(self, specs, precision=FP64, use_table=True):
+        import torch
+        N.require_cuda()
+        self.torch = torch
+        self.specs = list(specs)
+        self.precision = int(precision)
+        self.nsp = int(self.specs[0].fm.nsp)
+        assert all(s.fm.nsp == self.nsp for s in self.specs), "one species count per batch"
+        self.nladders = len(self.specs)
+        self.nslots = sum(s.nrep for s in self.specs)
+        self.use_table = bool(use_table) and self.precision != FP64
+        self.host = (N.Ladder * self.nladders)()
+        self.keep = []                      # device tensors the descriptors point to
+        self.bufs = []                      # per-ladder dict of named tensors
+        slot0 = 0
+        slot_ladder = []
+        for li, s in enumerate(self.specs):
+            self.bufs.append(self._build_ladder(li, s, slot0))
+            slot_ladder += [li] * s.nrep
+            slot0 += s.nrep
+        self.slot_ladder = N.to_dev(np.array(slot_ladder, np.int32))
+        self.stepc = torch.zeros(1, dtype=torch.int64, device="cuda")
+        self.ticket = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.err = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self._upload()
+
+    # ------------------------------------------------------------ building
+    def _t(self, a, dtype=None):
+        t = N.to_dev(a, dtype)
+        self.keep.append(t)
+        return t
+
+    def _build_ladder(self, li, s, slot0):
+        torch = self.torch
+        fm = s.fm
+        L = self.host[li]
+        nsp, nk, nrep = self.nsp, fm.nk, s.nrep
+        i_np, j_np = fm.i_idx, fm.j_idx
+        natoms = fm.natoms
+        z = np.bincount(i_np, minlength=natoms)
+        assert z.min() == z.max(), "expected uniform coordination"
+        ncoord = int(z[0])
+        assert np.array_equal(i_np, np.repeat(np.arange(natoms), ncoord)), \
+            "pairs must be i-major (pair p = i * ncoord + o)"
+        from .lattice import build_reverse_index
+        rev = build_reverse_index(i_np, j_np, natoms)
+        ideal = np.ascontiguousarray(fm.cell.ideal, np.float64)
+        shift = _host(fm.d_shift).astype(np.float64)
+        sig2 = _host(fm.d_sig2).astype(np.float64)
+        shell = fm.shell
+        d0 = np.linalg.norm((ideal[j_np] + shift) - ideal[i_np], axis=1)
+        first = np.array([np.argmax(shell == q) for q in range(fm.nshell)])
+        r_shell, s2_shell = d0[first], sig2[first]
+        pair_tab = ((np.abs(d0 - r_shell[shell]) <= 1e-12 * r_shell[shell])
+                    & (sig2 == s2_shell[shell])).astype(np.uint8)
+        b = dict(rev=self._t(rev), ideal=self._t(ideal), shift=self._t(shift),
+                 sig2=self._t(sig2), pair_tab=self._t(pair_tab))
+        L.natoms, L.ncoord, L.npairs, L.nshell, L.nsp, L.nk = (natoms, ncoord, fm.npairs,
+                                                              fm.nshell, nsp, nk)
+        L.iidx, L.jidx, L.rev = N.dptr(fm.d_i), N.dptr(fm.d_j), N.dptr(b["rev"])
+        L.shift, L.shell, L.sig2 = N.dptr(b["shift"]), N.dptr(fm.d_shell), N.dptr(b["sig2"])
+        L.pair_tab, L.ideal = N.dptr(b["pair_tab"]), N.dptr(b["ideal"])
+        L.ftab, L.dtab, L.lamtab, L.ktab = (N.dptr(fm.d_f), N.dptr(fm.d_delta),
+                                            N.dptr(fm.d_lam), N.dptr(fm.d_k))
+        L.drtab, L.c3tab, L.s2tab = N.dptr(fm.d_dr), N.dptr(fm.d_c3), N.dptr(fm.d_s2tab)
+        self.keep += [fm.d_i, fm.d_j, fm.d_shell, fm.d_f, fm.d_delta, fm.d_lam, fm.d_k,
+                      fm.d_dr, fm.d_c3, fm.d_s2tab]
+        L.s02 = fm.s02
+        if self.use_table:
+            b["sstab"] = torch.empty((fm.nshell * nsp * nsp, nk), dtype=torch.float64,
+                                     device="cuda")
+            self.keep.append(b["sstab"])
+            L.sstab = N.dptr(b["sstab"])
+            rs, ss = self._t(r_shell), self._t(s2_shell)
+            N.call("chx_shell_table", C.byref(L), N.ptr(rs), N.ptr(ss), N.ptr(b["sstab"]),
+                   N.stream())
+        else:
+            L.sstab = 0
+        # exact multiple scattering
+        ms = s.ms
+        if ms is not None:
+            d = ms.paths.device()
+            L.ms_nblk, L.ms_M = ms.nblk, ms.M
+            L.ms_inc, L.ms_cls_off, L.ms_T = (N.dptr(d["inc_rec"]), N.dptr(d["cls_off"]),
+                                              N.dptr(ms.T))
+            self.keep += [d["inc_rec"], d["cls_off"], ms.T]
+        else:
+            L.ms_nblk, L.ms_M, L.ms_inc, L.ms_cls_off, L.ms_T = 0, 0, 0, 0, 0
+        # pair-interaction prior (method_a_rmc.py:147-157)
+        if s.energy_prior is not None:
+            V, T_ann = s.energy_prior
+            V = np.asarray(V, float)
+            tab = np.zeros((fm.nshell, nsp * nsp))
+            m = min(fm.nshell, V.shape[0])
+            tab[:m] = 0.5 * V[:m].reshape(m, nsp * nsp)
+            b["etab"] = self._t(tab.reshape(-1))
+            L.etab = N.dptr(b["etab"])
+            L.energy_beta = 1.0 / (KB_EV * float(T_ann))
+        else:
+            L.etab, L.energy_beta = 0, 0.0
+        # transform and target
+        f = _ft_setup(s.ft, nsp)
+        win = np.nonzero(s.mask)[0].astype(np.int32)
+        cplx = bool(np.iscomplexobj(s.target))
+        tm = np.ascontiguousarray(s.target[:, s.mask])
+        sm = np.ascontiguousarray(s.sigma_R[:, s.mask], np.float64)
+        b.update(ft_n0=self._t(f["n0"]), ft_idx=self._t(f["idx"]), ft_frac=self._t(f["frac"]),
+                 ft_w=self._t(f["w"]), win=self._t(win), tw=self._t(_twiddles(f["nfft"])),
+                 tm_re=self._t(np.ascontiguousarray(tm.real, np.float64)),
+                 tm_im=self._t(np.ascontiguousarray(tm.imag if cplx else np.zeros(tm.shape),
+                                                    np.float64)),
+                 sm=self._t(sm))
+        if f["extra"] is not None:
+            b["extra"] = self._t(np.ascontiguousarray(f["extra"], np.float64))
+        L.nchan, L.nkw, L.nwin, L.nfft, L.ncoef = (f["nchan"], f["nkw"], int(win.size),
+                                                  f["nfft"], f["ncoef"])
+        L.ft_n0, L.ft_idx, L.ft_frac, L.ft_w = (N.dptr(b["ft_n0"]), N.dptr(b["ft_idx"]),
+                                                N.dptr(b["ft_frac"]), N.dptr(b["ft_w"]))
+        L.win_bin, L.tw64, L.ft_norm = N.dptr(b["win"]), N.dptr(b["tw"]), f["norm"]
+        L.chi_extra = N.dptr(b.get("extra"))
+        L.tm_re, L.tm_im, L.sm = N.dptr(b["tm_re"]), N.dptr(b["tm_im"]), N.dptr(b["sm"])
+        L.cplx, L.profile = int(cplx), int(s.profile_scale)
+        self.nfit_of = getattr(self, "nfit_of", []) + [int(s.mask.sum()) * f["nchan"] * (2 if cplx else 1)]
+        L.nfit = float(self.nfit_of[-1])
+        # sampler constants
+        L.seed = s.seed & (2 ** 64 - 1)
+        L.swap_frac, L.disp_sigma, L.max_disp = s.swap_frac, s.disp_sigma, s.max_disp
+        L.nrep, L.slot0 = nrep, slot0
+        beta = 1.0 / np.geomspace(s.tmin, s.tmax, nrep)
+        b["beta"] = self._t(beta)
+        L.beta_rung = N.dptr(b["beta"])
+        L.u_stream, L.u_steps = 0, 0
+        # state
+        z32 = lambda *sh: torch.zeros(sh, dtype=torch.int32, device="cuda")
+        f64 = lambda *sh: torch.zeros(sh, dtype=torch.float64, device="cuda")
+        b.update(species=z32(nrep, natoms), pos=f64(nrep, natoms, 3),
+                 moved=torch.zeros((nrep, natoms), dtype=torch.uint8, device="cuda"),
+                 chi=f64(nrep, nsp, nk), chi2=f64(nrep), count=f64(nrep, nsp),
+                 rung_of=z32(nrep), slot_of=z32(nrep), best_chi2=f64(nrep),
+                 best_sp=z32(nrep, natoms), best_pos=f64(nrep, natoms, 3),
+                 ms_C=z32(nrep, ms.nent if ms is not None else 1),
+                 acc=torch.zeros(nrep, dtype=torch.uint8, device="cuda"), n_acc=z32(nrep),
+                 exch_att=z32(max(nrep, 1)), exch_acc=z32(max(nrep, 1)))
+        for key in ("species", "pos", "moved", "chi", "chi2", "count", "rung_of", "slot_of",
+                    "best_chi2", "best_sp", "best_pos", "ms_C", "acc", "n_acc", "exch_att",
+                    "exch_acc"):
+            self.keep.append(b[key])
+        L.species, L.pos, L.moved, L.chi = (N.dptr(b["species"]), N.dptr(b["pos"]),
+                                            N.dptr(b["moved"]), N.dptr(b["chi"]))
+        L.chi2, L.count, L.rung_of, L.slot_of = (N.dptr(b["chi2"]), N.dptr(b["count"]),
+                                                 N.dptr(b["rung_of"]), N.dptr(b["slot_of"]))
+        L.best_chi2, L.best_sp, L.best_pos = (N.dptr(b["best_chi2"]), N.dptr(b["best_sp"]),
+                                              N.dptr(b["best_pos"]))
+        L.ms_C, L.acc_rung, L.n_acc = N.dptr(b["ms_C"]), N.dptr(b["acc"]), N.dptr(b["n_acc"])
+        L.exch_att, L.exch_acc = N.dptr(b["exch_att"]), N.dptr(b["exch_acc"])
+        b["beta_host"] = beta
+        b["cplx"] = cplx
+        return b
+
+    def _upload(self):
+        import torch
+        raw = bytes(C.string_at(C.addressof(self.host), C.sizeof(self.host)))
+        dev = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to("cuda")
+        self.d_ladders = dev
+        return dev
+
+    def set_field(self, li, name, value):
+        setattr(self.host[li], name, value)
+        self._upload()
+
+    # --------------------------------------------------------------- state
+    def init_state(self, li, species0, pos0, stream_species=None):
+        """Every rung of ladder li starts from (species0, pos0)."""
+        torch = self.torch
+        s, b = self.specs[li], self.bufs[li]
+        fm = s.fm
+        nrep = s.nrep
+        sp = np.repeat(np.asarray(species0, np.int32)[None], nrep, 0)
+        pos = np.repeat(np.asarray(pos0, np.float64)[None], nrep, 0)
+        b["species"].copy_(torch.from_numpy(sp))
+        b["pos"].copy_(torch.from_numpy(pos))
+        ideal = _host(fm.cell.ideal)
+        b["moved"].copy_(torch.from_numpy(np.any(pos != ideal[None], axis=-1).astype(np.uint8)))
+        chi = fm.chi_full(b["pos"], b["species"], precision=FP64)
+        if s.ms is not None:
+            C_ = s.ms.counts(b["species"])
+            b["ms_C"].copy_(C_)
+            chi = chi + s.ms.chi_of(C_)
+        b["chi"].copy_(chi)
+        cnt = np.stack([(sp == q).sum(1) for q in range(self.nsp)], axis=1).astype(np.float64)
+        b["count"].copy_(torch.from_numpy(cnt))
+        b["rung_of"].copy_(torch.arange(nrep, dtype=torch.int32))
+        b["slot_of"].copy_(torch.arange(nrep, dtype=torch.int32))
+        b["acc"].zero_()
+        b["n_acc"].zero_()
+        b["exch_att"].zero_()
+        b["exch_acc"].zero_()
+
+    def eval_chi2(self, chi_in=None, count_in=None):
+        """chi^2 of every slot (nslots) by the step's own transform."""
+        torch = self.torch
+        out = torch.empty(self.nslots, dtype=torch.float64, device="cuda")
+        N.call("chx_eval_chi2", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
+               N.ptr(self.slot_ladder), self.nslots, self.precision,
+               N.ptr(chi_in) if chi_in is not None else None,
+               N.ptr(count_in) if count_in is not None else None, N.ptr(out), N.stream())
+        return out
+
+    def refresh_chi2(self, reset_best=False):
+        c2 = self.eval_chi2()
+        for li, b in enumerate(self.bufs):
+            s0 = self.host[li].slot0
+            b["chi2"].copy_(c2[s0:s0 + self.specs[li].nrep])
+            if reset_best:
+                b["best_chi2"].copy_(b["chi2"])
+                b["best_sp"].copy_(b["species"])
+                b["best_pos"].copy_(b["pos"])
+
+    def reanchor(self):
+        """Replace every slot's running chi by an FP64 recompute from its
+        species and positions (and exact MS counts), then its chi^2."""
+        for s, b in zip(self.specs, self.bufs):
+            chi = s.fm.chi_full(b["pos"], b["species"], precision=FP64)
+            if s.ms is not None:
+                chi = chi + s.ms.chi_of(b["ms_C"])
+            b["chi"].copy_(chi)
+            b["n_acc"].zero_()
+        self.refresh_chi2()
+
+    # --------------------------------------------------------------- steps
+    def step(self):
+        N.call("chx_sampler_step", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
+               N.ptr(self.slot_ladder), self.nslots, self.precision, N.ptr(self.stepc),
+               N.ptr(self.ticket), N.ptr(self.err), N.stream())
+
+    def exchange_device(self):
+        N.call("chx_replica_exchange", N.ptr(self.d_ladders), self.nladders, N.ptr(self.stepc),
+               N.stream())
+
+    def apply_exchange(self, li, order):
+        o = N.to_dev(np.asarray(order, np.int32))
+        N.call("chx_apply_exchange", N.ptr(self.d_ladders), li, N.ptr(o), N.stream())
+        self._last_order = o                # keep alive until the launch has run
+
+    def device_error(self):
+        return int(self.err.item())
+
+
+class RMCSampler:
+    """Device PT-RMC with the reference RMCSampler's interface."""
+
+    def __init__(self, fm, ft, target, mask, sigma_R, nrep=48, tmin=0.02, tmax=5.0, seed=0,
+                 swap_frac=0.75, disp_sigma=0.015, max_disp=0.30, nsp=None,
+                 collect_after=None, collect_every=25, adapt_every=0, target_accept=0.35,
+                 profile_scale=True, collect_beta=0.5, n_collect=4, energy_prior=None,
+                 ms_library=None, precision=FP64, reproduce=True, use_table=True):
+        self.fm, self.ft = fm, ft
+        self.nsp = int(nsp) if nsp is not None else int(fm.nsp)
+        self.nrep = int(nrep)
+        self.collect_after = collect_after
+        self.collect_every = int(collect_every)
+        self.collect_beta = None if collect_beta is None else float(collect_beta)
+        self.n_collect = int(n_collect)
+        self.adapt_every = int(adapt_every)
+        self.target_accept = float(target_accept)
+        self.profile_scale = bool(profile_scale)
+        self.samples = []
+        self.seed = int(seed)
+        self.rng = np.random.default_rng(seed)              # exchange stream
+        self._u_gen = np.random.default_rng(seed)            # acceptance stream
+        self.swap_frac, self.disp_sigma, self.max_disp = swap_frac, disp_sigma, max_disp
+        self.reproduce = bool(reproduce)
+        self.spec = LadderSpec(fm, ft, target, mask, sigma_R, nrep=nrep, tmin=tmin, tmax=tmax,
+                               seed=seed, swap_frac=swap_frac, disp_sigma=disp_sigma,
+                               max_disp=max_disp, profile_scale=profile_scale,
+                               energy_prior=energy_prior, ms_library=ms_library)
+        self.ms = ms_library
+        self.lad = Ladders([self.spec], precision=precision, use_table=use_table)
+        self.b = self.lad.bufs[0]
+        self.complex = self.b["cplx"]
+        self.nfit = self.lad.nfit_of[0]
+        self.natoms, self.npairs, self.nk = fm.natoms, fm.npairs, fm.nk
+        self.exch_attempts = np.zeros(max(nrep - 1, 1))
+        self.exch_accepted = np.zeros(max(nrep - 1, 1))
+        self._u_host = np.zeros((0, self.nrep))
+        self._stepc = 0
+
+    # ------------------------------------------------------------ state
+    def init_state(self, species0, pos0):
+        self.lad.init_state(0, species0, pos0)
+        self.lad.refresh_chi2(reset_best=True)
+
+    def _ensure_uniforms(self, upto):
+        """Acceptance uniforms for steps 1..upto, PCG64(seed).random(nrep)
+        per step (the reference's cp_rng draws, method_a_rmc.py:284)."""
+        if not self.reproduce or self._u_host.shape[0] >= upto:
+            return
+        grow = max(upto - self._u_host.shape[0], 1024)
+        more = self._u_gen.random(grow * self.nrep).reshape(grow, self.nrep)
+        self._u_host = np.concatenate([self._u_host, more])
+        self._u_dev = N.to_dev(self._u_host)
+        L = self.lad.host[0]
+        L.u_stream, L.u_steps = N.dptr(self._u_dev), self._u_host.shape[0]
+        self.lad._upload()
+
+    @property
+    def _rung_slots(self):
+        return self.b["slot_of"].long()
+
+    @property
+    def chi2(self):
+        """(nrep,) chi^2 by rung (device)."""
+        return self.b["chi2"][self._rung_slots]
+
+    @property
+    def species(self):
+        return self.b["species"][self._rung_slots]
+
+    @property
+    def pos(self):
+        return self.b["pos"][self._rung_slots]
+
+    @property
+    def chi(self):
+        return self.b["chi"][self._rung_slots]
+
+    @property
+    def beta(self):
+        return self.b["beta"]
+
+    @property
+    def best_chi2(self):
+        return self.b["best_chi2"]
+
+    def scales(self, chi_un=None):
+        raise NotImplementedError("profiled scales are evaluated inside the device step")
+
+    # ------------------------------------------------------------ moves
+    def step(self):
+        """One proposal per rung; returns the accept flags by rung (device)."""
+        self._stepc += 1
+        self._ensure_uniforms(self._stepc)
+        self.lad.step()
+        return self.b["acc"].bool()
+
+    def replica_exchange(self, return_rates=False):
+        """Host-decided exchange on the reference's PCG64 stream
+        (method_a_rmc.py:332-373); the state stays put, the rungs move."""
+        c2 = _host(self.chi2)
+        beta = self.b["beta_host"]
+        order = np.arange(self.nrep)
+        start = self.rng.integers(0, 2)
+        nsw = 0
+        rates = np.full(self.nrep - 1, np.nan)
+        for i in range(start, self.nrep - 1, 2):
+            d = (beta[i] - beta[i + 1]) * (c2[order[i]] - c2[order[i + 1]]) * self.nfit
+            ok = d >= 0 or self.rng.random() < np.exp(max(d, -60.0))
+            rates[i] = 1.0 if ok else 0.0
+            self.exch_attempts[i] += 1
+            if ok:
+                order[i], order[i + 1] = order[i + 1], order[i]
+                nsw += 1
+                self.exch_accepted[i] += 1
+        if nsw:
+            self.lad.apply_exchange(0, order)
+        if return_rates:
+            filled = np.where(np.isnan(rates),
+                              np.nanmean(rates) if np.any(~np.isnan(rates)) else 0.3, rates)
+            return nsw, filled
+        return nsw
+
+    def adapt(self, window_acc, window_exch):
+        """Retune the displacement step and the ladder (method_a_rmc.py:376-398)."""
+        if window_acc is not None and window_acc > 0:
+            self.disp_sigma *= float(np.clip((window_acc / self.target_accept) ** 0.35, 0.7, 1.4))
+            self.disp_sigma = float(np.clip(self.disp_sigma, 1e-4, 0.15))
+            self.lad.set_field(0, "disp_sigma", self.disp_sigma)
+        if window_exch is None or self.nrep < 4:
+            return
+        b = np.log(self.b["beta_host"])
+        gaps = np.diff(b)
+        rate = np.clip(window_exch, 0.02, 0.98)
+        scale = (rate / max(rate.mean(), 1e-6)) ** 0.5
+        gaps = gaps * scale
+        gaps *= (b[-1] - b[0]) / gaps.sum()
+        beta = np.exp(np.concatenate([[b[0]], b[0] + np.cumsum(gaps)]))
+        self.b["beta_host"] = beta
+        self.b["beta"].copy_(N.to_dev(beta))
+
+    # ------------------------------------------------------------- loop
+    def run(self, nsteps, exchange_every=25, log_every=500, callback=None):
+        """Run the chain (method_a_rmc.py:401-455)."""
+        import torch
+        hist = []
+        acc_run = torch.zeros((), dtype=torch.float64, device="cuda")
+        self._ensure_uniforms(self._stepc + nsteps)
+        t0 = time.time()
+        win_acc, win_exch = [], []
+        for it in range(nsteps):
+            acc = self.step()
+            acc_run += acc.double().mean()
+            if self.adapt_every:
+                win_acc.append(acc.double().mean())
+            if exchange_every and (it + 1) % exchange_every == 0:
+                if self.reproduce:
+                    _, per_pair = self.replica_exchange(return_rates=True)
+                    if self.adapt_every:
+                        win_exch.append(per_pair)
+                else:
+                    self.lad.exchange_device()
+            if self.adapt_every and (it + 1) % self.adapt_every == 0:
+                wa = float(torch.stack(win_acc).mean()) if win_acc else None
+                we = np.mean(win_exch, axis=0) if win_exch else None
+                self.adapt(wa, we)
+                win_acc, win_exch = [], []
+            if (self.collect_after is not None and it >= self.collect_after
+                    and (it + 1) % self.collect_every == 0):
+                self._collect()
+            if (it + 1) % log_every == 0 or it == 0:
+                best = float(self.best_chi2.min())
+                hist.append((it + 1, best, float(acc_run) / (it + 1), time.time() - t0))
+                if callback:
+                    callback(it + 1, best, hist[-1][2])
+        if not self.reproduce:
+            att = _host(self.b["exch_att"])[:self.nrep - 1]
+            acc_ = _host(self.b["exch_acc"])[:self.nrep - 1]
+            self.exch_attempts += att
+            self.exch_accepted += acc_
+            self.b["exch_att"].zero_()
+            self.b["exch_acc"].zero_()
+        self.lad.refresh_chi2()
+        torch.cuda.synchronize()
+        bsp, bpos, _ = self.best()
+        chk = self.fm.chi_full(N.to_dev(bpos[None]), N.to_dev(bsp[None].astype(np.int32)),
+                               precision=FP64)
+        if self.ms is not None:
+            chk = chk + self.ms.full(N.to_dev(bsp[None].astype(np.int32)))
+        cnt = N.to_dev(np.array([[(bsp == s).sum() for s in range(self.nsp)]], np.float64))
+        chi_in = chk.expand(self.lad.nslots, -1, -1).contiguous()
+        cnt_in = cnt.expand(self.lad.nslots, -1).contiguous()
+        self.best_verified = float(self.lad.eval_chi2(chi_in, cnt_in)[0])
+        self.walltime = time.time() - t0
+        self.history = hist
+        with np.errstate(invalid="ignore", divide="ignore"):
+            self.exchange_rate = np.where(self.exch_attempts > 0,
+                                          self.exch_accepted / np.maximum(self.exch_attempts, 1),
+                                          np.nan)
+        if self.lad.device_error():
+            raise N.ChxError(f"device error word {self.lad.device_error()} set during the run")
+        return hist
+
+    def collect_rungs(self):
+        beta = self.b["beta_host"]
+        k = min(self.n_collect, self.nrep)
+        if self.collect_beta is None:
+            return np.argsort(beta)[::-1][:k]
+        return np.argsort(np.abs(np.log(beta) - np.log(self.collect_beta)))[:k]
+
+    def _collect(self):
+        idx = self.collect_rungs()
+        sp = _host(self.species)[idx]
+        c2 = _host(self.chi2)[idx]
+        for a, b in zip(sp, c2):
+            self.samples.append((a.astype(np.int32), float(b)))
+
+    def posterior_wc(self, shell_r, i_idx, j_idx, shift, cell, nsp=None, tol=0.15):
+        from .lattice import warren_cowley
+        if not self.samples:
+            raise RuntimeError("no samples collected; set collect_after in the constructor")
+        n = nsp if nsp is not None else self.nsp
+        arr = np.array([warren_cowley(sp, i_idx, j_idx, shift, cell, shell_r, tol=tol,
+                                      nsp=n)[np.triu_indices(n)] for sp, _ in self.samples])
+        return arr.mean(0), arr.std(0), len(arr)
+
+    def best(self):
+        bc = _host(self.b["best_chi2"])
+        s = int(bc.argmin())
+        return (_host(self.b["best_sp"][s]).astype(np.int32), _host(self.b["best_pos"][s]),
+                float(bc[s]))
+
+
+class BatchedSampler:
+    """Many independent ladders in one launch per step, replayed as CUDA
+    graphs (one graph = `exchange_every` steps + a device replica exchange),
+    with FP64 re-anchoring of the running chi every `reanchor_every`
+    accepted moves (checked every `check_every` blocks)."""
+
+    def __init__(self, specs, precision=FP32C, exchange_every=25, use_table=True,
+                 reanchor_every=1000, check_every=40):
+        import torch
+        self.torch = torch
+        self.lad = Ladders(specs, precision=precision, use_table=use_table)
+        self.exchange_every = int(exchange_every)
+        self.reanchor_every = int(reanchor_every)
+        self.check_every = int(check_every)
+        self.graph = None
+        self.blocks = 0
+        self.reanchors = 0
+        self.steps = 0
+
+    @property
+    def nslots(self):
+        return self.lad.nslots
+
+    def init_state(self, species0, pos0):
+        """species0 / pos0: one array per ladder (or one shared by all)."""
+        for li in range(self.lad.nladders):
+            sp = species0[li] if isinstance(species0, (list, tuple)) else species0
+            ps = pos0[li] if isinstance(pos0, (list, tuple)) else pos0
+            self.lad.init_state(li, sp, ps)
+        self.lad.refresh_chi2(reset_best=True)
+
+    def block(self):
+        """One exchange period: exchange_every steps, then the exchange."""
+        for _ in range(self.exchange_every):
+            self.lad.step()
+        self.lad.exchange_device()
+
+    def capture(self):
+        torch = self.torch
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self.block()                      # sets kernel attributes before capture
+        torch.cuda.current_stream().wait_stream(side)
+        self.blocks += 1
+        self.steps += self.exchange_every
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.block()
+        self.graph = g
+        return g
+
+    def run_blocks(self, nblocks):
+        if self.graph is None:
+            self.capture()
+        for _ in range(nblocks):
+            self.graph.replay()
+            self.blocks += 1
+            self.steps += self.exchange_every
+            if self.reanchor_every and self.blocks % self.check_every == 0:
+                if int(max(int(b["n_acc"].max()) for b in self.lad.bufs)) >= self.reanchor_every:
+                    self.lad.reanchor()
+                    self.reanchors += 1
+
+    def best(self, li):
+        b = self.lad.bufs[li]
+        bc = _host(b["best_chi2"])
+        s = int(bc.argmin())
+        return _host(b["best_sp"][s]).astype(np.int32), float(bc[s])
+
+    def accept_rate(self):
+        tot = sum(int(b["n_acc"].sum()) for b in self.lad.bufs)
+        return tot

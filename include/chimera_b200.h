@@ -1,0 +1,298 @@
+/*
+ * chimera_b200.h -- C ABI of libchimera_b200.so, the B200 (sm_100a) EXAFS
+ * path-sum and parallel-tempering RMC hot path.
+ *
+ * Conventions
+ *   - Every function is extern "C", returns int: CHX_OK (0) or a negative
+ *     CHX_ERR_* code; chx_last_error() returns the message of the last failure
+ *     on the calling thread. Nothing aborts or traps.
+ *   - Every buffer is caller-allocated device memory (row-major, contiguous,
+ *     int32 indices, float64 unless stated). The library allocates nothing on
+ *     the hot path; kernels that need scratch take a caller buffer sized by the
+ *     matching *_scratch_bytes() query.
+ *   - Every launch is asynchronous on the caller's stream (`stream` is a
+ *     cudaStream_t passed as void*; NULL is the legacy default stream).
+ *   - Device-side faults are never provoked: kernels that detect an
+ *     out-of-range index or an exhausted bounded wait set a device error word
+ *     (CHX_DEVERR_*) that the caller reads back.
+ *
+ * Reference interfaces each entry point replaces are cited as file:line in
+ * the reference project (dluccioni/CHIMERA).
+ */
+#ifndef CHIMERA_B200_H
+#define CHIMERA_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CHX_API __attribute__((visibility("default")))
+#else
+#define CHX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHX_OK 0
+#define CHX_ERR_ARG (-1)          /* bad argument (null pointer, size, nsp)   */
+#define CHX_ERR_CUDA (-2)         /* a CUDA runtime call failed               */
+#define CHX_ERR_UNSUPPORTED (-3)  /* configuration outside the built kernels  */
+#define CHX_ERR_SCRATCH (-4)      /* scratch buffer smaller than required     */
+
+/* bits of the device error word */
+#define CHX_DEVERR_INDEX 1        /* an index read from a table was out of range */
+#define CHX_DEVERR_MSCOUNT 2      /* an MS count delta left the exact range      */
+
+/* precision of the path sums */
+#define CHX_FP64 0                /* FP64 throughout (reproduction mode)        */
+#define CHX_FP32C 1               /* FP32 transcendentals, FP64 phase reduction  */
+                                  /* and FP64 (compensated) accumulation         */
+
+CHX_API int chx_version(void);
+/* sizeof / offsetof of the ABI structs, for binding self-checks:
+ * 0 sizeof(chx_pairs_t), 1 sizeof(chx_ladder_t),
+ * 2 offsetof(chx_ladder_t, exch_acc), 3 offsetof(chx_ladder_t, seed) */
+CHX_API int64_t chx_struct_size(int which);
+CHX_API int chx_last_error(char *buf, int n);
+
+/* ------------------------------------------------------------------------
+ * 1. Entry points of the reference kernel module, same arguments and meaning.
+ *    These are what exafs_gpu/kernels.py:get(name, nsp) hands out
+ *    (kernels.py:685-686); nsp replaces the -DNSP=<n> compile option
+ *    (kernels.py:666-682).
+ * ------------------------------------------------------------------------ */
+
+/* exafs_gpu/kernels.py:53-78 (launched forward.py:154) */
+CHX_API int chx_compute_r(const double *pos, const int *iidx, const int *jidx,
+                  const double *shift, double *r, double *evec,
+                  int npairs, int natoms, int nconf, void *stream);
+
+/* exafs_gpu/kernels.py:81-96 (launched forward.py:163) */
+CHX_API int chx_build_ptype(const int *species, const int *iidx, const int *jidx, int *ptype,
+                    int npairs, int natoms, int nconf, int nsp, void *stream);
+
+/* exafs_gpu/kernels.py:99-163 (launched forward.py:177): full single-scattering
+ * path sum, FP64, chi (nconf, nsp, nk) unnormalised. */
+CHX_API int chx_chi_forward(const double *r, const int *ptype, const int *shell,
+                    const double *sig2, const double *ftab, const double *dtab,
+                    const double *lamtab, const double *ktab, const double *drtab,
+                    const double *c3tab, const double *s2tab, double *chi,
+                    int npairs, int nk, int nconf, double s02, int nsp, void *stream);
+
+/* exafs_gpu/kernels.py:243-325 (launched method_a_rmc.py:267) */
+CHX_API int chx_chi_delta(const double *r_old, const int *pt_old, const int *shell,
+                  const int *aff, const double *r_new, const int *pt_new,
+                  const double *sig2, const double *ftab, const double *dtab,
+                  const double *lamtab, const double *ktab, const double *drtab,
+                  const double *c3tab, const double *s2tab, double *dchi,
+                  int npairs, int nk, int nrep, int maxaff, double s02, int nsp,
+                  void *stream);
+
+/* exafs_gpu/kernels.py:328-346 (launched method_a_rmc.py:290) */
+CHX_API int chx_commit_move(const int *aff, const double *r_new, const int *pt_new,
+                    const uint8_t *accept, double *r_old, int *pt_old,
+                    int npairs, int nrep, int maxaff, void *stream);
+
+/* exafs_gpu/kernels.py:362-423 (launched method_a_rmc.py:253); the splitmix64
+ * stream keyed (seed, stepc, replica) is reproduced bit for bit. */
+CHX_API int chx_propose_select(const int *species, const double *pos, const double *ideal,
+                       int *a_out, int *b_out, int *newsa, int *newsb, double *newpa,
+                       uint8_t *isswap, int natoms, int nrep, uint64_t seed,
+                       uint64_t stepc, double swap_frac, double disp_sigma,
+                       double max_disp, void *stream);
+
+/* exafs_gpu/kernels.py:425-488 (launched method_a_rmc.py:260) */
+CHX_API int chx_propose_build(const int *species, const double *pos, const int *nbr,
+                      const int *rev, const int *iidx, const int *jidx,
+                      const double *shift, const int *a_in, const int *b_in,
+                      const int *newsa, const int *newsb, const double *newpa,
+                      int *aff, double *r_new, int *pt_new, int natoms, int ncoord,
+                      int npairs, int nrep, int maxaff, int nsp, void *stream);
+
+/* exafs_gpu/kernels.py:490-511 (launched method_a_rmc.py:294) */
+CHX_API int chx_commit_state(const uint8_t *accept, const int *a_in, const int *b_in,
+                     const int *newsa, const int *newsb, const double *newpa,
+                     const uint8_t *isswap, int *species, double *pos,
+                     int natoms, int nrep, void *stream);
+
+/* ------------------------------------------------------------------------
+ * 2. Full path sum from positions and species (A1): what ForwardModel.chi
+ *    computes with compute_r + build_ptype + chi_forward
+ *    (exafs_gpu/forward.py:169-188), without the (nconf, npairs) r/ptype
+ *    intermediates. Pair records are built per chunk of pairs into scratch and
+ *    staged into shared memory by bulk-async (TMA) copies; each chunk's partial
+ *    spectrum is reduced in a fixed order, so the result is deterministic.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    int natoms, ncoord, npairs, nsp, nk, nshell;
+    const int *iidx, *jidx;          /* (npairs), pair p = (iidx[p], jidx[p])   */
+    const double *shift;             /* (npairs, 3) periodic image of j         */
+    const int *shell;                /* (npairs)                                 */
+    const double *sig2;              /* (npairs)                                 */
+    const double *ftab;              /* (nsp, nk)   amplitude by scatterer       */
+    const double *dtab;              /* (nsp*nsp, nk) phase by pair type         */
+    const double *lamtab, *ktab;     /* (nk)                                     */
+    const double *drtab;             /* (nshell*nsp*nsp) bond-length offset      */
+    const double *c3tab;             /* (nshell) third cumulant                  */
+    const double *s2tab;             /* (nshell*nsp*nsp) extra sigma^2           */
+    double s02;
+} chx_pairs_t;
+
+CHX_API int64_t chx_chi_full_scratch_bytes(const chx_pairs_t *P, int nconf);
+/* chi (nconf, nsp, nk) unnormalised; precision CHX_FP64 or CHX_FP32C */
+CHX_API int chx_chi_full(const chx_pairs_t *P, const double *pos, const int *species, int nconf,
+                 int precision, double *chi, void *scratch, int64_t scratch_bytes,
+                 void *stream);
+
+/* ------------------------------------------------------------------------
+ * 3. Exact supercell multiple scattering (A2): entry counts of every
+ *    configuration (chimera/mslibrary.py:436-451) and chi_MS = counts @ table
+ *    per absorber block (mslibrary.py:453-457).
+ *    A path record is 4 int32: {absorber | class << 20, slot0, slot1, slot2},
+ *    slots -1 when unused; entry = s_abs*nblk + cls_off[class] + sum_q s_q nsp^q
+ *    (mslibrary.py:190-198, 433-434).
+ * ------------------------------------------------------------------------ */
+CHX_API int chx_ms_counts(const int *species, int nconf, int natoms, const int *paths,
+                  int64_t npath, const int *cls_off, int nsp, int nblk, int *counts,
+                  void *stream);
+/* Entry-count change of each replica's proposal (swap a <-> b to species nsa,
+ * nsb; a == b for a displacement, which changes nothing): paths through a and
+ * through b, a path through both counted once (mslibrary.py:466-486).
+ * inc (natoms, M, 4) holds the records of the paths incident on each site
+ * (padding rows -1); dC (nrep, nsp*nblk). */
+CHX_API int chx_ms_delta(const int *species, int nrep, int natoms, const int *inc, int M,
+                         const int *cls_off, int nsp, int nblk, const int *a, const int *b,
+                         const int *nsa, const int *nsb, int *dC, void *stream);
+/* chi (nconf, nsp, nk) += counts (nconf, nsp*nblk) @ T (nsp*nblk, nk), per block */
+CHX_API int chx_ms_chi_of(const int *counts, const double *T, int nconf, int nsp, int nblk,
+                  int nk, double *chi, void *stream);
+
+/* ------------------------------------------------------------------------
+ * 4. The fused PT-RMC step (A3-A7) and replica exchange (A8) of
+ *    methods/method_a_rmc.py:RMCSampler, for a batch of independent ladders.
+ *    One CTA per replica slot does: propose (kernels.py:362-423) -> affected
+ *    pairs (kernels.py:425-488) -> delta-chi of the pairs (kernels.py:243-325)
+ *    and of the MS paths through the two sites (mslibrary.py:466-486) ->
+ *    trial chi(R) on the fit window (fourier.py:75-80, multift.py:58-63) ->
+ *    profiled chi^2 (method_a_rmc.py:190-227) -> Metropolis
+ *    (method_a_rmc.py:280-285) -> commit (kernels.py:328-346, 490-511,
+ *    mslibrary.py:488-489) -> best-state retention (method_a_rmc.py:304-307).
+ *    Temperatures are exchanged by permuting the rung<->slot maps; the state
+ *    never moves, and every rung keeps its own proposal and acceptance
+ *    streams (keyed by rung), exactly as when the reference moves the state.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    /* topology and tables of this ladder's supercell */
+    int natoms, ncoord, npairs, nshell, nsp, nk;
+    const int *iidx, *jidx, *rev;    /* (npairs), i-major with uniform ncoord    */
+    const double *shift;             /* (npairs, 3)                              */
+    const int *shell;                /* (npairs)                                 */
+    const double *sig2;              /* (npairs)                                 */
+    const uint8_t *pair_tab;         /* (npairs) 1: pair may use the shell table */
+    const double *ideal;             /* (natoms, 3)                              */
+    const double *ftab, *dtab, *lamtab, *ktab, *drtab, *c3tab, *s2tab;
+    double s02;
+    const double *sstab;             /* (nshell*nsp*nsp, nk) ideal-shell terms, or NULL */
+    /* exact multiple scattering, ms_nblk == 0 when off */
+    int ms_nblk, ms_M;
+    const int *ms_inc;               /* (natoms, ms_M, 4) records incident on a site */
+    const int *ms_cls_off;
+    const double *ms_T;              /* (nsp*ms_nblk, nk)                         */
+    /* pair-interaction prior, etab NULL when off (method_a_rmc.py:147-157,310-320) */
+    const double *etab;              /* (nshell*nsp*nsp) eV per directed pair     */
+    double energy_beta;
+    /* transform (one channel per (edge, k weight), edge-major) and target */
+    int nchan, nkw, nwin, nfft, ncoef;
+    const int *ft_n0;                /* (nchan) first uniform-grid index          */
+    const int *ft_idx;               /* (nchan, ncoef) resample index             */
+    const double *ft_frac;           /* (nchan, ncoef) resample fraction          */
+    const double *ft_w;              /* (nchan, ncoef) inside * window * k^w      */
+    const int *win_bin;              /* (nwin) R bins of the fit window           */
+    const double *chi_extra;         /* (nsp, nk) added before the transform, or NULL */
+    const double *tw64;              /* (nfft, 2) cos, -sin of 2 pi j / nfft      */
+    double ft_norm;
+    const double *tm_re, *tm_im, *sm;/* (nchan, nwin) target window and sigma     */
+    int cplx, profile;
+    double nfit;
+    /* sampler constants */
+    uint64_t seed;
+    double swap_frac, disp_sigma, max_disp;
+    int nrep;                        /* rungs in this ladder                      */
+    int slot0;                       /* first slot of this ladder                 */
+    const double *beta_rung;         /* (nrep) inverse temperature of each rung   */
+    const double *u_stream;          /* (u_steps, nrep) acceptance uniforms, or NULL */
+    int64_t u_steps;
+    /* state, indexed by slot - slot0 */
+    int *species;                    /* (nrep, natoms)                            */
+    double *pos;                     /* (nrep, natoms, 3)                         */
+    uint8_t *moved;                  /* (nrep, natoms) 1 once displaced           */
+    double *chi;                     /* (nrep, nsp, nk) unnormalised, FP64        */
+    double *chi2;                    /* (nrep)                                    */
+    const double *count;             /* (nrep, nsp) absorber counts               */
+    int *rung_of;                    /* (nrep) slot -> rung                       */
+    int *slot_of;                    /* (nrep) rung -> slot                       */
+    double *best_chi2;               /* (nrep)                                    */
+    int *best_sp;                    /* (nrep, natoms)                            */
+    double *best_pos;                /* (nrep, natoms, 3)                         */
+    int *ms_C;                       /* (nrep, nsp*ms_nblk) entry counts          */
+    uint8_t *acc_rung;               /* (nrep) accept flag of the last step, by rung */
+    int *n_acc;                      /* (nrep) accepted moves per slot            */
+    int *exch_att, *exch_acc;        /* (nrep) exchange bookkeeping per rung pair */
+} chx_ladder_t;
+
+/* Bytes of dynamic shared memory the step kernel needs for these ladders. */
+CHX_API int chx_sampler_smem_bytes(const chx_ladder_t *host_ladders, int nladders, int precision);
+
+/* Fill sstab (nshell*nsp*nsp, nk) with the ideal-lattice term of every
+ * (shell, pair type) for ladder L: r = shell radius rshell[sh], sigma^2 =
+ * s2shell[sh]. FP64. */
+CHX_API int chx_shell_table(const chx_ladder_t *L, const double *rshell, const double *s2shell,
+                    double *sstab, void *stream);
+
+/* One sampler step for every slot. d_ladders: device array of nladders
+ * descriptors; slot_ladder (nslots): ladder of each slot. d_stepc: device
+ * counter, read as the step number (the reference's `_stepc`, first step = 1)
+ * and advanced by one when the step completes. d_err: device error word. */
+CHX_API int chx_sampler_step(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                     int nladders, const int *slot_ladder, int nslots, int precision,
+                     uint64_t *d_stepc, int *d_ticket, int *d_err, void *stream);
+
+/* chi^2 of every slot's state chi (chi_in NULL) or of chi_in (nslots, nsp, nk)
+ * with absorber counts count_in (nslots, nsp) (count NULL: the state's), by
+ * the step's own transform and profiled chi^2, into out (nslots). */
+CHX_API int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                          int nladders, const int *slot_ladder, int nslots, int precision,
+                          const double *chi_in, const double *count_in, double *out,
+                          void *stream);
+
+/* Replica exchange decided on the device (method_a_rmc.py:332-373): alternate
+ * adjacent rung pairs from a random start parity, accept d >= 0 or
+ * u < exp(max(d, -60)) with d = (b_i - b_{i+1})(E_i - E_{i+1}) nfit. The
+ * uniforms come from a splitmix64 stream keyed (seed, *round_key), round_key
+ * a device word (the step counter), so a captured graph draws fresh uniforms
+ * on every replay. */
+CHX_API int chx_replica_exchange(const chx_ladder_t *d_ladders, int nladders,
+                                 const uint64_t *round_key, void *stream);
+
+/* Apply a host-decided exchange: order (nrep) as the reference builds it
+ * (method_a_rmc.py:344-366); rung i takes the state rung order[i] held. */
+CHX_API int chx_apply_exchange(const chx_ladder_t *d_ladders, int ladder, const int *order,
+                       void *stream);
+
+/* ------------------------------------------------------------------------
+ * 5. Windowed FT of a batch of spectra to chi(R) on arbitrary R points (A5,
+ *    fourier.py:75-80 generalised to a direct transform). X (rows, nR) complex
+ *    interleaved; basis (nk, nR) complex = w(k) k^kw dk/sqrt(pi) e^{-2ikR}.
+ *    precision: 0 FP64 (SIMT), 1 TF32-class (FP32 SIMT), 2 split-BF16
+ *    three-product on tcgen05 tensor cores with FP32 accumulation.
+ * ------------------------------------------------------------------------ */
+CHX_API int chx_ft_batch(const double *chi, int rows, int nk, const double *basis, int nR,
+                 int precision, double *out, void *scratch, int64_t scratch_bytes,
+                 void *stream);
+CHX_API int64_t chx_ft_batch_scratch_bytes(int rows, int nk, int nR, int precision);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHIMERA_B200_H */

@@ -1,0 +1,68 @@
+"""The fused device sampler step (A3-A8) against the reference's golden
+traces and against full recomputes."""
+import numpy as np
+import pytest
+
+from cases import device_objects, trace_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["rmc_trace.npz", "rmc_trace_disp.npz", "rmc_trace_ms.npz"])
+def test_fp64_reproduces_reference_accept_sequence(cuda, name):
+    """FP64 acceptance fed the reference's RNG streams gives the reference's
+    accepted-swap sequence, exchanges and final configuration."""
+    d = trace_inputs(name)
+    smp, fm = device_objects(d, precision=0, reproduce=True)
+    smp.init_state(d["species0"], d["ideal"])
+    acc, c2 = [], []
+    for it in range(int(d["nsteps"])):
+        acc.append(smp.step().cpu().numpy())
+        c2.append(smp.chi2.cpu().numpy())
+        if (it + 1) % 25 == 0:
+            smp.replica_exchange()
+    acc = np.array(acc)
+    mism = np.argwhere(acc != d["accepted"])
+    assert mism.size == 0, f"first mismatch at step/rung {mism[0]}"
+    assert np.allclose(np.array(c2), d["chi2_log"], rtol=1e-9, atol=0)
+    assert np.array_equal(smp.species.cpu().numpy(), d["final_species"])
+    assert np.allclose(smp.pos.cpu().numpy(), d["final_pos"], rtol=0, atol=1e-13)
+    assert np.allclose(smp.chi.cpu().numpy(), d["final_chi"], rtol=1e-9, atol=1e-11)
+    assert smp.lad.device_error() == 0
+
+
+def test_run_matches_reference_run_summary(cuda):
+    d = trace_inputs("rmc_trace.npz")
+    smp, fm = device_objects(d, precision=0, reproduce=True)
+    smp.init_state(d["species0"], d["ideal"])
+    smp.run(int(d["nsteps"]), exchange_every=25, log_every=10 ** 9)
+    bsp, bpos, bc2 = smp.best()
+    assert np.array_equal(bsp, d["best_species"])
+    assert abs(bc2 - float(d["best_chi2"])) <= 1e-9 * abs(float(d["best_chi2"]))
+    assert abs(smp.best_verified - float(d["best_verified"])) <= 1e-9 * abs(float(d["best_verified"]))
+    assert np.allclose(smp.exchange_rate, d["exchange_rate"], equal_nan=True)
+
+
+@pytest.mark.parametrize("name", ["rmc_trace.npz", "rmc_trace_disp.npz", "rmc_trace_ms.npz"])
+def test_fp32c_tracks_full_recompute(cuda, name):
+    """FP32C (tabulated ideal shells, FP32 transforms): after a device-only run
+    the running chi equals an FP64 recompute of the state to 1e-6 (per absorber),
+    the composition is conserved and the best state verifies."""
+    torch = cuda
+    d = trace_inputs(name)
+    smp, fm = device_objects(d, precision=1, reproduce=False)
+    smp.init_state(d["species0"], d["ideal"])
+    smp.run(300, exchange_every=25, log_every=10 ** 9)
+    lad, b = smp.lad, smp.b
+    chi = b["chi"].cpu().numpy()
+    full = fm.chi_full(b["pos"], b["species"]).cpu().numpy()
+    if smp.ms is not None:
+        full = full + smp.ms.chi_of(b["ms_C"]).cpu().numpy()
+        assert np.array_equal(b["ms_C"].cpu().numpy(), smp.ms.counts(b["species"]).cpu().numpy())
+    cnt = b["count"].cpu().numpy()[:, :, None]
+    assert np.abs(chi / cnt - full / cnt).max() <= 1e-6
+    sp = b["species"].cpu().numpy()
+    assert (np.bincount(sp[0], minlength=2) == np.bincount(d["species0"], minlength=2)).all()
+    assert all((np.sort(s) == np.sort(d["species0"])).all() for s in sp)
+    assert abs(smp.best_verified - smp.best()[2]) <= 1e-3 * abs(smp.best()[2])
+    assert lad.device_error() == 0
