@@ -11,8 +11,8 @@ chi(R) fitted on 1.4-5.0 A; 16 sample positions (seeded noise) x 32 PT rungs =
 reduction and accumulation, FP64 re-anchoring every 1,000 accepted moves.
 
 One bench "step" is one exchange period: 25 sampler steps of every replica
-(one fused launch each) and one device replica exchange, replayed as a CUDA
-graph. value = swap attempts per second over all ranks. With --gpus N every
+(one persistent fused launch) and one device replica exchange, replayed as a
+CUDA graph. value = swap attempts per second over all ranks. With --gpus N every
 rank runs its own 16 ladders (weak scaling, no collective in the timed loop).
 
 --impl reference times the CPU restatement of the reference sampler (oracle/,
@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "PT-RMC GPU-s to plain's R-factor: learned+batched vs plain GPU; chi err vs FP64"
 UNIT = "swap attempts/s"
-NPOS, NREP, EXCH = 16, 32, 25
+NPOS, NREP, EXCH = 16, 32, 25      # positions (ladders) per GPU, rungs, steps per block
 
 
 def workload_config():
@@ -148,25 +148,41 @@ def time_graph(fn, reps):
     return a.elapsed_time(b) / 1e3
 
 
-def cpu_baseline(prob, nsteps=40, nrep=NREP):
-    """The oracle's plain sampler on one ladder of this workload, one core."""
+def oracle_problem(prob, p):
+    """The oracle's problem for sample position p, built on the host only:
+    the target comes from the oracle's own path sum, MS counts and FFT."""
+    from oracle import kernels as K
     from oracle import sampler as OS
-    st = prob.position(0)
-    chans = []
-    for c, f in enumerate(prob.ft.fts):
-        chans.append(OS.Channel(f._idx, f._frac, f._inside, f._w, f.nfft, f._norm,
-                                int(prob.ft.chan_edge[c])))
-    ms = prob.ms
+    chans = [OS.Channel(f._idx, f._frac, f._inside, f._w, f.nfft, f._norm,
+                        int(prob.ft.chan_edge[c])) for c, f in enumerate(prob.ft.fts)]
     msd = None
-    if ms is not None:
-        P = ms.paths
+    if prob.paths is not None:
+        P = prob.paths
         msd = dict(p_abs=P.p_abs, p_cls=P.p_cls, p_slot=P.p_slot, inc=P.inc, cls_off=P.cls_off,
-                   nblk=P.nblk, T=ms.T.cpu().numpy())
+                   nblk=P.nblk, T=prob.ms_table)
+    nchan = len(chans)
     pr = OS.Problem(prob.cell.ideal, prob.top.i, prob.top.j, prob.top.shift, prob.top.shell,
                     prob.top.sigma2, prob.k, prob.tables.f, prob.tables.delta, prob.tables.lam,
-                    prob.tables.s02, chans, st.target, st.mask, st.sigma_R, prob.nsp, ms=msd)
-    smp = OS.PlainSampler(pr, nrep, 1e-4, 1e-1, 0, 1.0, 0.012, 0.10)
-    smp.init_state(prob.random_config(0), prob.cell.ideal)
+                    prob.tables.s02, chans, np.zeros((nchan, 1024), complex), prob.mask,
+                    prob.sigma_R(), prob.nsp, ms=msd)
+    sp = prob.target_species[None]
+    chi, _, _ = pr.chi_full(prob.cell.ideal[None], sp)
+    if msd is not None:
+        chi = chi + pr.ms_chi(pr.ms_counts(sp))
+    cnt = np.bincount(prob.target_species, minlength=prob.nsp).astype(float)
+    chi = chi[0] / np.maximum(cnt, 1)[:, None] + prob.noise_k(p)
+    target = pr.observe(chi[None])[0]
+    pr.target, pr.tm = target, np.ascontiguousarray(target[:, prob.mask])
+    del K
+    return pr
+
+
+def cpu_baseline(prob, nsteps=40, nrep=NREP, p=0):
+    """The oracle's plain sampler on one ladder of this workload, one core."""
+    from oracle import sampler as OS
+    pr = oracle_problem(prob, p)
+    smp = OS.PlainSampler(pr, nrep, 1e-4, 1e-1, p, 1.0, 0.012, 0.10)
+    smp.init_state(prob.random_config(p), prob.cell.ideal)
     smp.step()
     t0 = time.perf_counter()
     for it in range(nsteps):
@@ -185,10 +201,9 @@ def run_reference(args):
     if rank != 0:
         return 0
     import multiprocessing as mp
-    prob = build_problem()
     ncores = os.cpu_count() or 1
     nproc = max(1, min(NPOS, ncores))
-    steps = max(1, args.steps) * 4
+    steps = max(5, min(args.steps, 40))
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(nproc) as pool:
@@ -215,19 +230,24 @@ def _ref_worker(arg):
     sys.path.insert(0, ROOT)
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     prob = build_problem()
-    r = cpu_baseline(prob, nsteps=steps)
+    r = cpu_baseline(prob, nsteps=steps, p=p)
     return {"attempts": steps * NREP, "seconds": steps * NREP / r["value"]}
 
 
 def main():
+    global NPOS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--positions", type=int, default=16,
+                    help="ladders per GPU (fewer for a small profiling case)")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
+    NPOS = args.positions
     if args.impl == "reference":
         return run_reference(args)
 
@@ -272,18 +292,16 @@ def main():
     attempts = smp.nslots * EXCH * args.steps * world
     value = attempts / dt
 
-    # ---- dominant kernel: the fused step, timed alone as a graph of 25 launches
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(g):
-        for _ in range(EXCH):
-            smp.lad.step()
-    g.replay()
+    # ---- dominant kernel: the fused step (one launch = 25 steps of every
+    # replica), timed alone on its stream; per_step = one replica-step sweep
+    smp.lad.step(EXCH)
     torch.cuda.synchronize()
     reps = 20
-    t_steps = time_graph(g.replay, reps)
-    per_launch = t_steps / (reps * EXCH)
+    t_steps = time_graph(lambda: smp.lad.step(EXCH), reps)
+    per_launch = t_steps / reps
+    per_step = per_launch / EXCH
     hbm, src = peaks()
-    achieved = step_bytes(prob) * smp.nslots / per_launch / 1e9
+    achieved = step_bytes(prob) * smp.nslots * EXCH / per_launch / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "step_traffic.json")
     if os.path.exists(tp):
@@ -293,9 +311,12 @@ def main():
     torch.cuda.synchronize()
     e2e_blocks = max(4, args.steps // 4)
     t0 = time.perf_counter()
-    smp2 = make_sampler(prob, rank)
-    smp2.init_state(sp0, prob.cell.ideal)
-    smp2.run_blocks(e2e_blocks)
+    if not args.no_e2e:
+        smp2 = make_sampler(prob, rank)
+        smp2.init_state(sp0, prob.cell.ideal)
+        smp2.run_blocks(e2e_blocks)
+    else:
+        smp2 = smp
     best = [smp2.best(li) for li in range(NPOS)]
     torch.cuda.synchronize()
     e2e_dt = time.perf_counter() - t0
@@ -317,15 +338,15 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "peak_source": src, "kernel": "k_step (fused sampler step)",
-                         "launch_us": per_launch * 1e6,
-                         "bytes_per_launch": step_bytes(prob) * smp.nslots},
+                         "launch_us": per_launch * 1e6, "step_us": per_step * 1e6,
+                         "bytes_per_launch": step_bytes(prob) * smp.nslots * EXCH},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": h2d / (e2e_blocks + 1),
                     "d2h_bytes_per_step": d2h / (e2e_blocks + 1),
                     "note": "fresh sampler from host arrays: upload, init, run, best configs "
                             "back; bytes amortised over the run's bench steps"},
-            "gpu_launches": args.steps * (EXCH + 1),
+            "gpu_launches": args.steps * 2,
             "clocks": clocks,
             "device_error": err,
             "reanchors": smp.reanchors,

@@ -47,12 +47,13 @@ class Ladder(C.Structure):
         ("iidx", c_p), ("jidx", c_p), ("rev", c_p), ("shift", c_p), ("shell", c_p),
         ("sig2", c_p), ("pair_tab", c_p), ("ideal", c_p),
         ("ftab", c_p), ("dtab", c_p), ("lamtab", c_p), ("ktab", c_p), ("drtab", c_p),
-        ("c3tab", c_p), ("s2tab", c_p), ("s02", c_d), ("sstab", c_p),
-        ("ms_nblk", c_i), ("ms_M", c_i), ("ms_inc", c_p), ("ms_cls_off", c_p), ("ms_T", c_p),
+        ("c3tab", c_p), ("s2tab", c_p), ("s02", c_d), ("sstab", c_p), ("sstab32", c_p),
+        ("ms_nblk", c_i), ("ms_M", c_i), ("ms_inc", c_p), ("ms_T", c_p),
+        ("ms_T32", c_p),
         ("etab", c_p), ("energy_beta", c_d),
         ("nchan", c_i), ("nkw", c_i), ("nwin", c_i), ("nfft", c_i), ("ncoef", c_i),
         ("ft_n0", c_p), ("ft_idx", c_p), ("ft_frac", c_p), ("ft_w", c_p), ("win_bin", c_p),
-        ("chi_extra", c_p), ("tw64", c_p), ("ft_norm", c_d),
+        ("chi_extra", c_p), ("ft_norm", c_d),
         ("tm_re", c_p), ("tm_im", c_p), ("sm", c_p), ("cplx", c_i), ("profile", c_i),
         ("nfit", c_d),
         ("seed", c_u64), ("swap_frac", c_d), ("disp_sigma", c_d), ("max_disp", c_d),
@@ -60,7 +61,7 @@ class Ladder(C.Structure):
         ("u_steps", c_i64),
         ("species", c_p), ("pos", c_p), ("moved", c_p), ("chi", c_p), ("chi2", c_p),
         ("count", c_p), ("rung_of", c_p), ("slot_of", c_p), ("best_chi2", c_p),
-        ("best_sp", c_p), ("best_pos", c_p), ("ms_C", c_p), ("acc_rung", c_p), ("n_acc", c_p),
+        ("best_sp", c_p), ("best_pos", c_p), ("ms_C", c_p), ("acc_rung", c_p), ("acc_log", c_p), ("n_acc", c_p),
         ("exch_att", c_p), ("exch_acc", c_p)]
 
 
@@ -79,13 +80,13 @@ _SIGS = {
     "chx_commit_state": ([c_p] * 9 + [c_i, c_i, c_p], c_i),
     "chx_chi_full_scratch_bytes": ([c_p, c_i], c_i64),
     "chx_chi_full": ([c_p, c_p, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),
-    "chx_ms_counts": ([c_p, c_i, c_i, c_p, c_i64, c_p, c_i, c_i, c_p, c_p], c_i),
-    "chx_ms_delta": ([c_p, c_i, c_i, c_p, c_i, c_p, c_i, c_i, c_p, c_p, c_p, c_p, c_p, c_p], c_i),
+    "chx_ms_counts": ([c_p, c_i, c_i, c_p, c_i64, c_i, c_i, c_p, c_p], c_i),
+    "chx_ms_delta": ([c_p, c_i, c_i, c_p, c_i, c_i, c_i, c_p, c_p, c_p, c_p, c_p, c_p], c_i),
     "chx_eval_chi2": ([c_p, c_p, c_i, c_p, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
     "chx_ms_chi_of": ([c_p, c_p, c_i, c_i, c_i, c_i, c_p, c_p], c_i),
     "chx_sampler_smem_bytes": ([c_p, c_i, c_i], c_i),
     "chx_shell_table": ([c_p, c_p, c_p, c_p, c_p], c_i),
-    "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
+    "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
     "chx_replica_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_apply_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_ft_batch": ([c_p, c_i, c_i, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),

@@ -177,7 +177,8 @@ __global__ void k_propose_select(const int *__restrict__ species, const double *
     const int *S = species + (long)c * natoms;
     const double *P = pos + (long)c * natoms * 3;
     const double *Id = ideal + (long)c * natoms * 3;
-    Proposal pr = propose_one(S, P, Id, natoms, seed, stepc, c, swap_frac, disp_sigma, max_disp);
+    Proposal pr = propose_one([S](int i) { return S[i]; }, P, Id, natoms, seed, stepc, c,
+                              swap_frac, disp_sigma, max_disp);
     isswap[c] = (uint8_t)pr.swap;
     a_out[c] = pr.a;
     b_out[c] = pr.b;

@@ -11,9 +11,12 @@ struct Proposal {
     double np[3];
 };
 
-__device__ __forceinline__ Proposal propose_one(const int *S, const double *P, const double *Id, int natoms,
-                                uint64_t seed, uint64_t stepc, int c, double swap_frac,
-                                double disp_sigma, double max_disp) {
+// S(i) returns the species of site i (an array or a shared-memory accessor).
+template <typename SpeciesOf>
+__device__ __forceinline__ Proposal propose_one(SpeciesOf S, const double *P, const double *Id,
+                                                int natoms, uint64_t seed, uint64_t stepc, int c,
+                                                double swap_frac, double disp_sigma,
+                                                double max_disp) {
     Proposal pr;
     uint64_t h = splitmix64(seed ^ (stepc * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)c << 32));
     h = splitmix64(h);
@@ -21,13 +24,13 @@ __device__ __forceinline__ Proposal propose_one(const int *S, const double *P, c
     h = splitmix64(h);
     int a = (int)(u01(h) * natoms);
     if (a >= natoms) a = natoms - 1;
-    int sa = S[a], b = a, sb = sa;
+    int sa = S(a), b = a, sb = sa;
     if (sw) {
         for (int t = 0; t < 8; ++t) {
             h = splitmix64(h);
             int cand = (int)(u01(h) * natoms);
             if (cand >= natoms) cand = natoms - 1;
-            int sc = S[cand];
+            int sc = S(cand);
             if (sc != sa) {
                 b = cand;
                 sb = sc;

@@ -201,10 +201,9 @@ static PathsumPlan plan_pathsum(const chx_pairs_t *P, int nconf) {
 
 // ------------------------------------------------------- multiple scattering
 // Entry of one path record {abs | cls << 20, s0, s1, s2} (mslibrary.py:433-434)
-__device__ __forceinline__ int ms_entry(const int *S, int4 rc, const int *cls_off, int nsp,
-                                        int nblk) {
-    int ab = rc.x & 0xFFFFF, cl = rc.x >> 20;
-    int e = S[ab] * nblk + cls_off[cl];
+__device__ __forceinline__ int ms_entry(const int *S, int4 rc, int nsp, int nblk) {
+    int ab = rc.x & 0xFFFFF;
+    int e = S[ab] * nblk + (rc.x >> 20);
     int pw = 1;
     if (rc.y >= 0) e += S[rc.y] * pw;
     pw *= nsp;
@@ -217,8 +216,7 @@ __device__ __forceinline__ int ms_entry(const int *S, int4 rc, const int *cls_of
 // grid (ncta, nconf): a shared-memory histogram of entries per CTA
 __global__ void __launch_bounds__(256) k_ms_counts(const int *__restrict__ species, int natoms,
                                                    const int4 *__restrict__ paths, long npath,
-                                                   const int *__restrict__ cls_off, int nsp,
-                                                   int nblk, int *__restrict__ counts,
+                                                   int nsp, int nblk, int *__restrict__ counts,
                                                    long per_cta) {
     extern __shared__ int hist[];
     int nent = nsp * nblk;
@@ -229,7 +227,7 @@ __global__ void __launch_bounds__(256) k_ms_counts(const int *__restrict__ speci
     long p0 = (long)blockIdx.x * per_cta, p1 = min(npath, p0 + per_cta);
     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
         int4 rc = __ldg(&paths[p]);
-        atomicAdd(&hist[ms_entry(S, rc, cls_off, nsp, nblk)], 1);
+        atomicAdd(&hist[ms_entry(S, rc, nsp, nblk)], 1);
     }
     __syncthreads();
     for (int e = threadIdx.x; e < nent; e += blockDim.x)
@@ -240,8 +238,7 @@ __global__ void __launch_bounds__(256) k_ms_counts(const int *__restrict__ speci
 // one CTA per replica: the change of the entry counts along the paths through
 // a and b (the sampler step does the same inline)
 __global__ void __launch_bounds__(256) k_ms_delta(const int *__restrict__ species, int natoms,
-                                                  const int4 *__restrict__ inc, int M,
-                                                  const int *__restrict__ cls_off, int nsp,
+                                                  const int4 *__restrict__ inc, int M, int nsp,
                                                   int nblk, const int *__restrict__ a_in,
                                                   const int *__restrict__ b_in,
                                                   const int *__restrict__ nsa_in,
@@ -259,10 +256,10 @@ __global__ void __launch_bounds__(256) k_ms_delta(const int *__restrict__ specie
         if (half && b == a) break;
         int4 rc = __ldg(&inc[(long)(half ? b : a) * M + (m - half * M)]);
         if (rc.x < 0) continue;
-        int ab = rc.x & 0xFFFFF, cl = rc.x >> 20;
+        int ab = rc.x & 0xFFFFF;
         if (half && (ab == a || rc.y == a || rc.z == a || rc.w == a)) continue;
-        int eo = ms_entry(S, rc, cls_off, nsp, nblk);
-        int en = sp(ab) * nblk + cls_off[cl];
+        int eo = ms_entry(S, rc, nsp, nblk);
+        int en = sp(ab) * nblk + (rc.x >> 20);
         int pw = 1;
         if (rc.y >= 0) en += sp(rc.y) * pw;
         pw *= nsp;
@@ -364,8 +361,8 @@ int chx_chi_full(const chx_pairs_t *P, const double *pos, const int *species, in
 }
 
 int chx_ms_counts(const int *species, int nconf, int natoms, const int *paths, int64_t npath,
-                  const int *cls_off, int nsp, int nblk, int *counts, void *stream) {
-    CHX_REQUIRE(species && paths && cls_off && counts && nconf > 0 && npath > 0 && nsp >= 2 &&
+                  int nsp, int nblk, int *counts, void *stream) {
+    CHX_REQUIRE(species && paths && counts && nconf > 0 && npath > 0 && nsp >= 2 &&
                     nblk > 0 && natoms > 0 && natoms < (1 << 20),
                 "ms_counts: bad arguments");
     int nent = nsp * nblk;
@@ -381,15 +378,15 @@ int chx_ms_counts(const int *species, int nconf, int natoms, const int *paths, i
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_ms_counts, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_ms_counts<<<dim3(ncta, nconf), 256, smem, st>>>(species, natoms, (const int4 *)paths, npath,
-                                                      cls_off, nsp, nblk, counts, per_cta);
+                                                      nsp, nblk, counts, per_cta);
     CHX_CHECK_LAUNCH("ms_counts");
     return CHX_OK;
 }
 
-int chx_ms_delta(const int *species, int nrep, int natoms, const int *inc, int M,
-                 const int *cls_off, int nsp, int nblk, const int *a, const int *b,
-                 const int *nsa, const int *nsb, int *dC, void *stream) {
-    CHX_REQUIRE(species && inc && cls_off && a && b && nsa && nsb && dC && nrep > 0 && M > 0 &&
+int chx_ms_delta(const int *species, int nrep, int natoms, const int *inc, int M, int nsp,
+                 int nblk, const int *a, const int *b, const int *nsa, const int *nsb, int *dC,
+                 void *stream) {
+    CHX_REQUIRE(species && inc && a && b && nsa && nsb && dC && nrep > 0 && M > 0 &&
                     nsp >= 2 && nblk > 0,
                 "ms_delta: bad arguments");
     size_t smem = sizeof(int) * (size_t)nsp * nblk;
@@ -397,7 +394,7 @@ int chx_ms_delta(const int *species, int nrep, int natoms, const int *inc, int M
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_ms_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_ms_delta<<<nrep, 256, smem, as_stream(stream)>>>(species, natoms, (const int4 *)inc, M,
-                                                       cls_off, nsp, nblk, a, b, nsa, nsb, dC);
+                                                       nsp, nblk, a, b, nsa, nsb, dC);
     CHX_CHECK_LAUNCH("ms_delta");
     return CHX_OK;
 }

@@ -1,13 +1,17 @@
 // chx_sampler.cu -- the fused parallel-tempering RMC step (A3-A7), the
 // replica exchange (A8) and the ideal-shell term table.
 //
-// One CTA per replica slot runs the whole step of methods/method_a_rmc.py
-// (RMCSampler.step, :250-308) for its replica:
+// One CTA per replica slot runs `nsteps` consecutive steps of
+// methods/method_a_rmc.py (RMCSampler.step, :250-308) for its replica.
+// Replicas only interact at replica exchange, so a launch covers the steps
+// between two exchanges and the replica's species live in shared memory for
+// all of them (one byte per site: species in bits 0-6, "displaced from its
+// ideal site" in bit 7). Each step:
 //   1. propose: the reference's splitmix64 stream keyed (seed, step, rung),
 //      bit-identical (exafs_gpu/kernels.py:362-423);
 //   2. the affected directed pairs: both directions of every bond of a, and of
 //      b with the pairs through a dropped (kernels.py:425-488); old and new
-//      (r, type) of each, r recomputed from the positions;
+//      (r, type) of each, r recomputed from the positions when needed;
 //   3. delta chi(k) of those pairs (kernels.py:243-325). In CHX_FP32C a pair
 //      whose two atoms sit on their ideal sites takes its term from the
 //      (shell, pair type) table, so a swap costs a count of type changes
@@ -17,31 +21,28 @@
 //      the entry table;
 //   4. the trial chi, normalised per absorber and shifted by chi_extra, is
 //      resampled, windowed and transformed on the fit-window R bins only
-//      (exafs_gpu/fourier.py:69-80, chimera/multift.py:58-63) by a direct
-//      transform against a twiddle table in shared memory;
+//      (exafs_gpu/fourier.py:69-80, chimera/multift.py:58-63): one thread per
+//      (bin, half of the taps) accumulates every channel, the twiddle
+//      e^{-2 pi i n m / nfft} advanced by complex rotation and re-seeded
+//      exactly (sincospi) every 32 taps;
 //   5. profiled-scale chi^2 (method_a_rmc.py:190-227), Metropolis with the
 //      energy prior (method_a_rmc.py:280-285, 310-320);
 //   6. commit of species, position, chi, chi^2, MS counts and best state
 //      (kernels.py:328-346, 490-511; method_a_rmc.py:298-307).
-// The last CTA to finish advances the step counter, so a sequence of steps is
-// a sequence of identical launches (CUDA-graph capturable).
-#include <algorithm>
+// The last CTA to finish advances the step counter, so a sequence of blocks
+// is a sequence of identical launches (CUDA-graph capturable).
 #include "chx_device.cuh"
 
 namespace chx {
 
 constexpr int kStepThreads = 256;
 constexpr int kMaxCoord = 256;
-
-struct DirRec {      // one directly evaluated term: a PairRec plus its sign
-    PairRec r;
-    int neg;
-    int pad[3];
-};
+constexpr int kReseed = 32;      // taps between exact twiddles in the transform
+constexpr int kMaxSplit = 2;     // threads sharing one bin's taps
 
 // Shared-memory carve-up of one step CTA (all offsets 16-byte aligned).
 struct StepSmem {
-    size_t tw, u, x, tr, dchi, dir, dirv, hist, dn, list, total;
+    size_t u, x, tr, dchi, dir, dirv, hist, dn, list, sp, total;
 };
 
 template <typename T>
@@ -54,22 +55,23 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     int maxaff = 4 * L.ncoord;
     int nent = L.ms_nblk ? L.nsp * L.ms_nblk : 0;
     int ndn = L.nshell * L.nsp * L.nsp;
-    s.tw = o; o += f64 ? al16<double2>(L.nfft) : al16<float2>(L.nfft);
     s.u = o; o += f64 ? al16<double>((size_t)L.nchan * L.ncoef) : al16<float>((size_t)L.nchan * L.ncoef);
-    s.x = o; o += f64 ? al16<double2>((size_t)L.nchan * L.nwin) : al16<float2>((size_t)L.nchan * L.nwin);
+    s.x = o; o += (f64 ? al16<double2>((size_t)kMaxSplit * L.nchan * L.nwin)
+                       : al16<float2>((size_t)kMaxSplit * L.nchan * L.nwin));
     s.tr = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.dchi = o; o += al16<double>((size_t)L.nsp * L.nk);
-    s.dir = o; o += al16<DirRec>((size_t)2 * maxaff);
+    s.dir = o; o += al16<PairRec>((size_t)2 * maxaff);
     s.dirv = o; o += al16<int>((size_t)2 * maxaff);
     s.hist = o; o += al16<int>((size_t)std::max(nent, 1));
     s.dn = o; o += al16<int>((size_t)std::max(ndn, 1));
-    s.list = o; o += al16<int>((size_t)(2 * maxaff + ndn + nent + 32));
+    s.list = o; o += al16<int>((size_t)(2 * maxaff + 2 * ndn + 2 * nent + 64));
+    s.sp = o; o += al16<uint8_t>((size_t)L.natoms);
     s.total = o;
     return s;
 }
 
 // Deterministic in-order compaction by one warp: writes the indices i < n
-// with flag(i) into out, returns the count (valid in lane 0's view for all).
+// with flag(i) into out, returns the count.
 template <typename F>
 __device__ __forceinline__ int warp_compact(int n, F flag, int *out) {
     int lane = threadIdx.x & 31, cnt = 0;
@@ -83,11 +85,24 @@ __device__ __forceinline__ int warp_compact(int n, F flag, int *out) {
     return cnt;
 }
 
-__device__ __forceinline__ int ms_entry_new(const int *S, int4 rc, const int *cls_off, int nsp,
-                                            int nblk, int a, int b, int nsa, int nsb) {
-    auto sp = [&](int site) { return site == a ? nsa : (site == b ? nsb : S[site]); };
-    int ab = rc.x & 0xFFFFF, cl = rc.x >> 20;
-    int e = sp(ab) * nblk + cls_off[cl];
+// The same compaction of the non-zero entries of cnt[0..n) as (index, count).
+__device__ __forceinline__ int warp_compact_pairs(int n, const int *cnt, int2 *out) {
+    int lane = threadIdx.x & 31, tot = 0;
+    for (int i0 = 0; i0 < n; i0 += 32) {
+        int i = i0 + lane;
+        int v = i < n ? cnt[i] : 0;
+        unsigned m = __ballot_sync(0xffffffffu, v != 0);
+        if (v != 0) out[tot + __popc(m & ((1u << lane) - 1))] = make_int2(i, v);
+        tot += __popc(m);
+    }
+    return tot;
+}
+
+// Library entry of a path record {abs | class entry offset << 20, s0, s1, s2}
+// under the species accessor sp (mslibrary.py:433-434).
+template <typename SpeciesOf>
+__device__ __forceinline__ int ms_entry(SpeciesOf sp, int4 rc, int nsp, int nblk) {
+    int e = sp(rc.x & 0xFFFFF) * nblk + (rc.x >> 20);
     int pw = 1;
     if (rc.y >= 0) e += sp(rc.y) * pw;
     pw *= nsp;
@@ -96,52 +111,99 @@ __device__ __forceinline__ int ms_entry_new(const int *S, int4 rc, const int *cl
     if (rc.w >= 0) e += sp(rc.w) * pw;
     return e;
 }
-__device__ __forceinline__ int ms_entry_old(const int *S, int4 rc, const int *cls_off, int nsp,
-                                            int nblk) {
-    return ms_entry_new(S, rc, cls_off, nsp, nblk, -1, -1, 0, 0);
+
+template <int PREC>
+struct Real {
+    typedef float T;
+    typedef float2 T2;
+};
+template <>
+struct Real<CHX_FP64> {
+    typedef double T;
+    typedef double2 T2;
+};
+
+// e^{-2 pi i j / nfft} for an integer j reduced mod nfft (nfft a power of 2,
+// so 2 j / nfft is exact): sincospi evaluates it to FP32/FP64 rounding.
+__device__ __forceinline__ float2 twiddle(int j, float inv_half) {
+    float s, c;
+    sincospif((float)j * inv_half, &s, &c);
+    return make_float2(c, -s);
+}
+__device__ __forceinline__ double2 twiddle(int j, double inv_half) {
+    double s, c;
+    sincospi((double)j * inv_half, &s, &c);
+    return make_double2(c, -s);
 }
 
-// Steps 4-5 of the step (and the whole of k_eval_chi2): resample x window x
-// k^w the normalised trial chi s_tr (nsp, nk), transform it on the window
-// bins against the twiddles s_tw, and reduce the profiled chi^2 into s_c2.
+// Steps 4-5 (and the whole of k_eval_chi2): resample x window x k^w the
+// normalised trial chi s_tr (nsp, nk) into s_u [tap][channel], transform it
+// on the window bins, and reduce the profiled chi^2 into *s_c2.
 template <int NSP, int PREC>
-__device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr,
-                        const typename std::conditional<PREC == CHX_FP64, double2, float2>::type *s_tw,
-                        typename std::conditional<PREC == CHX_FP64, double, float>::type *s_u,
-                        typename std::conditional<PREC == CHX_FP64, double2, float2>::type *s_x,
-                        double *s_num, double *s_den, double *s_sq, double *s_scale,
-                        double *s_c2) {
-    typedef typename std::conditional<PREC == CHX_FP64, double, float>::type real;
-    typedef typename std::conditional<PREC == CHX_FP64, double2, float2>::type real2;
+__device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real<PREC>::T *s_u,
+                        typename Real<PREC>::T2 *s_x, double *s_num, double *s_den,
+                        double *s_sq, double *s_scale, double *s_c2) {
+    typedef typename Real<PREC>::T real;
+    typedef typename Real<PREC>::T2 real2;
+    constexpr int MAXCH = 3 * NSP;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nk = L.nk;
     const int nchan = L.nchan, ncoef = L.ncoef, nwin = L.nwin, nkw = L.nkw;
     for (int q = tid; q < nchan * ncoef; q += blockDim.x) {
-        int ch = q / ncoef, e = ch / nkw;
+        int ch = q / ncoef, j = q - ch * ncoef, e = ch / nkw;
         int id = L.ft_idx[q];
         double va = s_tr[e * nk + id], vb = s_tr[e * nk + id + 1];
-        s_u[q] = (real)((va + (vb - va) * L.ft_frac[q]) * L.ft_w[q]);
+        s_u[j * nchan + ch] = (real)((va + (vb - va) * L.ft_frac[q]) * L.ft_w[q]);
     }
     __syncthreads();
     const int fmask = L.nfft - 1;
-    for (int o = tid; o < nchan * nwin; o += blockDim.x) {
-        int ch = o / nwin, q = o - ch * nwin;
-        int m = L.win_bin[q];
-        int idx = (int)(((long)L.ft_n0[ch] * m) & fmask), stp = m & fmask;
-        const real *u = s_u + (long)ch * ncoef;
-        real sr = 0, si = 0;
-        for (int j = 0; j < ncoef; ++j) {
-            real2 w = s_tw[idx];
-            real uj = u[j];
-            sr = fma(uj, w.x, sr);
-            si = fma(uj, w.y, si);
-            idx = (idx + stp) & fmask;
+    const int n0 = L.ft_n0[0];
+    const int nsplit = max(1, min(kMaxSplit, (int)blockDim.x / max(nwin, 1)));
+    const int jper = (ncoef + nsplit - 1) / nsplit;
+    const int nx = nchan * nwin;
+    for (int item = tid; item < nsplit * nwin; item += blockDim.x) {
+        int part = item / nwin, q = item - part * nwin;
+        int m = L.win_bin[q] & fmask;
+        int j0 = part * jper, j1 = min(ncoef, j0 + jper);
+        real ar[MAXCH], ai[MAXCH];
+#pragma unroll
+        for (int c = 0; c < MAXCH; ++c) ar[c] = ai[c] = 0;
+        const real inv_half = (real)2.0 / (real)L.nfft;
+        const real2 rot = twiddle(m, inv_half);
+        for (int jb = j0; jb < j1; jb += kReseed) {
+            real2 z = twiddle((int)(((long)(n0 + jb) * m) & fmask), inv_half);
+            int je = min(j1, jb + kReseed);
+            for (int j = jb; j < je; ++j) {
+                const real *uj = s_u + j * nchan;
+#pragma unroll
+                for (int c = 0; c < MAXCH; ++c)
+                    if (c < nchan) {
+                        real u = uj[c];
+                        ar[c] = fma(u, z.x, ar[c]);
+                        ai[c] = fma(u, z.y, ai[c]);
+                    }
+                real zx = z.x * rot.x - z.y * rot.y;
+                z.y = fma(z.x, rot.y, z.y * rot.x);
+                z.x = zx;
+            }
         }
-        s_x[o] = real2{(real)(sr * L.ft_norm), (real)(si * L.ft_norm)};
+#pragma unroll
+        for (int c = 0; c < MAXCH; ++c)
+            if (c < nchan) s_x[part * nx + c * nwin + q] = real2{ar[c], ai[c]};
+    }
+    __syncthreads();
+    for (int o = tid; o < nx; o += blockDim.x) {
+        real2 v = s_x[o];
+        for (int p = 1; p < nsplit; ++p) {
+            real2 w = s_x[p * nx + o];
+            v.x += w.x;
+            v.y += w.y;
+        }
+        s_x[o] = real2{(real)(v.x * L.ft_norm), (real)(v.y * L.ft_norm)};
     }
     __syncthreads();
 
-    // ---- 5. profiled chi^2
+    // profiled chi^2
     for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
         double nu = 0.0, dn = 0.0;
         for (int q = lane; q < nwin; q += 32) {
@@ -198,7 +260,6 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr,
         if (lane == 0) s_sq[ch] = acc;
     }
     __syncthreads();
-
     if (tid == 0) {
         double tot = 0.0;
         for (int ch = 0; ch < L.nchan; ++ch) tot += s_sq[ch];
@@ -207,22 +268,23 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr,
     __syncthreads();
 }
 
-template <int NSP, int PREC>
-__global__ void __launch_bounds__(kStepThreads) k_step(const chx_ladder_t *__restrict__ Ls,
-                                                      const int *__restrict__ slot_ladder,
-                                                      int nslots, StepSmem so,
-                                                      uint64_t *__restrict__ stepc,
-                                                      int *__restrict__ ticket,
-                                                      int *__restrict__ err) {
-    typedef typename std::conditional<PREC == CHX_FP64, double, float>::type real;
-    typedef typename std::conditional<PREC == CHX_FP64, double2, float2>::type real2;
+template <int NSP, int PREC, int NT>
+__global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladder_t *__restrict__ Ls,
+                                                         const int *__restrict__ slot_ladder,
+                                                         int nslots, int nsteps, StepSmem so,
+                                                         uint64_t *__restrict__ stepc,
+                                                         int *__restrict__ ticket,
+                                                         int *__restrict__ err) {
+    typedef typename Real<PREC>::T real;
+    typedef typename Real<PREC>::T2 real2;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ chx_ladder_t L;
     __shared__ Proposal prop;
-    __shared__ uint64_t s_step;
+    __shared__ uint64_t s_step, s_base;
     __shared__ int s_rung, s_ndir, s_ndn, s_nhist, s_acc;
-    __shared__ double s_num[32], s_den[32], s_sq[32], s_scale[8], s_de[kStepThreads / 32];
+    __shared__ double s_num[32], s_den[32], s_sq[32], s_scale[8], s_de[NT / 32];
     __shared__ double s_c2;
+    __shared__ int s_msb[NSP + 1];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int slot = blockIdx.x;
@@ -237,247 +299,308 @@ __global__ void __launch_bounds__(kStepThreads) k_step(const chx_ladder_t *__res
     const int maxaff = 4 * z;
     const int nent = L.ms_nblk ? NSP * L.ms_nblk : 0;
     const int ndn = L.nshell * nn;
-    const int *S = L.species + (long)c * natoms;
-    const double *P = L.pos + (long)c * natoms * 3;
-    const uint8_t *MV = L.moved + (long)c * natoms;
+    int *Sg = L.species + (long)c * natoms;
+    double *P = L.pos + (long)c * natoms * 3;
+    uint8_t *MVg = L.moved + (long)c * natoms;
 
-    real2 *s_tw = (real2 *)(smem + so.tw);
     real *s_u = (real *)(smem + so.u);
     real2 *s_x = (real2 *)(smem + so.x);
     double *s_tr = (double *)(smem + so.tr);
     double *s_dchi = (double *)(smem + so.dchi);
-    DirRec *s_dir = (DirRec *)(smem + so.dir);
+    PairRec *s_dir = (PairRec *)(smem + so.dir);
     int *s_dirv = (int *)(smem + so.dirv);
     int *s_hist = (int *)(smem + so.hist);
     int *s_dn = (int *)(smem + so.dn);
     int *s_list = (int *)(smem + so.list);
+    uint8_t *s_sp = (uint8_t *)(smem + so.sp);
+    auto spc = [s_sp](int i) { return (int)(s_sp[i] & 0x7F); };
 
-    // ---- 1. proposal (one thread) while the others stage the twiddles
     if (tid == 0) {
-        s_step = *(volatile uint64_t *)stepc + 1;
-        int rung = L.rung_of[c];
-        s_rung = rung;
-        prop = propose_one(S, P, L.ideal, natoms, L.seed, s_step, rung, L.swap_frac,
-                           L.disp_sigma, L.max_disp);
+        s_base = *(volatile uint64_t *)stepc;
+        s_rung = L.rung_of[c];
     }
-    for (int j = tid; j < L.nfft; j += blockDim.x) {
-        double2 t = ((const double2 *)L.tw64)[j];
-        s_tw[j] = real2{(real)t.x, (real)t.y};
-    }
-    for (int e = tid; e < nent; e += blockDim.x) s_hist[e] = 0;
-    for (int e = tid; e < ndn; e += blockDim.x) s_dn[e] = 0;
+    if (tid <= NSP) s_msb[tid] = 0;
+    for (int i = tid; i < natoms; i += blockDim.x)
+        s_sp[i] = (uint8_t)((Sg[i] & 0x7F) | (MVg[i] ? 0x80 : 0));
     __syncthreads();
-    const int a = prop.a, b = prop.b, nsa = prop.nsa, nsb = prop.nsb, swp = prop.swap;
-    const bool use_tab = (PREC != CHX_FP64) && L.sstab != nullptr;
+    const bool use_tab = (PREC != CHX_FP64) && L.sstab32 != nullptr;
+    const float *msT32 = L.ms_T32;
 
-    // ---- 2. affected pairs: old/new terms, table counts or direct records
-    double de = 0.0;
-    for (int q = tid; q < maxaff; q += blockDim.x) {
-        int blk = q / z, o = q - (q / z) * z;
-        int site = (blk < 2) ? a : b;
-        int p = site * z + o;
-        if (blk & 1) p = L.rev[p];
-        int i = -1, j = -1;
-        if ((unsigned)p < (unsigned)L.npairs) {
-            i = L.iidx[p];
-            j = L.jidx[p];
-        }
-        if ((unsigned)i >= (unsigned)natoms || (unsigned)j >= (unsigned)natoms) {
-            atomicOr(err, CHX_DEVERR_INDEX);
-            p = -1;
-        }
-        if (blk >= 2 && p >= 0 && (b == a || ((blk == 2) ? j : i) == a)) p = -1;
-        s_dirv[2 * q] = 0;
-        s_dirv[2 * q + 1] = 0;
-        if (p < 0) continue;
-        const double *sh3 = L.shift + 3 * (long)p;
-        const double *pi = P + 3 * (long)i, *pj = P + 3 * (long)j;
-        double dx = pj[0] + sh3[0] - pi[0], dy = pj[1] + sh3[1] - pi[1], dz = pj[2] + sh3[2] - pi[2];
-        double r_old = sqrt(dx * dx + dy * dy + dz * dz);
-        double r_new = r_old;
-        if (!swp) {  // a displacement: atom a moves to prop.np
-            const double *ni = (i == a) ? prop.np : pi, *nj = (j == a) ? prop.np : pj;
-            dx = nj[0] + sh3[0] - ni[0];
-            dy = nj[1] + sh3[1] - ni[1];
-            dz = nj[2] + sh3[2] - ni[2];
-            r_new = sqrt(dx * dx + dy * dy + dz * dz);
-        }
-        int si = S[i], sj = S[j];
-        int t_old = si * NSP + sj;
-        int ni_ = (i == a) ? nsa : ((i == b) ? nsb : si);
-        int nj_ = (j == a) ? nsa : ((j == b) ? nsb : sj);
-        int t_new = ni_ * NSP + nj_;
-        int sh = L.shell[p];
-        if (L.etab) de += L.etab[sh * nn + t_new] - L.etab[sh * nn + t_old];
-        bool tab_ok = use_tab && L.pair_tab[p] && !MV[i] && !MV[j];
-        bool tab_new = tab_ok && swp;  // a displaced atom leaves its site
-        double s2 = L.sig2[p];
-        auto make = [&](double r, int t, int neg) {
-            DirRec d;
-            double reff = r + L.drtab[sh * nn + t];
-            d.r.reff = reff;
-            d.r.s2 = s2 + L.s2tab[sh * nn + t];
-            d.r.c3 = L.c3tab[sh];
-            d.r.inv_r2 = (float)(1.0 / (reff * reff));
-            d.r.t = t;
-            d.neg = neg;
-            return d;
-        };
-        if (tab_ok) atomicSub(&s_dn[sh * nn + t_old], 1);
-        else { s_dir[2 * q] = make(r_old, t_old, 1); s_dirv[2 * q] = 1; }
-        if (tab_new) atomicAdd(&s_dn[sh * nn + t_new], 1);
-        else { s_dir[2 * q + 1] = make(r_new, t_new, 0); s_dirv[2 * q + 1] = 1; }
-    }
-    if (L.etab) {
-        de = warp_sum(de);
-        if (lane == 0) s_de[warp] = de;
-    }
-    // ---- MS entry changes along the paths through a and b
-    if (nent && swp) {
-        const int M = L.ms_M;
-        const int4 *inc = (const int4 *)L.ms_inc;
-        for (int m = tid; m < 2 * M; m += blockDim.x) {
-            int half = m >= M;
-            int site = half ? b : a;
-            int4 rc = __ldg(&inc[(long)site * M + (m - half * M)]);
-            if (rc.x < 0) continue;
-            if (half) {
-                int ab = rc.x & 0xFFFFF;
-                if (ab == a || rc.y == a || rc.z == a || rc.w == a) continue;
-            }
-            int eo = ms_entry_old(S, rc, L.ms_cls_off, NSP, L.ms_nblk);
-            int en = ms_entry_new(S, rc, L.ms_cls_off, NSP, L.ms_nblk, a, b, nsa, nsb);
-            if (eo != en) {
-                atomicAdd(&s_hist[en], 1);
-                atomicSub(&s_hist[eo], 1);
-            }
-        }
-    }
-    __syncthreads();
-    // compact: warp 0 the direct records, warp 1 the table counts, warp 2 the MS entries
-    int *l_dir = s_list, *l_dn = s_list + 2 * maxaff, *l_ms = l_dn + ndn;
-    if (warp == 0) {
-        int n = warp_compact(2 * maxaff, [&](int i) { return s_dirv[i] != 0; }, l_dir);
-        if (lane == 0) s_ndir = n;
-    } else if (warp == 1) {
-        int n = warp_compact(ndn, [&](int i) { return s_dn[i] != 0; }, l_dn);
-        if (lane == 0) s_ndn = n;
-    } else if (warp == 2) {
-        int n = (nent && swp) ? warp_compact(nent, [&](int i) { return s_hist[i] != 0; }, l_ms) : 0;
-        if (lane == 0) s_nhist = n;
-    }
-    __syncthreads();
-
-    // ---- 3. delta chi(k): thread per k
-    const int ndir = s_ndir, ndnz = s_ndn, nms = s_nhist;
-    const double *CH = L.chi + (long)c * NSP * nk;
-    const double *CNT = L.count + (long)c * NSP;
-    for (int ik = tid; ik < nk; ik += blockDim.x) {
-        double acc[NSP];
-#pragma unroll
-        for (int s = 0; s < NSP; ++s) acc[s] = 0.0;
-        if (ndir) {
-            KConst<NSP> kc;
-            load_kconst<NSP>(kc, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, ik);
-            for (int q = 0; q < ndir; ++q) {
-                const DirRec &d = s_dir[l_dir[q]];
-                double v = rec_term<NSP, PREC>(d.r, kc);
-                add_by_species<NSP>(acc, d.r.t / NSP, d.neg ? -v : v);
-            }
-        }
-        for (int q = 0; q < ndnz; ++q) {
-            int jt = l_dn[q];
-            add_by_species<NSP>(acc, (jt % nn) / NSP, (double)s_dn[jt] * L.sstab[(long)jt * nk + ik]);
-        }
-        for (int q = 0; q < nms; ++q) {
-            int e = l_ms[q];
-            add_by_species<NSP>(acc, e / L.ms_nblk, (double)s_hist[e] * L.ms_T[(long)e * nk + ik]);
-        }
-#pragma unroll
-        for (int s = 0; s < NSP; ++s) {
-            s_dchi[s * nk + ik] = acc[s];
-            double v = (CH[s * nk + ik] + acc[s]) / fmax(CNT[s], 1.0);
-            if (L.chi_extra) v += L.chi_extra[s * nk + ik];
-            s_tr[s * nk + ik] = v;
-        }
-    }
-    __syncthreads();
-
-    // ---- 4-5. trial chi(R) on the window and its profiled chi^2
-    ft_chi2<NSP, PREC>(L, s_tr, s_tw, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
-
-    // ---- 6. Metropolis
-    if (tid == 0) {
-        double c2 = s_c2;
-        int rung = s_rung;
-        double x = L.beta_rung[rung] * (c2 - L.chi2[c]) * L.nfit;
-        if (L.etab) {
-            double d = 0.0;
-            for (int w = 0; w < (int)(blockDim.x / 32); ++w) d += s_de[w];
-            x += L.energy_beta * d;
-        }
-        double u;
-        long ui = (long)(s_step - 1);
-        if (L.u_stream && ui < L.u_steps) {
-            u = L.u_stream[ui * L.nrep + rung];
-        } else {
-            if (L.u_stream) atomicOr(err, CHX_DEVERR_INDEX);
-            uint64_t h = splitmix64(splitmix64(L.seed ^ 0xD1B54A32D192ED03ULL) ^
-                                    (s_step * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)rung << 32));
-            u = u01(splitmix64(h));
-        }
-        int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
-        s_acc = acc;
-        L.acc_rung[rung] = (uint8_t)acc;
-    }
-    __syncthreads();
-
-    // ---- 7. commit
-    if (s_acc) {
-        int *Sw = L.species + (long)c * natoms;
-        double *Pw = L.pos + (long)c * natoms * 3;
-        double *CHw = L.chi + (long)c * NSP * nk;
-        for (int q = tid; q < NSP * nk; q += blockDim.x) CHw[q] += s_dchi[q];
-        if (nent && swp) {
-            int *C = L.ms_C + (long)c * nent;
-            for (int q = tid; q < nms; q += blockDim.x) C[l_ms[q]] += s_hist[l_ms[q]];
-        }
+    for (int st = 0; st < nsteps; ++st) {
+        // ---- 1. proposal (one thread)
         if (tid == 0) {
-            Sw[a] = nsa;
-            Sw[b] = nsb;
-            if (!swp) {
-                Pw[3 * a] = prop.np[0];
-                Pw[3 * a + 1] = prop.np[1];
-                Pw[3 * a + 2] = prop.np[2];
-                L.moved[(long)c * natoms + a] = 1;
+            s_step = s_base + st + 1;
+            prop = propose_one(spc, P, L.ideal, natoms, L.seed, s_step, s_rung, L.swap_frac,
+                               L.disp_sigma, L.max_disp);
+        }
+        for (int e = tid; e < nent; e += blockDim.x) s_hist[e] = 0;
+        for (int e = tid; e < ndn; e += blockDim.x) s_dn[e] = 0;
+        __syncthreads();
+        const int a = prop.a, b = prop.b, nsa = prop.nsa, nsb = prop.nsb, swp = prop.swap;
+
+        // ---- 2. affected pairs: old/new terms, table counts or direct records
+        double de = 0.0;
+        for (int q = tid; q < maxaff; q += blockDim.x) {
+            int blk = q / z, o = q - blk * z;
+            int site = (blk < 2) ? a : b;
+            int p = site * z + o;
+            if (blk & 1) p = L.rev[p];
+            int i = -1, j = -1;
+            if ((unsigned)p < (unsigned)L.npairs) {
+                i = (blk & 1) ? L.iidx[p] : site;
+                j = (blk & 1) ? site : L.jidx[p];
             }
-            L.chi2[c] = s_c2;
-            L.n_acc[c] += 1;
+            if ((unsigned)i >= (unsigned)natoms || (unsigned)j >= (unsigned)natoms) {
+                atomicOr(err, CHX_DEVERR_INDEX);
+                p = -1;
+            }
+            if (blk >= 2 && p >= 0 && (b == a || ((blk == 2) ? j : i) == a)) p = -1;
+            s_dirv[2 * q] = 0;
+            s_dirv[2 * q + 1] = 0;
+            if (p < 0) continue;
+            int si = spc(i), sj = spc(j);
+            int t_old = si * NSP + sj;
+            int ni_ = (i == a) ? nsa : ((i == b) ? nsb : si);
+            int nj_ = (j == a) ? nsa : ((j == b) ? nsb : sj);
+            int t_new = ni_ * NSP + nj_;
+            int sh = L.shell[p];
+            if (L.etab) de += L.etab[sh * nn + t_new] - L.etab[sh * nn + t_old];
+            bool tab_ok = use_tab && L.pair_tab[p] && !(s_sp[i] & 0x80) && !(s_sp[j] & 0x80);
+            bool tab_new = tab_ok && swp;  // a displaced atom leaves its site
+            if (tab_ok && tab_new) {
+                if (t_old != t_new) {
+                    atomicSub(&s_dn[sh * nn + t_old], 1);
+                    atomicAdd(&s_dn[sh * nn + t_new], 1);
+                }
+                continue;
+            }
+            const double *sh3 = L.shift + 3 * (long)p;
+            const double *pi = P + 3 * (long)i, *pj = P + 3 * (long)j;
+            double dx = pj[0] + sh3[0] - pi[0], dy = pj[1] + sh3[1] - pi[1],
+                   dz = pj[2] + sh3[2] - pi[2];
+            double r_old = sqrt(dx * dx + dy * dy + dz * dz);
+            double r_new = r_old;
+            if (!swp) {  // a displacement: atom a moves to prop.np
+                const double *ni = (i == a) ? prop.np : pi, *nj = (j == a) ? prop.np : pj;
+                dx = nj[0] + sh3[0] - ni[0];
+                dy = nj[1] + sh3[1] - ni[1];
+                dz = nj[2] + sh3[2] - ni[2];
+                r_new = sqrt(dx * dx + dy * dy + dz * dz);
+            }
+            double s2 = L.sig2[p];
+            auto make = [&](double r, int t, int neg) {  // sign kept in bit 16 of t
+                PairRec d;
+                double reff = r + L.drtab[sh * nn + t];
+                d.reff = reff;
+                d.s2 = s2 + L.s2tab[sh * nn + t];
+                d.c3 = L.c3tab[sh];
+                d.inv_r2 = (float)(1.0 / (reff * reff));
+                d.t = t | (neg << 16);
+                return d;
+            };
+            if (tab_ok) {
+                atomicSub(&s_dn[sh * nn + t_old], 1);
+            } else {
+                s_dir[2 * q] = make(r_old, t_old, 1);
+                s_dirv[2 * q] = 1;
+            }
+            s_dir[2 * q + 1] = make(r_new, t_new, 0);
+            s_dirv[2 * q + 1] = 1;
+        }
+        if (L.etab) {
+            de = warp_sum(de);
+            if (lane == 0) s_de[warp] = de;
+        }
+        // ---- MS entry changes along the paths through a and b
+        if (nent && swp) {
+            const int M = L.ms_M;
+            const int4 *inc = (const int4 *)L.ms_inc;
+            auto spn = [&](int site) {
+                return site == a ? nsa : (site == b ? nsb : (int)(s_sp[site] & 0x7F));
+            };
+#pragma unroll 4
+            for (int m = tid; m < 2 * M; m += blockDim.x) {
+                int half = m >= M;
+                int4 rc = __ldg(&inc[(long)(half ? b : a) * M + (m - half * M)]);
+                if (rc.x < 0) continue;
+                if (half) {
+                    int ab = rc.x & 0xFFFFF;
+                    if (ab == a || rc.y == a || rc.z == a || rc.w == a) continue;
+                }
+                int eo = ms_entry(spc, rc, NSP, L.ms_nblk);
+                int en = ms_entry(spn, rc, NSP, L.ms_nblk);
+                if (eo != en) {
+                    atomicAdd(&s_hist[en], 1);
+                    atomicSub(&s_hist[eo], 1);
+                }
+            }
         }
         __syncthreads();
-        if (s_c2 < L.best_chi2[c]) {
-            int *B = L.best_sp + (long)c * natoms;
-            double *BP = L.best_pos + (long)c * natoms * 3;
-            for (int q = tid; q < natoms; q += blockDim.x) B[q] = Sw[q];
-            for (int q = tid; q < 3 * natoms; q += blockDim.x) BP[q] = Pw[q];
-            __syncthreads();
-            if (tid == 0) L.best_chi2[c] = s_c2;
+        // compact: warp 0 the direct records, warp 1 the table counts, warp 2 the
+        // MS entries, as (index, count) pairs in ascending index order; the MS
+        // list is split into one run per absorber species (entry / nblk)
+        int *l_dir = s_list;
+        int2 *l_dn = (int2 *)(s_list + 2 * maxaff);
+        int2 *l_ms = l_dn + ndn;
+        if (warp == 0) {
+            int n = warp_compact(2 * maxaff, [&](int i) { return s_dirv[i] != 0; }, l_dir);
+            if (lane == 0) s_ndir = n;
+        } else if (warp == 1) {
+            int n = warp_compact_pairs(ndn, s_dn, l_dn);
+            if (lane == 0) s_ndn = n;
+        } else if (warp == 2) {
+            int n = (nent && swp) ? warp_compact_pairs(nent, s_hist, l_ms) : 0;
+            if (lane == 0) s_nhist = n;
+            // first list position of each absorber block
+            for (int a_ = lane; a_ <= NSP; a_ += 32) {
+                int lo = 0, hi = n, key = a_ * L.ms_nblk;
+                while (lo < hi) {
+                    int mid = (lo + hi) >> 1;
+                    if (l_ms[mid].x < key) lo = mid + 1;
+                    else hi = mid;
+                }
+                s_msb[a_] = lo;
+            }
         }
-    }
+        __syncthreads();
+
+        // ---- 3. delta chi(k): thread per k
+        const int ndir = s_ndir, ndnz = s_ndn, nms = s_nhist;
+        const double *CH = L.chi + (long)c * NSP * nk;
+        const double *CNT = L.count + (long)c * NSP;
+        for (int ik = tid; ik < nk; ik += blockDim.x) {
+            double acc[NSP];
+#pragma unroll
+            for (int s = 0; s < NSP; ++s) acc[s] = 0.0;
+            if (ndir) {
+                KConst<NSP> kc;
+                load_kconst<NSP>(kc, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, ik);
+                for (int q = 0; q < ndir; ++q) {
+                    PairRec d = s_dir[l_dir[q]];
+                    int neg = d.t >> 16;
+                    d.t &= 0xFFFF;
+                    double v = rec_term<NSP, PREC>(d, kc);
+                    add_by_species<NSP>(acc, d.t / NSP, neg ? -v : v);
+                }
+            }
+            if (use_tab) {
+#pragma unroll 4
+                for (int q = 0; q < ndnz; ++q) {
+                    int2 jc = l_dn[q];
+                    add_by_species<NSP>(acc, (jc.x % nn) / NSP,
+                                        (double)((float)jc.y *
+                                                 __ldg(&L.sstab32[(long)jc.x * nk + ik])));
+                }
+            }
+            // MS rows, one run per absorber block: independent loads, no divides
+#pragma unroll
+            for (int a_ = 0; a_ < NSP; ++a_) {
+                const int q0 = s_msb[a_], q1 = s_msb[a_ + 1];
+                if (PREC == CHX_FP64 || msT32 == nullptr) {
+                    double sa = 0.0;
+#pragma unroll 8
+                    for (int q = q0; q < q1; ++q) {
+                        int2 ec = l_ms[q];
+                        sa = fma((double)ec.y, __ldg(&L.ms_T[(long)ec.x * nk + ik]), sa);
+                    }
+                    acc[a_] += sa;
+                } else {
+                    float sa = 0.f;
+#pragma unroll 8
+                    for (int q = q0; q < q1; ++q) {
+                        int2 ec = l_ms[q];
+                        sa = fmaf((float)ec.y, __ldg(&msT32[(long)ec.x * nk + ik]), sa);
+                    }
+                    acc[a_] += (double)sa;
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < NSP; ++s) {
+                s_dchi[s * nk + ik] = acc[s];
+                double v = (CH[s * nk + ik] + acc[s]) / fmax(CNT[s], 1.0);
+                if (L.chi_extra) v += L.chi_extra[s * nk + ik];
+                s_tr[s * nk + ik] = v;
+            }
+        }
+        __syncthreads();
+
+        // ---- 4-5. trial chi(R) on the window and its profiled chi^2
+        ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
+
+        // ---- 6. Metropolis
+        if (tid == 0) {
+            double c2 = s_c2;
+            int rung = s_rung;
+            double x = L.beta_rung[rung] * (c2 - L.chi2[c]) * L.nfit;
+            if (L.etab) {
+                double d = 0.0;
+                for (int w = 0; w < (int)(blockDim.x / 32); ++w) d += s_de[w];
+                x += L.energy_beta * d;
+            }
+            double u;
+            long ui = (long)(s_step - 1);
+            if (L.u_stream && ui < L.u_steps) {
+                u = L.u_stream[ui * L.nrep + rung];
+            } else {
+                if (L.u_stream) atomicOr(err, CHX_DEVERR_INDEX);
+                uint64_t h = splitmix64(splitmix64(L.seed ^ 0xD1B54A32D192ED03ULL) ^
+                                        (s_step * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)rung << 32));
+                u = u01(splitmix64(h));
+            }
+            int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
+            s_acc = acc;
+            L.acc_rung[rung] = (uint8_t)acc;
+            if (L.acc_log) L.acc_log[(long)st * L.nrep + rung] = (uint8_t)acc;
+        }
+        __syncthreads();
+
+        // ---- 7. commit
+        if (s_acc) {
+            double *CHw = L.chi + (long)c * NSP * nk;
+            for (int q = tid; q < NSP * nk; q += blockDim.x) CHw[q] += s_dchi[q];
+            if (nent && swp) {
+                int *C = L.ms_C + (long)c * nent;
+                for (int q = tid; q < nms; q += blockDim.x) C[l_ms[q].x] += l_ms[q].y;
+            }
+            if (tid == 0) {
+                s_sp[a] = (uint8_t)((s_sp[a] & 0x80) | nsa);
+                s_sp[b] = (uint8_t)((s_sp[b] & 0x80) | nsb);
+                Sg[a] = nsa;
+                Sg[b] = nsb;
+                if (!swp) {
+                    P[3 * a] = prop.np[0];
+                    P[3 * a + 1] = prop.np[1];
+                    P[3 * a + 2] = prop.np[2];
+                    s_sp[a] |= 0x80;
+                    MVg[a] = 1;
+                }
+                L.chi2[c] = s_c2;
+                L.n_acc[c] += 1;
+            }
+            __syncthreads();
+            if (s_c2 < L.best_chi2[c]) {
+                int *B = L.best_sp + (long)c * natoms;
+                double *BP = L.best_pos + (long)c * natoms * 3;
+                for (int q = tid; q < natoms; q += blockDim.x) B[q] = s_sp[q] & 0x7F;
+                for (int q = tid; q < 3 * natoms; q += blockDim.x) BP[q] = P[q];
+                __syncthreads();
+                if (tid == 0) L.best_chi2[c] = s_c2;
+            }
+        }
+        __syncthreads();
+    }  // steps
 
     // ---- the last CTA of the launch advances the step counter
-    __syncthreads();
     if (tid == 0) {
         __threadfence();
         int t = atomicAdd(ticket, 1);
         if (t == nslots - 1) {
             *ticket = 0;
-            *(volatile uint64_t *)stepc = s_step;
+            *(volatile uint64_t *)stepc = s_base + nsteps;
             __threadfence();
         }
     }
 }
-
 
 // chi^2 of each slot's chi (or of chi_in, same layout) without a move: the
 // state's initial and end-of-run chi^2 (method_a_rmc.py:180, 437, 448).
@@ -488,8 +611,8 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
                                                            const double *__restrict__ chi_in,
                                                            const double *__restrict__ count_in,
                                                            double *__restrict__ out) {
-    typedef typename std::conditional<PREC == CHX_FP64, double, float>::type real;
-    typedef typename std::conditional<PREC == CHX_FP64, double2, float2>::type real2;
+    typedef typename Real<PREC>::T real;
+    typedef typename Real<PREC>::T2 real2;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ chx_ladder_t L;
     __shared__ double s_num[32], s_den[32], s_sq[32], s_scale[8], s_c2;
@@ -501,14 +624,9 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
     }
     __syncthreads();
     const int c = slot - L.slot0, nk = L.nk;
-    real2 *s_tw = (real2 *)(smem + so.tw);
     real *s_u = (real *)(smem + so.u);
     real2 *s_x = (real2 *)(smem + so.x);
     double *s_tr = (double *)(smem + so.tr);
-    for (int j = tid; j < L.nfft; j += blockDim.x) {
-        double2 t = ((const double2 *)L.tw64)[j];
-        s_tw[j] = real2{(real)t.x, (real)t.y};
-    }
     const double *CH = chi_in ? chi_in + (long)slot * NSP * nk : L.chi + (long)c * NSP * nk;
     const double *CNT = count_in ? count_in + (long)slot * NSP : L.count + (long)c * NSP;
     for (int q = tid; q < NSP * nk; q += blockDim.x) {
@@ -517,7 +635,7 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
         s_tr[q] = v;
     }
     __syncthreads();
-    ft_chi2<NSP, PREC>(L, s_tr, s_tw, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
+    ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
     if (tid == 0) out[slot] = s_c2;
 }
 
@@ -531,7 +649,8 @@ __global__ void k_exchange(const chx_ladder_t *__restrict__ Ls, int nladders,
     if (li >= nladders) return;
     uint64_t round = *(volatile const uint64_t *)round_key;
     const chx_ladder_t &L = Ls[li];
-    uint64_t h = splitmix64(splitmix64(L.seed ^ 0x5851F42D4C957F2DULL) ^ (round * 0x9E3779B97F4A7C15ULL));
+    uint64_t h = splitmix64(splitmix64(L.seed ^ 0x5851F42D4C957F2DULL) ^
+                            (round * 0x9E3779B97F4A7C15ULL));
     h = splitmix64(h);
     int start = (u01(h) < 0.5) ? 0 : 1;
     for (int i = start; i < L.nrep - 1; i += 2) {
@@ -583,6 +702,85 @@ __global__ void k_shell_table(chx_ladder_t L, const double *__restrict__ rshell,
     }
 }
 
+template <int NSP, int PREC, int NT>
+static int launch_step_nt(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
+                          int nsteps, const StepSmem &so, size_t smem, uint64_t *d_stepc,
+                          int *d_ticket, int *d_err, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(k_step<NSP, PREC, NT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "sampler_step attribute");
+    k_step<NSP, PREC, NT><<<nslots, NT, smem, st>>>(d_ladders, slot_ladder, nslots, nsteps, so,
+                                                    d_stepc, d_ticket, d_err);
+    CHX_CHECK_LAUNCH("sampler_step");
+    return CHX_OK;
+}
+
+template <int NSP, int PREC>
+static int launch_step(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
+                       int nsteps, int threads, const StepSmem &so, size_t smem,
+                       uint64_t *d_stepc, int *d_ticket, int *d_err, cudaStream_t st) {
+    if (threads == 128)
+        return launch_step_nt<NSP, PREC, 128>(d_ladders, slot_ladder, nslots, nsteps, so, smem,
+                                              d_stepc, d_ticket, d_err, st);
+    return launch_step_nt<NSP, PREC, 256>(d_ladders, slot_ladder, nslots, nsteps, so, smem,
+                                          d_stepc, d_ticket, d_err, st);
+}
+
+template <int NSP, int PREC>
+static int launch_eval(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
+                       const StepSmem &so, size_t smem, const double *chi_in,
+                       const double *count_in, double *out, cudaStream_t st) {
+    cudaError_t e = cudaFuncSetAttribute(k_eval_chi2<NSP, PREC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "eval_chi2 attribute");
+    k_eval_chi2<NSP, PREC><<<nslots, kStepThreads, smem, st>>>(d_ladders, slot_ladder, so,
+                                                               chi_in, count_in, out);
+    CHX_CHECK_LAUNCH("eval_chi2");
+    return CHX_OK;
+}
+
+// One carve-up for all ladders of a launch: the largest extent of each field.
+static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, StepSmem *out,
+                        size_t *bytes) {
+    int nsp = H[0].nsp;
+    StepSmem mx{};
+    for (int i = 0; i < nladders; ++i) {
+        const chx_ladder_t &L = H[i];
+        CHX_REQUIRE(L.nsp == nsp, "sampler: one launch needs one species count");
+        CHX_REQUIRE(L.ncoord > 0 && L.ncoord <= kMaxCoord && L.nk > 0 && L.nkw >= 1 &&
+                        L.nkw <= 3 && L.nchan == L.nsp * L.nkw && (L.nfft & (L.nfft - 1)) == 0 &&
+                        L.natoms < (1 << 20) && L.nwin > 0,
+                    "sampler: ladder %d outside the built limits", i);
+        StepSmem s = step_smem(L, precision);
+        // field sizes of this ladder, then the running maximum of each
+        // field sizes of this ladder, then the running maximum of each
+        size_t f[10] = {s.x - s.u, s.tr - s.x, s.dchi - s.tr, s.dir - s.dchi, s.dirv - s.dir,
+                        s.hist - s.dirv, s.dn - s.hist, s.list - s.dn, s.sp - s.list,
+                        s.total - s.sp};
+        size_t *g[10] = {&mx.u, &mx.x, &mx.tr, &mx.dchi, &mx.dir, &mx.dirv, &mx.hist, &mx.dn,
+                         &mx.list, &mx.sp};
+        for (int q = 0; q < 10; ++q) *g[q] = std::max(*g[q], f[q]);
+    }
+    // mx holds field sizes; turn them into offsets
+    StepSmem o;
+    size_t at = 0;
+    o.u = at; at += mx.u;
+    o.x = at; at += mx.x;
+    o.tr = at; at += mx.tr;
+    o.dchi = at; at += mx.dchi;
+    o.dir = at; at += mx.dir;
+    o.dirv = at; at += mx.dirv;
+    o.hist = at; at += mx.hist;
+    o.dn = at; at += mx.dn;
+    o.list = at; at += mx.list;
+    o.sp = at; at += mx.sp;
+    o.total = at;
+    CHX_REQUIRE(at <= 220 * 1024, "sampler: %zu bytes of shared memory needed", at);
+    *out = o;
+    *bytes = at;
+    return CHX_OK;
+}
+
 }  // namespace chx
 
 using namespace chx;
@@ -591,9 +789,10 @@ extern "C" {
 
 int chx_sampler_smem_bytes(const chx_ladder_t *host_ladders, int nladders, int precision) {
     if (!host_ladders || nladders <= 0) return CHX_ERR_ARG;
-    size_t m = 0;
-    for (int i = 0; i < nladders; ++i) m = std::max(m, step_smem(host_ladders[i], precision).total);
-    return (int)m;
+    StepSmem so;
+    size_t bytes = 0;
+    int rc = plan_ladders(host_ladders, nladders, precision, &so, &bytes);
+    return rc == CHX_OK ? (int)bytes : rc;
 }
 
 int chx_shell_table(const chx_ladder_t *L, const double *rshell, const double *s2shell,
@@ -612,63 +811,39 @@ int chx_shell_table(const chx_ladder_t *L, const double *rshell, const double *s
 }
 
 int chx_sampler_step(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
-                     int nladders, const int *slot_ladder, int nslots, int precision,
-                     uint64_t *d_stepc, int *d_ticket, int *d_err, void *stream) {
+                     int nladders, const int *slot_ladder, int nslots, int precision, int nsteps,
+                     int threads, uint64_t *d_stepc, int *d_ticket, int *d_err, void *stream) {
     CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && d_stepc && d_ticket && d_err &&
-                    nladders > 0 && nslots > 0,
+                    nladders > 0 && nslots > 0 && nsteps > 0,
                 "sampler_step: bad arguments");
     CHX_REQUIRE(precision == CHX_FP64 || precision == CHX_FP32C, "sampler_step: bad precision");
-    int nsp = host_ladders[0].nsp;
+    CHX_REQUIRE(threads == 0 || threads == 128 || threads == 256,
+                "sampler_step: threads must be 128 or 256");
+    StepSmem so;
     size_t smem = 0;
-    StepSmem so{};
-    for (int i = 0; i < nladders; ++i) {
-        const chx_ladder_t &L = host_ladders[i];
-        CHX_REQUIRE(L.nsp == nsp, "sampler_step: one launch needs one species count");
-        CHX_REQUIRE(L.ncoord > 0 && L.ncoord <= kMaxCoord && L.nk > 0 && L.nchan <= 32 &&
-                        L.nchan == L.nsp * L.nkw && (L.nfft & (L.nfft - 1)) == 0 &&
-                        L.natoms < (1 << 20),
-                    "sampler_step: ladder %d outside the built limits", i);
-        StepSmem s = step_smem(L, precision);
-        if (s.total > smem) {
-            smem = s.total;
-            so = s;
-        }
-    }
-    // every ladder must share one carve-up: lay out for the largest of each field
-    for (int i = 0; i < nladders; ++i) {
-        StepSmem s = step_smem(host_ladders[i], precision);
-        CHX_REQUIRE(s.tw <= so.tw && s.u <= so.u && s.x <= so.x && s.tr <= so.tr &&
-                        s.dchi <= so.dchi && s.dir <= so.dir && s.hist <= so.hist &&
-                        s.dn <= so.dn && s.list <= so.list,
-                    "sampler_step: ladders of one launch need matching shapes");
-    }
-    CHX_REQUIRE(smem <= 220 * 1024, "sampler_step: %zu bytes of shared memory needed", smem);
+    int rc = plan_ladders(host_ladders, nladders, precision, &so, &smem);
+    if (rc != CHX_OK) return rc;
     cudaStream_t st = as_stream(stream);
-#define CHX_STEP(N, PR)                                                                         \
-    do {                                                                                        \
-        cudaFuncSetAttribute(k_step<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
-                             (int)smem);                                                        \
-        k_step<N, PR><<<nslots, kStepThreads, smem, st>>>(d_ladders, slot_ladder, nslots, so,    \
-                                                          d_stepc, d_ticket, d_err);            \
-    } while (0)
+    int nsp = host_ladders[0].nsp;
+#define CHX_STEP(N, PR) \
+    launch_step<N, PR>(d_ladders, slot_ladder, nslots, nsteps, threads, so, smem, d_stepc, \
+                       d_ticket, d_err, st)
     if (precision == CHX_FP64) {
         switch (nsp) {
-            case 2: CHX_STEP(2, CHX_FP64); break;
-            case 3: CHX_STEP(3, CHX_FP64); break;
-            case 4: CHX_STEP(4, CHX_FP64); break;
-            default: set_error("sampler_step: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+            case 2: return CHX_STEP(2, CHX_FP64);
+            case 3: return CHX_STEP(3, CHX_FP64);
+            case 4: return CHX_STEP(4, CHX_FP64);
         }
     } else {
         switch (nsp) {
-            case 2: CHX_STEP(2, CHX_FP32C); break;
-            case 3: CHX_STEP(3, CHX_FP32C); break;
-            case 4: CHX_STEP(4, CHX_FP32C); break;
-            default: set_error("sampler_step: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+            case 2: return CHX_STEP(2, CHX_FP32C);
+            case 3: return CHX_STEP(3, CHX_FP32C);
+            case 4: return CHX_STEP(4, CHX_FP32C);
         }
     }
 #undef CHX_STEP
-    CHX_CHECK_LAUNCH("sampler_step");
-    return CHX_OK;
+    set_error("sampler_step: nsp %d not built", nsp);
+    return CHX_ERR_UNSUPPORTED;
 }
 
 int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders, int nladders,
@@ -676,39 +851,29 @@ int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladder
                   const double *count_in, double *out, void *stream) {
     CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && out && nladders > 0 && nslots > 0,
                 "eval_chi2: bad arguments");
-    int nsp = host_ladders[0].nsp;
-    StepSmem so{};
+    StepSmem so;
     size_t smem = 0;
-    for (int i = 0; i < nladders; ++i) {
-        StepSmem s = step_smem(host_ladders[i], precision);
-        if (s.total > smem) { smem = s.total; so = s; }
-    }
+    int rc = plan_ladders(host_ladders, nladders, precision, &so, &smem);
+    if (rc != CHX_OK) return rc;
     cudaStream_t st = as_stream(stream);
-#define CHX_EV(N, PR)                                                                          \
-    do {                                                                                       \
-        cudaFuncSetAttribute(k_eval_chi2<N, PR>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
-                             (int)smem);                                                       \
-        k_eval_chi2<N, PR><<<nslots, kStepThreads, smem, st>>>(d_ladders, slot_ladder, so,      \
-                                                               chi_in, count_in, out);         \
-    } while (0)
+    int nsp = host_ladders[0].nsp;
+#define CHX_EV(N, PR) launch_eval<N, PR>(d_ladders, slot_ladder, nslots, so, smem, chi_in, count_in, out, st)
     if (precision == CHX_FP64) {
         switch (nsp) {
-            case 2: CHX_EV(2, CHX_FP64); break;
-            case 3: CHX_EV(3, CHX_FP64); break;
-            case 4: CHX_EV(4, CHX_FP64); break;
-            default: set_error("eval_chi2: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+            case 2: return CHX_EV(2, CHX_FP64);
+            case 3: return CHX_EV(3, CHX_FP64);
+            case 4: return CHX_EV(4, CHX_FP64);
         }
     } else {
         switch (nsp) {
-            case 2: CHX_EV(2, CHX_FP32C); break;
-            case 3: CHX_EV(3, CHX_FP32C); break;
-            case 4: CHX_EV(4, CHX_FP32C); break;
-            default: set_error("eval_chi2: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+            case 2: return CHX_EV(2, CHX_FP32C);
+            case 3: return CHX_EV(3, CHX_FP32C);
+            case 4: return CHX_EV(4, CHX_FP32C);
         }
     }
 #undef CHX_EV
-    CHX_CHECK_LAUNCH("eval_chi2");
-    return CHX_OK;
+    set_error("eval_chi2: nsp %d not built", nsp);
+    return CHX_ERR_UNSUPPORTED;
 }
 
 int chx_replica_exchange(const chx_ladder_t *d_ladders, int nladders, const uint64_t *round_key,

@@ -21,8 +21,8 @@ reference uses, from its own enumeration:
     with slot 0 fastest (mslibrary.py:190-198, 275).
   * `SupercellPaths` places every image at every site of a periodic fcc/bcc/sc
     supercell (mslibrary.py:357-404) and packs, per site, the records of the
-    paths through it {absorber | class << 20, slot0, slot1, slot2} that the
-    device kernels stream.
+    paths through it {absorber | class entry offset << 20, slot0, slot1,
+    slot2} that the device kernels stream.
 
 The per-entry spectra come from a path library on the model's k grid; with
 no FEFF library available, `synthetic_table` defines a smooth seeded one.
@@ -246,7 +246,7 @@ class SupercellPaths:
         inc[site, np.arange(site.size) - start[site]] = pid
         self.inc = inc.astype(np.int32)
         self.records = np.empty((self.npath, 4), np.int32)
-        self.records[:, 0] = self.p_abs | (self.p_cls << 20)
+        self.records[:, 0] = self.p_abs | (self.cls_off[self.p_cls] << 20)
         self.records[:, 1:] = self.p_slot
         pad = np.full((1, 4), -1, np.int32)
         self.inc_rec = np.concatenate([self.records, pad])[self.inc]
@@ -254,8 +254,7 @@ class SupercellPaths:
     def device(self):
         """Device copies of the records, incidence records and offsets."""
         if not hasattr(self, "_dev"):
-            self._dev = dict(records=N.to_dev(self.records), inc_rec=N.to_dev(self.inc_rec),
-                             cls_off=N.to_dev(self.cls_off))
+            self._dev = dict(records=N.to_dev(self.records), inc_rec=N.to_dev(self.inc_rec))
         return self._dev
 
 
@@ -290,7 +289,7 @@ class SupercellMS:
         d = self.paths.device()
         out = torch.empty((nrep, self.nent), dtype=torch.int32, device="cuda")
         N.call("chx_ms_counts", N.ptr(sp), nrep, self.natoms, N.ptr(d["records"]), self.npath,
-               N.ptr(d["cls_off"]), self.nsp, self.nblk, N.ptr(out), N.stream())
+               self.nsp, self.nblk, N.ptr(out), N.stream())
         return out
 
     def chi_of(self, C):
@@ -317,7 +316,6 @@ class SupercellMS:
         args = [torch.as_tensor(x).to("cuda", torch.int32).contiguous() for x in (a, b, nsa, nsb)]
         dC = torch.empty((nrep, self.nent), dtype=torch.int32, device="cuda")
         N.call("chx_ms_delta", N.ptr(sp), nrep, self.natoms, N.ptr(d["inc_rec"]), self.M,
-               N.ptr(d["cls_off"]), self.nsp, self.nblk, *[N.ptr(x) for x in args], N.ptr(dC),
-               N.stream())
+               self.nsp, self.nblk, *[N.ptr(x) for x in args], N.ptr(dC), N.stream())
         self._dC = dC
         return self.chi_of(dC)

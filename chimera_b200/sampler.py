@@ -32,6 +32,7 @@ from . import _native as N
 from .forward import FP64, FP32C
 
 KB_EV = 8.617333262e-5
+MAX_BLOCK = 256          # steps per launch at most (rows of the accept log)
 
 
 def _host(x):
@@ -53,31 +54,31 @@ def _ft_setup(ft, nsp):
     assert nkw * nsp == len(fts), f"{len(fts)} channels do not divide into {nsp} edges"
     assert np.array_equal(chan_edge, np.repeat(np.arange(nsp), nkw)), \
         "channels must be ordered edge-major"
-    rows = []
+    # every channel's non-zero taps, placed on one shared run of the uniform
+    # grid [n0, n0 + ncoef) (zero weight outside a channel's own window)
+    spans = []
     for f in fts:
-        idx, frac = _host(f._idx), _host(f._frac)
         wt = _host(f._w) * _host(f._inside)
         nz = np.nonzero(wt)[0]
-        n0, n1 = (int(nz[0]), int(nz[-1]) + 1) if nz.size else (0, 1)
-        rows.append((n0, idx[n0:n1].astype(np.int32), frac[n0:n1], wt[n0:n1]))
-    ncoef = max(r[1].size for r in rows)
-    n0 = np.array([r[0] for r in rows], np.int32)
-    I = np.zeros((len(rows), ncoef), np.int32)
-    F = np.zeros((len(rows), ncoef))
-    W = np.zeros((len(rows), ncoef))
-    for c, (_, i, fr, w) in enumerate(rows):
-        I[c, :i.size], F[c, :i.size], W[c, :i.size] = i, fr, w
+        spans.append((int(nz[0]), int(nz[-1]) + 1) if nz.size else (0, 1))
+    n0u = min(a for a, _ in spans)
+    ncoef = max(b for _, b in spans) - n0u
+    I = np.zeros((len(fts), ncoef), np.int32)
+    F = np.zeros((len(fts), ncoef))
+    W = np.zeros((len(fts), ncoef))
+    for c, f in enumerate(fts):
+        idx, frac = _host(f._idx), _host(f._frac)
+        wt = _host(f._w) * _host(f._inside)
+        a, b = spans[c]
+        I[c, a - n0u:b - n0u] = idx[a:b]
+        F[c, a - n0u:b - n0u] = frac[a:b]
+        W[c, a - n0u:b - n0u] = wt[a:b]
+    n0 = np.full(len(fts), n0u, np.int32)
     nfft = int(fts[0].nfft)
     norm = float(fts[0]._norm)
     extra = getattr(ft, "chi_extra", None)
     return dict(nchan=len(fts), nkw=nkw, n0=n0, idx=I, frac=F, w=W, ncoef=ncoef, nfft=nfft,
                 norm=norm, extra=None if extra is None else _host(extra))
-
-
-def _twiddles(nfft):
-    j = np.arange(nfft)
-    ang = 2.0 * np.pi * j / nfft
-    return np.ascontiguousarray(np.stack([np.cos(ang), -np.sin(ang)], axis=1))
 
 
 class LadderSpec:
@@ -100,9 +101,10 @@ class LadderSpec:
 class Ladders:
     """Device state and descriptors of a batch of ladders (see module doc)."""
 
-    def __init__(self, specs, precision=FP64, use_table=True):
+    def __init__(self, specs, precision=FP64, use_table=True, threads=256):
         import torch
         N.require_cuda()
+        self.threads = int(threads)
         self.torch = torch
         self.specs = list(specs)
         self.precision = int(precision)
@@ -176,18 +178,26 @@ class Ladders:
             rs, ss = self._t(r_shell), self._t(s2_shell)
             N.call("chx_shell_table", C.byref(L), N.ptr(rs), N.ptr(ss), N.ptr(b["sstab"]),
                    N.stream())
+            b["sstab32"] = b["sstab"].float().contiguous()
+            self.keep.append(b["sstab32"])
+            L.sstab32 = N.dptr(b["sstab32"])
         else:
-            L.sstab = 0
+            L.sstab, L.sstab32 = 0, 0
         # exact multiple scattering
         ms = s.ms
         if ms is not None:
             d = ms.paths.device()
             L.ms_nblk, L.ms_M = ms.nblk, ms.M
-            L.ms_inc, L.ms_cls_off, L.ms_T = (N.dptr(d["inc_rec"]), N.dptr(d["cls_off"]),
-                                              N.dptr(ms.T))
-            self.keep += [d["inc_rec"], d["cls_off"], ms.T]
+            L.ms_inc, L.ms_T = N.dptr(d["inc_rec"]), N.dptr(ms.T)
+            self.keep += [d["inc_rec"], ms.T]
+            if self.precision != FP64:
+                b["msT32"] = ms.T.float().contiguous()
+                self.keep.append(b["msT32"])
+                L.ms_T32 = N.dptr(b["msT32"])
+            else:
+                L.ms_T32 = 0
         else:
-            L.ms_nblk, L.ms_M, L.ms_inc, L.ms_cls_off, L.ms_T = 0, 0, 0, 0, 0
+            L.ms_nblk, L.ms_M, L.ms_inc, L.ms_T, L.ms_T32 = 0, 0, 0, 0, 0
         # pair-interaction prior (method_a_rmc.py:147-157)
         if s.energy_prior is not None:
             V, T_ann = s.energy_prior
@@ -207,7 +217,7 @@ class Ladders:
         tm = np.ascontiguousarray(s.target[:, s.mask])
         sm = np.ascontiguousarray(s.sigma_R[:, s.mask], np.float64)
         b.update(ft_n0=self._t(f["n0"]), ft_idx=self._t(f["idx"]), ft_frac=self._t(f["frac"]),
-                 ft_w=self._t(f["w"]), win=self._t(win), tw=self._t(_twiddles(f["nfft"])),
+                 ft_w=self._t(f["w"]), win=self._t(win),
                  tm_re=self._t(np.ascontiguousarray(tm.real, np.float64)),
                  tm_im=self._t(np.ascontiguousarray(tm.imag if cplx else np.zeros(tm.shape),
                                                     np.float64)),
@@ -218,7 +228,7 @@ class Ladders:
                                                   f["nfft"], f["ncoef"])
         L.ft_n0, L.ft_idx, L.ft_frac, L.ft_w = (N.dptr(b["ft_n0"]), N.dptr(b["ft_idx"]),
                                                 N.dptr(b["ft_frac"]), N.dptr(b["ft_w"]))
-        L.win_bin, L.tw64, L.ft_norm = N.dptr(b["win"]), N.dptr(b["tw"]), f["norm"]
+        L.win_bin, L.ft_norm = N.dptr(b["win"]), f["norm"]
         L.chi_extra = N.dptr(b.get("extra"))
         L.tm_re, L.tm_im, L.sm = N.dptr(b["tm_re"]), N.dptr(b["tm_im"]), N.dptr(b["sm"])
         L.cplx, L.profile = int(cplx), int(s.profile_scale)
@@ -241,11 +251,13 @@ class Ladders:
                  rung_of=z32(nrep), slot_of=z32(nrep), best_chi2=f64(nrep),
                  best_sp=z32(nrep, natoms), best_pos=f64(nrep, natoms, 3),
                  ms_C=z32(nrep, ms.nent if ms is not None else 1),
-                 acc=torch.zeros(nrep, dtype=torch.uint8, device="cuda"), n_acc=z32(nrep),
+                 acc=torch.zeros(nrep, dtype=torch.uint8, device="cuda"),
+                 acc_log=torch.zeros((MAX_BLOCK, nrep), dtype=torch.uint8, device="cuda"),
+                 n_acc=z32(nrep),
                  exch_att=z32(max(nrep, 1)), exch_acc=z32(max(nrep, 1)))
         for key in ("species", "pos", "moved", "chi", "chi2", "count", "rung_of", "slot_of",
-                    "best_chi2", "best_sp", "best_pos", "ms_C", "acc", "n_acc", "exch_att",
-                    "exch_acc"):
+                    "best_chi2", "best_sp", "best_pos", "ms_C", "acc", "acc_log", "n_acc",
+                    "exch_att", "exch_acc"):
             self.keep.append(b[key])
         L.species, L.pos, L.moved, L.chi = (N.dptr(b["species"]), N.dptr(b["pos"]),
                                             N.dptr(b["moved"]), N.dptr(b["chi"]))
@@ -254,6 +266,7 @@ class Ladders:
         L.best_chi2, L.best_sp, L.best_pos = (N.dptr(b["best_chi2"]), N.dptr(b["best_sp"]),
                                               N.dptr(b["best_pos"]))
         L.ms_C, L.acc_rung, L.n_acc = N.dptr(b["ms_C"]), N.dptr(b["acc"]), N.dptr(b["n_acc"])
+        L.acc_log = N.dptr(b["acc_log"])
         L.exch_att, L.exch_acc = N.dptr(b["exch_att"]), N.dptr(b["exch_acc"])
         b["beta_host"] = beta
         b["cplx"] = cplx
@@ -330,10 +343,13 @@ class Ladders:
         self.refresh_chi2()
 
     # --------------------------------------------------------------- steps
-    def step(self):
+    def step(self, nsteps=1):
+        """nsteps steps of every slot in one launch (nsteps <= MAX_BLOCK)."""
+        assert 0 < nsteps <= MAX_BLOCK
         N.call("chx_sampler_step", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
-               N.ptr(self.slot_ladder), self.nslots, self.precision, N.ptr(self.stepc),
-               N.ptr(self.ticket), N.ptr(self.err), N.stream())
+               N.ptr(self.slot_ladder), self.nslots, self.precision, int(nsteps),
+               self.threads, N.ptr(self.stepc), N.ptr(self.ticket), N.ptr(self.err),
+               N.stream())
 
     def exchange_device(self):
         N.call("chx_replica_exchange", N.ptr(self.d_ladders), self.nladders, N.ptr(self.stepc),
@@ -442,8 +458,15 @@ class RMCSampler:
         """One proposal per rung; returns the accept flags by rung (device)."""
         self._stepc += 1
         self._ensure_uniforms(self._stepc)
-        self.lad.step()
+        self.lad.step(1)
         return self.b["acc"].bool()
+
+    def steps(self, n):
+        """n proposals per rung in one launch; accept flags (n, nrep) by rung."""
+        self._stepc += n
+        self._ensure_uniforms(self._stepc)
+        self.lad.step(n)
+        return self.b["acc_log"][:n]
 
     def replica_exchange(self, return_rates=False):
         """Host-decided exchange on the reference's PCG64 stream
@@ -491,38 +514,58 @@ class RMCSampler:
 
     # ------------------------------------------------------------- loop
     def run(self, nsteps, exchange_every=25, log_every=500, callback=None):
-        """Run the chain (method_a_rmc.py:401-455)."""
+        """Run the chain (method_a_rmc.py:401-455). Steps between two host
+        events (exchange, adaptation, collection, log) go in one launch."""
         import torch
         hist = []
         acc_run = torch.zeros((), dtype=torch.float64, device="cuda")
         self._ensure_uniforms(self._stepc + nsteps)
         t0 = time.time()
         win_acc, win_exch = [], []
-        for it in range(nsteps):
-            acc = self.step()
-            acc_run += acc.double().mean()
+
+        def next_mult(it, every):
+            return (it // every + 1) * every
+
+        it = 0
+        while it < nsteps:
+            nxt = min(nsteps, it + MAX_BLOCK)
+            for every in (exchange_every, self.adapt_every, log_every):
+                if every:
+                    nxt = min(nxt, next_mult(it, every))
+            if it == 0:
+                nxt = min(nxt, 1)
+            if self.collect_after is not None:
+                t = max(next_mult(it, self.collect_every), 0)
+                while t - 1 < self.collect_after:
+                    t += self.collect_every
+                nxt = min(nxt, t)
+            n = nxt - it
+            flags = self.steps(n).double()
+            per_step = flags.mean(dim=1)
+            acc_run += per_step.sum()
             if self.adapt_every:
-                win_acc.append(acc.double().mean())
-            if exchange_every and (it + 1) % exchange_every == 0:
+                win_acc.extend(per_step.unbind(0))
+            it = nxt
+            if exchange_every and it % exchange_every == 0:
                 if self.reproduce:
                     _, per_pair = self.replica_exchange(return_rates=True)
                     if self.adapt_every:
                         win_exch.append(per_pair)
                 else:
                     self.lad.exchange_device()
-            if self.adapt_every and (it + 1) % self.adapt_every == 0:
+            if self.adapt_every and it % self.adapt_every == 0:
                 wa = float(torch.stack(win_acc).mean()) if win_acc else None
                 we = np.mean(win_exch, axis=0) if win_exch else None
                 self.adapt(wa, we)
                 win_acc, win_exch = [], []
-            if (self.collect_after is not None and it >= self.collect_after
-                    and (it + 1) % self.collect_every == 0):
+            if (self.collect_after is not None and it - 1 >= self.collect_after
+                    and it % self.collect_every == 0):
                 self._collect()
-            if (it + 1) % log_every == 0 or it == 0:
+            if it % log_every == 0 or it == 1:
                 best = float(self.best_chi2.min())
-                hist.append((it + 1, best, float(acc_run) / (it + 1), time.time() - t0))
+                hist.append((it, best, float(acc_run) / it, time.time() - t0))
                 if callback:
-                    callback(it + 1, best, hist[-1][2])
+                    callback(it, best, hist[-1][2])
         if not self.reproduce:
             att = _host(self.b["exch_att"])[:self.nrep - 1]
             acc_ = _host(self.b["exch_acc"])[:self.nrep - 1]
@@ -588,10 +631,10 @@ class BatchedSampler:
     accepted moves (checked every `check_every` blocks)."""
 
     def __init__(self, specs, precision=FP32C, exchange_every=25, use_table=True,
-                 reanchor_every=1000, check_every=40):
+                 reanchor_every=1000, check_every=40, threads=256):
         import torch
         self.torch = torch
-        self.lad = Ladders(specs, precision=precision, use_table=use_table)
+        self.lad = Ladders(specs, precision=precision, use_table=use_table, threads=threads)
         self.exchange_every = int(exchange_every)
         self.reanchor_every = int(reanchor_every)
         self.check_every = int(check_every)
@@ -613,9 +656,9 @@ class BatchedSampler:
         self.lad.refresh_chi2(reset_best=True)
 
     def block(self):
-        """One exchange period: exchange_every steps, then the exchange."""
-        for _ in range(self.exchange_every):
-            self.lad.step()
+        """One exchange period: exchange_every steps in one launch, then the
+        device exchange."""
+        self.lad.step(self.exchange_every)
         self.lad.exchange_device()
 
     def capture(self):

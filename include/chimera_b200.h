@@ -149,21 +149,21 @@ CHX_API int chx_chi_full(const chx_pairs_t *P, const double *pos, const int *spe
  * 3. Exact supercell multiple scattering (A2): entry counts of every
  *    configuration (chimera/mslibrary.py:436-451) and chi_MS = counts @ table
  *    per absorber block (mslibrary.py:453-457).
- *    A path record is 4 int32: {absorber | class << 20, slot0, slot1, slot2},
- *    slots -1 when unused; entry = s_abs*nblk + cls_off[class] + sum_q s_q nsp^q
- *    (mslibrary.py:190-198, 433-434).
+ *    A path record is 4 int32: {absorber | entry_offset << 20, slot0, slot1,
+ *    slot2}, slots -1 when unused, entry_offset the first library entry of
+ *    the path's class (mslibrary.py:275); the path's entry is then
+ *    s_abs*nblk + entry_offset + sum_q s_q nsp^q (mslibrary.py:190-198, 433-434).
  * ------------------------------------------------------------------------ */
 CHX_API int chx_ms_counts(const int *species, int nconf, int natoms, const int *paths,
-                  int64_t npath, const int *cls_off, int nsp, int nblk, int *counts,
-                  void *stream);
+                          int64_t npath, int nsp, int nblk, int *counts, void *stream);
 /* Entry-count change of each replica's proposal (swap a <-> b to species nsa,
  * nsb; a == b for a displacement, which changes nothing): paths through a and
  * through b, a path through both counted once (mslibrary.py:466-486).
  * inc (natoms, M, 4) holds the records of the paths incident on each site
  * (padding rows -1); dC (nrep, nsp*nblk). */
 CHX_API int chx_ms_delta(const int *species, int nrep, int natoms, const int *inc, int M,
-                         const int *cls_off, int nsp, int nblk, const int *a, const int *b,
-                         const int *nsa, const int *nsb, int *dC, void *stream);
+                         int nsp, int nblk, const int *a, const int *b, const int *nsa,
+                         const int *nsb, int *dC, void *stream);
 /* chi (nconf, nsp, nk) += counts (nconf, nsp*nblk) @ T (nsp*nblk, nk), per block */
 CHX_API int chx_ms_chi_of(const int *counts, const double *T, int nconf, int nsp, int nblk,
                   int nk, double *chi, void *stream);
@@ -194,23 +194,24 @@ typedef struct {
     const double *ftab, *dtab, *lamtab, *ktab, *drtab, *c3tab, *s2tab;
     double s02;
     const double *sstab;             /* (nshell*nsp*nsp, nk) ideal-shell terms, or NULL */
+    const float *sstab32;            /* the same table in FP32 (CHX_FP32C), or NULL    */
     /* exact multiple scattering, ms_nblk == 0 when off */
     int ms_nblk, ms_M;
     const int *ms_inc;               /* (natoms, ms_M, 4) records incident on a site */
-    const int *ms_cls_off;
     const double *ms_T;              /* (nsp*ms_nblk, nk)                         */
+    const float *ms_T32;             /* the same table in FP32 (CHX_FP32C), or NULL */
     /* pair-interaction prior, etab NULL when off (method_a_rmc.py:147-157,310-320) */
     const double *etab;              /* (nshell*nsp*nsp) eV per directed pair     */
     double energy_beta;
     /* transform (one channel per (edge, k weight), edge-major) and target */
     int nchan, nkw, nwin, nfft, ncoef;
-    const int *ft_n0;                /* (nchan) first uniform-grid index          */
+    const int *ft_n0;                /* (nchan) first uniform-grid index, one value
+                                        for every channel (coefficients share taps) */
     const int *ft_idx;               /* (nchan, ncoef) resample index             */
     const double *ft_frac;           /* (nchan, ncoef) resample fraction          */
     const double *ft_w;              /* (nchan, ncoef) inside * window * k^w      */
     const int *win_bin;              /* (nwin) R bins of the fit window           */
     const double *chi_extra;         /* (nsp, nk) added before the transform, or NULL */
-    const double *tw64;              /* (nfft, 2) cos, -sin of 2 pi j / nfft      */
     double ft_norm;
     const double *tm_re, *tm_im, *sm;/* (nchan, nwin) target window and sigma     */
     int cplx, profile;
@@ -237,6 +238,8 @@ typedef struct {
     double *best_pos;                /* (nrep, natoms, 3)                         */
     int *ms_C;                       /* (nrep, nsp*ms_nblk) entry counts          */
     uint8_t *acc_rung;               /* (nrep) accept flag of the last step, by rung */
+    uint8_t *acc_log;                /* (steps, nrep) accept flags of every step of a
+                                        launch, by rung, or NULL                     */
     int *n_acc;                      /* (nrep) accepted moves per slot            */
     int *exch_att, *exch_acc;        /* (nrep) exchange bookkeeping per rung pair */
 } chx_ladder_t;
@@ -250,13 +253,17 @@ CHX_API int chx_sampler_smem_bytes(const chx_ladder_t *host_ladders, int nladder
 CHX_API int chx_shell_table(const chx_ladder_t *L, const double *rshell, const double *s2shell,
                     double *sstab, void *stream);
 
-/* One sampler step for every slot. d_ladders: device array of nladders
- * descriptors; slot_ladder (nslots): ladder of each slot. d_stepc: device
- * counter, read as the step number (the reference's `_stepc`, first step = 1)
- * and advanced by one when the step completes. d_err: device error word. */
+/* nsteps sampler steps of every slot in one launch (replicas are independent
+ * between exchanges, so one CTA runs all steps of its replica). d_ladders:
+ * device array of nladders descriptors; slot_ladder (nslots): ladder of each
+ * slot. d_stepc: device counter; step s of the launch is step *d_stepc + s + 1
+ * (the reference's `_stepc`, first step = 1), and the counter advances by
+ * nsteps when the launch completes. threads: CTA size, 128 or 256 (0 picks
+ * 256). d_err: device error word. */
 CHX_API int chx_sampler_step(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
-                     int nladders, const int *slot_ladder, int nslots, int precision,
-                     uint64_t *d_stepc, int *d_ticket, int *d_err, void *stream);
+                             int nladders, const int *slot_ladder, int nslots, int precision,
+                             int nsteps, int threads, uint64_t *d_stepc, int *d_ticket,
+                             int *d_err, void *stream);
 
 /* chi^2 of every slot's state chi (chi_in NULL) or of chi_in (nslots, nsp, nk)
  * with absorber counts count_in (nslots, nsp) (count NULL: the state's), by

@@ -62,7 +62,7 @@ def test_supercell_paths_and_oracle_counts(classes, nsp):
     assert digest(P_abs, P_cls, P_slot, sp.inc) == str(g[key + "digest"])
     # device records are the same paths, packed
     assert np.array_equal(sp.records[:, 0] & 0xFFFFF, sp.p_abs)
-    assert np.array_equal(sp.records[:, 0] >> 20, sp.p_cls)
+    assert np.array_equal(sp.records[:, 0] >> 20, sp.cls_off[sp.p_cls])
     assert np.array_equal(sp.inc_rec[5, :, 1:], np.vstack([sp.p_slot, -np.ones((1, 3))])[sp.inc[5]])
     C = K.ms_counts(g[key + "species"], sp.p_abs, sp.p_cls, sp.p_slot, sp.cls_off, nsp, sp.nblk)
     assert np.array_equal(C, g[key + "counts"])
