@@ -80,6 +80,8 @@ _SIGS = {
     "chx_commit_state": ([c_p] * 9 + [c_i, c_i, c_p], c_i),
     "chx_chi_full_scratch_bytes": ([c_p, c_i], c_i64),
     "chx_chi_full": ([c_p, c_p, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),
+    "chx_chi_full_noalloc_max_bytes": ([], c_i64),
+    "chx_chi_full_noalloc": ([c_p, c_p, c_p, c_i, c_i, c_p, c_p], c_i),
     "chx_ms_counts": ([c_p, c_i, c_i, c_p, c_i64, c_i, c_i, c_p, c_p], c_i),
     "chx_ms_delta": ([c_p, c_i, c_i, c_p, c_i, c_i, c_i, c_p, c_p, c_p, c_p, c_p, c_p], c_i),
     "chx_eval_chi2": ([c_p, c_p, c_i, c_p, c_i, c_i, c_p, c_p, c_p, c_p], c_i),

@@ -145,6 +145,21 @@ CHX_API int chx_chi_full(const chx_pairs_t *P, const double *pos, const int *spe
                  int precision, double *chi, void *scratch, int64_t scratch_bytes,
                  void *stream);
 
+/* The same path sum for callers that cannot allocate device memory (a host
+ * that reaches this library through a foreign-function interface with no
+ * device allocator of its own, or code running where allocating is not
+ * allowed). No counterpart in the reference: it exists only in this library.
+ * The scratch lives in a fixed device array of chx_chi_full_noalloc_max_bytes()
+ * bytes (32 MiB) that the library reserves on every GPU that loads it until
+ * the process exits; the call allocates nothing. Requests needing more
+ * scratch than that are rejected with CHX_ERR_SCRATCH. The first call on a
+ * device looks up the array's device address (and may load the module), so
+ * make it before any stream capture. All calls on a device share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+CHX_API int64_t chx_chi_full_noalloc_max_bytes(void);
+CHX_API int chx_chi_full_noalloc(const chx_pairs_t *P, const double *pos, const int *species,
+                                 int nconf, int precision, double *chi, void *stream);
+
 /* ------------------------------------------------------------------------
  * 3. Exact supercell multiple scattering (A2): entry counts of every
  *    configuration (chimera/mslibrary.py:436-451) and chi_MS = counts @ table
