@@ -115,3 +115,32 @@ def test_reference_kernels_match_oracle(cuda):
     K.commit_state(acc, o["a"], o["b"], o["nsa"], o["nsb"], npa_o, isw_o, sp, pos, natoms, nrep)
     assert np.array_equal(gsp.cpu().numpy(), sp)
     assert np.allclose(gp.cpu().numpy(), pos, rtol=0, atol=1e-14)
+
+
+def test_kernels_get_forwards_reference_argument_tuples(cuda):
+    """chimera_b200.kernels.get(name, nsp) takes the reference's call form."""
+    torch = cuda
+    from chimera_b200 import kernels as KK
+    d = trace_inputs("rmc_trace_disp.npz")
+    nsp = d["nsp"]
+    natoms = d["ideal"].shape[0]
+    npairs = d["i"].size
+    nrep = 2
+    rng = np.random.default_rng(5)
+    pos = np.repeat(d["ideal"][None], nrep, 0) + rng.normal(0, 0.01, (nrep, natoms, 3))
+    sp = np.stack([rng.permutation(d["species0"]) for _ in range(nrep)]).astype(np.int32)
+    r = torch.empty((nrep, npairs), dtype=torch.float64, device="cuda")
+    ev = torch.empty((nrep, npairs, 3), dtype=torch.float64, device="cuda")
+    KK.get("compute_r", nsp)((1,), (256,), (_dev(torch, pos), _dev(torch, d["i"]),
+                                            _dev(torch, d["j"]), _dev(torch, d["shift"]), r, ev,
+                                            np.int32(npairs), np.int32(natoms), np.int32(nrep)))
+    r_o = np.zeros((nrep, npairs))
+    K.compute_r(pos, d["i"], d["j"], d["shift"], r_o, None, npairs, natoms, nrep)
+    assert np.allclose(r.cpu().numpy(), r_o, rtol=1e-15, atol=0)
+    pt = torch.empty((nrep, npairs), dtype=torch.int32, device="cuda")
+    KK.get("build_ptype", nsp)((1,), (256,), (_dev(torch, sp), _dev(torch, d["i"]),
+                                              _dev(torch, d["j"]), pt, np.int32(npairs),
+                                              np.int32(natoms), np.int32(nrep)))
+    pt_o = np.zeros((nrep, npairs), np.int32)
+    K.build_ptype(sp, d["i"], d["j"], pt_o, npairs, natoms, nrep, nsp)
+    assert np.array_equal(pt.cpu().numpy(), pt_o)
