@@ -267,6 +267,7 @@ def main():
     rng = np.random.default_rng(rank)
     sp0 = [prob.random_config(int(rng.integers(1 << 30))) for _ in range(NPOS)]
     smp.init_state(sp0, prob.cell.ideal)
+    tuning = smp.autotune()
     smp.capture()
     smp.run_blocks(max(3, args.warmup))
     torch.cuda.synchronize()
@@ -313,6 +314,7 @@ def main():
     t0 = time.perf_counter()
     if not args.no_e2e:
         smp2 = make_sampler(prob, rank)
+        smp2.lad.threads, smp2.lad.min_blocks = smp.lad.threads, smp.lad.min_blocks
         smp2.init_state(sp0, prob.cell.ideal)
         smp2.run_blocks(e2e_blocks)
     else:
@@ -350,6 +352,7 @@ def main():
             "clocks": clocks,
             "device_error": err,
             "reanchors": smp.reanchors,
+            "autotune": tuning,
             "best_chi2_min": min(b[1] for b in best),
         }
         print(json.dumps(line), flush=True)

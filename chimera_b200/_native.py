@@ -48,13 +48,15 @@ class Ladder(C.Structure):
         ("sig2", c_p), ("pair_tab", c_p), ("ideal", c_p),
         ("ftab", c_p), ("dtab", c_p), ("lamtab", c_p), ("ktab", c_p), ("drtab", c_p),
         ("c3tab", c_p), ("s2tab", c_p), ("s02", c_d), ("sstab", c_p), ("sstab32", c_p),
-        ("ms_nblk", c_i), ("ms_M", c_i), ("ms_inc", c_p), ("ms_T", c_p),
+        ("ms_nblk", c_i), ("ms_M", c_i), ("ms_D", c_i), ("ms_tpl", c_p), ("ms_nbr", c_p),
+        ("ms_T", c_p),
         ("ms_T32", c_p),
         ("etab", c_p), ("energy_beta", c_d),
         ("nchan", c_i), ("nkw", c_i), ("nwin", c_i), ("nfft", c_i), ("ncoef", c_i),
         ("ft_n0", c_p), ("ft_idx", c_p), ("ft_frac", c_p), ("ft_w", c_p), ("win_bin", c_p),
         ("chi_extra", c_p), ("ft_norm", c_d),
-        ("tm_re", c_p), ("tm_im", c_p), ("sm", c_p), ("cplx", c_i), ("profile", c_i),
+        ("tm_re", c_p), ("tm_im", c_p), ("sm", c_p), ("w2", c_p), ("tnorm", c_p),
+        ("cplx", c_i), ("profile", c_i),
         ("nfit", c_d),
         ("seed", c_u64), ("swap_frac", c_d), ("disp_sigma", c_d), ("max_disp", c_d),
         ("nrep", c_i), ("slot0", c_i), ("beta_rung", c_p), ("u_stream", c_p),
@@ -88,7 +90,7 @@ _SIGS = {
     "chx_ms_chi_of": ([c_p, c_p, c_i, c_i, c_i, c_i, c_p, c_p], c_i),
     "chx_sampler_smem_bytes": ([c_p, c_i, c_i], c_i),
     "chx_shell_table": ([c_p, c_p, c_p, c_p, c_p], c_i),
-    "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
+    "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
     "chx_replica_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_apply_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_ft_batch": ([c_p, c_i, c_i, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),

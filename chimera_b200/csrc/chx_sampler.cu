@@ -42,7 +42,7 @@ constexpr int kMaxSplit = 2;     // threads sharing one bin's taps
 
 // Shared-memory carve-up of one step CTA (all offsets 16-byte aligned).
 struct StepSmem {
-    size_t u, x, tr, dchi, dir, dirv, hist, dn, list, sp, total;
+    size_t u, x, tr, dchi, dir, dirv, hist, dn, list, sp, nb, chi, total;
 };
 
 template <typename T>
@@ -66,6 +66,8 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     s.dn = o; o += al16<int>((size_t)std::max(ndn, 1));
     s.list = o; o += al16<int>((size_t)(2 * maxaff + 2 * ndn + 2 * nent + 64));
     s.sp = o; o += al16<uint8_t>((size_t)L.natoms);
+    s.nb = o; o += al16<uint16_t>((size_t)2 * std::max(L.ms_D, 1));
+    s.chi = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.total = o;
     return s;
 }
@@ -136,17 +138,18 @@ __device__ __forceinline__ double2 twiddle(int j, double inv_half) {
     return make_double2(c, -s);
 }
 
-// Steps 4-5 (and the whole of k_eval_chi2): resample x window x k^w the
-// normalised trial chi s_tr (nsp, nk) into s_u [tap][channel], transform it
-// on the window bins, and reduce the profiled chi^2 into *s_c2.
+// Resample x window x k^w the normalised trial chi s_tr (nsp, nk) into s_u
+// [tap][channel] and transform it on the window bins into s_x (channel-major).
+// Kept out of line so that its tap loop has the register file to itself: the
+// caller keeps many values live across the call.
 template <int NSP, int PREC>
-__device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real<PREC>::T *s_u,
-                        typename Real<PREC>::T2 *s_x, double *s_num, double *s_den,
-                        double *s_sq, double *s_scale, double *s_c2) {
+__device__ __noinline__ void ft_window(const chx_ladder_t &L, const double *s_tr,
+                                       typename Real<PREC>::T *s_u,
+                                       typename Real<PREC>::T2 *s_x) {
     typedef typename Real<PREC>::T real;
     typedef typename Real<PREC>::T2 real2;
     constexpr int MAXCH = 3 * NSP;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int nk = L.nk;
     const int nchan = L.nchan, ncoef = L.ncoef, nwin = L.nwin, nkw = L.nkw;
     for (int q = tid; q < nchan * ncoef; q += blockDim.x) {
@@ -202,8 +205,79 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real
         s_x[o] = real2{(real)(v.x * L.ft_norm), (real)(v.y * L.ft_norm)};
     }
     __syncthreads();
+}
 
-    // profiled chi^2
+// Steps 4-5 (and the whole of k_eval_chi2): trial chi(R) on the window bins
+// (ft_window), then the profiled chi^2 into *s_c2.
+template <int NSP, int PREC>
+__device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real<PREC>::T *s_u,
+                        typename Real<PREC>::T2 *s_x, double *s_num, double *s_den,
+                        double *s_sq, double *s_scale, double *s_c2) {
+    typedef typename Real<PREC>::T real;
+    typedef typename Real<PREC>::T2 real2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nchan = L.nchan, nwin = L.nwin, nkw = L.nkw;
+    ft_window<NSP, PREC>(L, s_tr, s_u, s_x);
+
+    if constexpr (PREC != CHX_FP64) {
+        // one pass: per channel num = Re<m,t>, den = <m,m> (the profiled scale)
+        // and A = <m,m>/s^2, B = Re<m,t>/s^2, C = <t,t>/s^2, so that
+        // sum |s m - t|^2 / s^2 = s^2 A - 2 s B + C (sums in FP64)
+        for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
+            double nu = 0.0, dn = 0.0, A = 0.0, B = 0.0, Cc = 0.0;
+            for (int q = lane; q < nwin; q += 32) {
+                real2 m = s_x[ch * nwin + q];
+                long g = (long)ch * nwin + q;
+                double tr = L.tm_re[g], ti = L.cplx ? L.tm_im[g] : 0.0;
+                double w = L.w2[g];
+                double mr = m.x, mi = m.y;
+                if (!L.cplx) {
+                    mr = sqrt(mr * mr + mi * mi);
+                    mi = 0.0;
+                }
+                double mt = mr * tr + mi * ti, mm = mr * mr + mi * mi;
+                nu += mt;
+                dn += mm;
+                A += mm * w;
+                B += mt * w;
+            }
+            nu = warp_sum(nu);
+            dn = warp_sum(dn);
+            A = warp_sum(A);
+            B = warp_sum(B);
+            Cc = L.tnorm[ch];
+            if (lane == 0) {
+                s_num[ch] = nu;
+                s_den[ch] = dn;
+                s_sq[ch] = A;
+                s_sq[12 + ch] = B;
+                s_sq[24 + ch] = Cc;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double tot = 0.0;
+            for (int e = 0; e < NSP; ++e) {
+                double s = 1.0;
+                if (L.profile) {
+                    double nu = 0.0, dn = 0.0;
+                    for (int q = 0; q < nkw; ++q) {
+                        nu += s_num[e * nkw + q];
+                        dn += s_den[e * nkw + q];
+                    }
+                    s = nu / fmax(dn, 1e-30);
+                }
+                for (int q = 0; q < nkw; ++q) {
+                    int ch = e * nkw + q;
+                    tot += s * s * s_sq[ch] - 2.0 * s * s_sq[12 + ch] + s_sq[24 + ch];
+                }
+            }
+            *s_c2 = tot / L.nfit;
+        }
+        __syncthreads();
+        return;
+    }
+    // profiled chi^2, the reference's two passes (FP64)
     for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
         double nu = 0.0, dn = 0.0;
         for (int q = lane; q < nwin; q += 32) {
@@ -268,8 +342,8 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real
     __syncthreads();
 }
 
-template <int NSP, int PREC, int NT>
-__global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladder_t *__restrict__ Ls,
+template <int NSP, int PREC, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restrict__ Ls,
                                                          const int *__restrict__ slot_ladder,
                                                          int nslots, int nsteps, StepSmem so,
                                                          uint64_t *__restrict__ stepc,
@@ -282,7 +356,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
     __shared__ Proposal prop;
     __shared__ uint64_t s_step, s_base;
     __shared__ int s_rung, s_ndir, s_ndn, s_nhist, s_acc;
-    __shared__ double s_num[32], s_den[32], s_sq[32], s_scale[8], s_de[NT / 32];
+    __shared__ double s_num[32], s_den[32], s_sq[40], s_scale[8], s_de[NT / 32];
     __shared__ double s_c2;
     __shared__ int s_msb[NSP + 1];
 
@@ -313,6 +387,8 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
     int *s_dn = (int *)(smem + so.dn);
     int *s_list = (int *)(smem + so.list);
     uint8_t *s_sp = (uint8_t *)(smem + so.sp);
+    uint16_t *s_nb = (uint16_t *)(smem + so.nb);
+    double *s_chi = (double *)(smem + so.chi);
     auto spc = [s_sp](int i) { return (int)(s_sp[i] & 0x7F); };
 
     if (tid == 0) {
@@ -322,6 +398,8 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
     if (tid <= NSP) s_msb[tid] = 0;
     for (int i = tid; i < natoms; i += blockDim.x)
         s_sp[i] = (uint8_t)((Sg[i] & 0x7F) | (MVg[i] ? 0x80 : 0));
+    double *CHg = L.chi + (long)c * NSP * nk;
+    for (int q = tid; q < NSP * nk; q += blockDim.x) s_chi[q] = CHg[q];
     __syncthreads();
     const bool use_tab = (PREC != CHX_FP64) && L.sstab32 != nullptr;
     const float *msT32 = L.ms_T32;
@@ -338,26 +416,28 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
         __syncthreads();
         const int a = prop.a, b = prop.b, nsa = prop.nsa, nsb = prop.nsb, swp = prop.swap;
 
-        // ---- 2. affected pairs: old/new terms, table counts or direct records
+        // ---- 2. affected pairs: old/new terms, table counts or direct records.
+        // Pair q of block blk is site -> neighbour (even blocks) or
+        // neighbour -> site (odd blocks), site = a (blocks 0, 1) or b (2, 3).
+        // In FP32C a reverse pair takes its shell, sigma^2 and geometry from the
+        // forward pair (the same bond); FP64 reads the reverse pair's own data.
+        const int sa_old = spc(a), sb_old = spc(b);
         double de = 0.0;
         for (int q = tid; q < maxaff; q += blockDim.x) {
             int blk = q / z, o = q - blk * z;
             int site = (blk < 2) ? a : b;
-            int p = site * z + o;
-            if (blk & 1) p = L.rev[p];
-            int i = -1, j = -1;
-            if ((unsigned)p < (unsigned)L.npairs) {
-                i = (blk & 1) ? L.iidx[p] : site;
-                j = (blk & 1) ? site : L.jidx[p];
-            }
-            if ((unsigned)i >= (unsigned)natoms || (unsigned)j >= (unsigned)natoms) {
-                atomicOr(err, CHX_DEVERR_INDEX);
-                p = -1;
-            }
-            if (blk >= 2 && p >= 0 && (b == a || ((blk == 2) ? j : i) == a)) p = -1;
+            int pf = site * z + o;
+            int jn = L.jidx[pf];
+            int p = pf;
+            if (PREC == CHX_FP64 && (blk & 1)) p = L.rev[pf];
             s_dirv[2 * q] = 0;
             s_dirv[2 * q + 1] = 0;
-            if (p < 0) continue;
+            if ((unsigned)jn >= (unsigned)natoms || (unsigned)p >= (unsigned)L.npairs) {
+                atomicOr(err, CHX_DEVERR_INDEX);
+                continue;
+            }
+            if (blk >= 2 && (b == a || jn == a)) continue;
+            const int i = (blk & 1) ? jn : site, j = (blk & 1) ? site : jn;
             int si = spc(i), sj = spc(j);
             int t_old = si * NSP + sj;
             int ni_ = (i == a) ? nsa : ((i == b) ? nsb : si);
@@ -374,14 +454,16 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
                 }
                 continue;
             }
+            // distance of the pair p = (pi -> pj + shift) before and after the move
+            const int pi_ = (PREC == CHX_FP64) ? i : site, pj_ = (PREC == CHX_FP64) ? j : jn;
             const double *sh3 = L.shift + 3 * (long)p;
-            const double *pi = P + 3 * (long)i, *pj = P + 3 * (long)j;
+            const double *pi = P + 3 * (long)pi_, *pj = P + 3 * (long)pj_;
             double dx = pj[0] + sh3[0] - pi[0], dy = pj[1] + sh3[1] - pi[1],
                    dz = pj[2] + sh3[2] - pi[2];
             double r_old = sqrt(dx * dx + dy * dy + dz * dz);
             double r_new = r_old;
             if (!swp) {  // a displacement: atom a moves to prop.np
-                const double *ni = (i == a) ? prop.np : pi, *nj = (j == a) ? prop.np : pj;
+                const double *ni = (pi_ == a) ? prop.np : pi, *nj = (pj_ == a) ? prop.np : pj;
                 dx = nj[0] + sh3[0] - ni[0];
                 dy = nj[1] + sh3[1] - ni[1];
                 dz = nj[2] + sh3[2] - ni[2];
@@ -411,24 +493,50 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
             de = warp_sum(de);
             if (lane == 0) s_de[warp] = de;
         }
-        // ---- MS entry changes along the paths through a and b
-        if (nent && swp) {
-            const int M = L.ms_M;
-            const int4 *inc = (const int4 *)L.ms_inc;
-            auto spn = [&](int site) {
-                return site == a ? nsa : (site == b ? nsb : (int)(s_sp[site] & 0x7F));
-            };
+        // ---- MS entry changes along the paths through a and b: the species of
+        // each site's neighbourhood (old | new << 8 | 0x8000 for site a), then
+        // the shared path templates
+        const bool do_ms = nent && swp;
+        if (do_ms) {
+            const int D = L.ms_D;
+            for (int d = tid; d < 2 * D; d += blockDim.x) {
+                int half = d >= D;
+                int site = __ldg(&L.ms_nbr[(long)(half ? b : a) * D + (d - half * D)]);
+                int so = s_sp[site] & 0x7F;
+                int sn = site == a ? nsa : (site == b ? nsb : so);
+                s_nb[d] = (uint16_t)(so | (sn << 8) | (site == a ? 0x8000 : 0));
+            }
+        }
+        __syncthreads();
+        if (do_ms) {
+            const int M = L.ms_M, D = L.ms_D, nblk = L.ms_nblk;
+            const uint2 *tpl = (const uint2 *)L.ms_tpl;
 #pragma unroll 4
             for (int m = tid; m < 2 * M; m += blockDim.x) {
-                int half = m >= M;
-                int4 rc = __ldg(&inc[(long)(half ? b : a) * M + (m - half * M)]);
-                if (rc.x < 0) continue;
-                if (half) {
-                    int ab = rc.x & 0xFFFFF;
-                    if (ab == a || rc.y == a || rc.z == a || rc.w == a) continue;
+                const int half = m >= M;
+                const uint2 t = __ldg(&tpl[m - half * M]);
+                const uint16_t *nb = s_nb + half * D;
+                const int so_self = half ? sb_old : sa_old, sn_self = half ? nsb : nsa;
+                int eo = (int)t.x, en = (int)t.x, hasa = 0;
+#pragma unroll
+                for (int pp = 0; pp < 4; ++pp) {
+                    const int v = (t.y >> (8 * pp)) & 0xFF;
+                    const int mul = pp == 0 ? nblk : (pp == 1 ? 1 : (pp == 2 ? NSP : NSP * NSP));
+                    if (v == 0xFF) continue;
+                    int so_, sn_;
+                    if (v == 0xFE) {
+                        so_ = so_self;
+                        sn_ = sn_self;
+                    } else {
+                        const int w = nb[v];
+                        so_ = w & 0x7F;
+                        sn_ = (w >> 8) & 0x7F;
+                        hasa |= w & 0x8000;
+                    }
+                    eo += so_ * mul;
+                    en += sn_ * mul;
                 }
-                int eo = ms_entry(spc, rc, NSP, L.ms_nblk);
-                int en = ms_entry(spn, rc, NSP, L.ms_nblk);
+                if (half && hasa) continue;     // a path through both sites counts once
                 if (eo != en) {
                     atomicAdd(&s_hist[en], 1);
                     atomicSub(&s_hist[eo], 1);
@@ -466,7 +574,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
 
         // ---- 3. delta chi(k): thread per k
         const int ndir = s_ndir, ndnz = s_ndn, nms = s_nhist;
-        const double *CH = L.chi + (long)c * NSP * nk;
+        const double *CH = s_chi;
         const double *CNT = L.count + (long)c * NSP;
         for (int ik = tid; ik < nk; ik += blockDim.x) {
             double acc[NSP];
@@ -506,7 +614,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
                     acc[a_] += sa;
                 } else {
                     float sa = 0.f;
-#pragma unroll 8
+#pragma unroll 16
                     for (int q = q0; q < q1; ++q) {
                         int2 ec = l_ms[q];
                         sa = fmaf((float)ec.y, __ldg(&msT32[(long)ec.x * nk + ik]), sa);
@@ -556,8 +664,7 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
 
         // ---- 7. commit
         if (s_acc) {
-            double *CHw = L.chi + (long)c * NSP * nk;
-            for (int q = tid; q < NSP * nk; q += blockDim.x) CHw[q] += s_dchi[q];
+            for (int q = tid; q < NSP * nk; q += blockDim.x) s_chi[q] += s_dchi[q];
             if (nent && swp) {
                 int *C = L.ms_C + (long)c * nent;
                 for (int q = tid; q < nms; q += blockDim.x) C[l_ms[q].x] += l_ms[q].y;
@@ -589,6 +696,8 @@ __global__ void __launch_bounds__(NT, (NT <= 128 ? 6 : 3)) k_step(const chx_ladd
         }
         __syncthreads();
     }  // steps
+    for (int q = tid; q < NSP * nk; q += blockDim.x) CHg[q] = s_chi[q];
+    __syncthreads();
 
     // ---- the last CTA of the launch advances the step counter
     if (tid == 0) {
@@ -615,7 +724,7 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
     typedef typename Real<PREC>::T2 real2;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ chx_ladder_t L;
-    __shared__ double s_num[32], s_den[32], s_sq[32], s_scale[8], s_c2;
+    __shared__ double s_num[32], s_den[32], s_sq[40], s_scale[8], s_c2;
     const int tid = threadIdx.x, slot = blockIdx.x;
     {
         const int *src = (const int *)&Ls[slot_ladder[slot]];
@@ -702,28 +811,31 @@ __global__ void k_shell_table(chx_ladder_t L, const double *__restrict__ rshell,
     }
 }
 
-template <int NSP, int PREC, int NT>
+template <int NSP, int PREC, int NT, int MINB>
 static int launch_step_nt(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
                           int nsteps, const StepSmem &so, size_t smem, uint64_t *d_stepc,
                           int *d_ticket, int *d_err, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_step<NSP, PREC, NT>,
+    cudaError_t e = cudaFuncSetAttribute(k_step<NSP, PREC, NT, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(e, "sampler_step attribute");
-    k_step<NSP, PREC, NT><<<nslots, NT, smem, st>>>(d_ladders, slot_ladder, nslots, nsteps, so,
-                                                    d_stepc, d_ticket, d_err);
+    k_step<NSP, PREC, NT, MINB><<<nslots, NT, smem, st>>>(d_ladders, slot_ladder, nslots, nsteps,
+                                                          so, d_stepc, d_ticket, d_err);
     CHX_CHECK_LAUNCH("sampler_step");
     return CHX_OK;
 }
 
 template <int NSP, int PREC>
 static int launch_step(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
-                       int nsteps, int threads, const StepSmem &so, size_t smem,
+                       int nsteps, int threads, int min_blocks, const StepSmem &so, size_t smem,
                        uint64_t *d_stepc, int *d_ticket, int *d_err, cudaStream_t st) {
     if (threads == 128)
-        return launch_step_nt<NSP, PREC, 128>(d_ladders, slot_ladder, nslots, nsteps, so, smem,
-                                              d_stepc, d_ticket, d_err, st);
-    return launch_step_nt<NSP, PREC, 256>(d_ladders, slot_ladder, nslots, nsteps, so, smem,
-                                          d_stepc, d_ticket, d_err, st);
+        return launch_step_nt<NSP, PREC, 128, 6>(d_ladders, slot_ladder, nslots, nsteps, so,
+                                                 smem, d_stepc, d_ticket, d_err, st);
+    if (min_blocks == 4)
+        return launch_step_nt<NSP, PREC, 256, 4>(d_ladders, slot_ladder, nslots, nsteps, so,
+                                                 smem, d_stepc, d_ticket, d_err, st);
+    return launch_step_nt<NSP, PREC, 256, 3>(d_ladders, slot_ladder, nslots, nsteps, so, smem,
+                                             d_stepc, d_ticket, d_err, st);
 }
 
 template <int NSP, int PREC>
@@ -747,6 +859,9 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
     for (int i = 0; i < nladders; ++i) {
         const chx_ladder_t &L = H[i];
         CHX_REQUIRE(L.nsp == nsp, "sampler: one launch needs one species count");
+        CHX_REQUIRE(!L.ms_nblk || (L.ms_tpl && L.ms_nbr && L.ms_D > 0 && L.ms_D < 0xFE &&
+                                   L.ms_M > 0 && L.natoms < 65536),
+                    "sampler: ladder %d has incomplete multiple-scattering templates", i);
         CHX_REQUIRE(L.ncoord > 0 && L.ncoord <= kMaxCoord && L.nk > 0 && L.nkw >= 1 &&
                         L.nkw <= 3 && L.nchan == L.nsp * L.nkw && (L.nfft & (L.nfft - 1)) == 0 &&
                         L.natoms < (1 << 20) && L.nwin > 0,
@@ -754,12 +869,12 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
         StepSmem s = step_smem(L, precision);
         // field sizes of this ladder, then the running maximum of each
         // field sizes of this ladder, then the running maximum of each
-        size_t f[10] = {s.x - s.u, s.tr - s.x, s.dchi - s.tr, s.dir - s.dchi, s.dirv - s.dir,
+        size_t f[12] = {s.x - s.u, s.tr - s.x, s.dchi - s.tr, s.dir - s.dchi, s.dirv - s.dir,
                         s.hist - s.dirv, s.dn - s.hist, s.list - s.dn, s.sp - s.list,
-                        s.total - s.sp};
-        size_t *g[10] = {&mx.u, &mx.x, &mx.tr, &mx.dchi, &mx.dir, &mx.dirv, &mx.hist, &mx.dn,
-                         &mx.list, &mx.sp};
-        for (int q = 0; q < 10; ++q) *g[q] = std::max(*g[q], f[q]);
+                        s.nb - s.sp, s.chi - s.nb, s.total - s.chi};
+        size_t *g[12] = {&mx.u, &mx.x, &mx.tr, &mx.dchi, &mx.dir, &mx.dirv, &mx.hist, &mx.dn,
+                         &mx.list, &mx.sp, &mx.nb, &mx.chi};
+        for (int q = 0; q < 12; ++q) *g[q] = std::max(*g[q], f[q]);
     }
     // mx holds field sizes; turn them into offsets
     StepSmem o;
@@ -774,6 +889,8 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
     o.dn = at; at += mx.dn;
     o.list = at; at += mx.list;
     o.sp = at; at += mx.sp;
+    o.nb = at; at += mx.nb;
+    o.chi = at; at += mx.chi;
     o.total = at;
     CHX_REQUIRE(at <= 220 * 1024, "sampler: %zu bytes of shared memory needed", at);
     *out = o;
@@ -812,13 +929,16 @@ int chx_shell_table(const chx_ladder_t *L, const double *rshell, const double *s
 
 int chx_sampler_step(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
                      int nladders, const int *slot_ladder, int nslots, int precision, int nsteps,
-                     int threads, uint64_t *d_stepc, int *d_ticket, int *d_err, void *stream) {
+                     int threads, int min_blocks, uint64_t *d_stepc, int *d_ticket, int *d_err,
+                     void *stream) {
     CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && d_stepc && d_ticket && d_err &&
                     nladders > 0 && nslots > 0 && nsteps > 0,
                 "sampler_step: bad arguments");
     CHX_REQUIRE(precision == CHX_FP64 || precision == CHX_FP32C, "sampler_step: bad precision");
-    CHX_REQUIRE(threads == 0 || threads == 128 || threads == 256,
-                "sampler_step: threads must be 128 or 256");
+    CHX_REQUIRE((threads == 0 && min_blocks == 0) || (threads == 128 && min_blocks == 6) ||
+                    (threads == 256 && (min_blocks == 3 || min_blocks == 4)),
+                "sampler_step: launch shape (%d, %d) not built; (128, 6), (256, 3) or (256, 4)",
+                threads, min_blocks);
     StepSmem so;
     size_t smem = 0;
     int rc = plan_ladders(host_ladders, nladders, precision, &so, &smem);
@@ -826,8 +946,8 @@ int chx_sampler_step(const chx_ladder_t *d_ladders, const chx_ladder_t *host_lad
     cudaStream_t st = as_stream(stream);
     int nsp = host_ladders[0].nsp;
 #define CHX_STEP(N, PR) \
-    launch_step<N, PR>(d_ladders, slot_ladder, nslots, nsteps, threads, so, smem, d_stepc, \
-                       d_ticket, d_err, st)
+    launch_step<N, PR>(d_ladders, slot_ladder, nslots, nsteps, threads, min_blocks, so, smem, \
+                       d_stepc, d_ticket, d_err, st)
     if (precision == CHX_FP64) {
         switch (nsp) {
             case 2: return CHX_STEP(2, CHX_FP64);

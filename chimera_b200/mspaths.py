@@ -251,10 +251,79 @@ class SupercellPaths:
         pad = np.full((1, 4), -1, np.int32)
         self.inc_rec = np.concatenate([self.records, pad])[self.inc]
 
-    def device(self):
-        """Device copies of the records, incidence records and offsets."""
+        self._templates(Xi, box, look)
+
+    # Every site of a cubic Bravais supercell sees the same paths up to a
+    # translation, so the paths through a site are one shared list of
+    # templates plus the site's own table of nearby sites.
+    SELF, NONE = 0xFE, 0xFF
+
+    def _templates(self, Xi, box, look):
+        """tpl (M, 2) int32: [class entry offset, 4 position bytes (absorber,
+        slot0, slot1, slot2): local index of the site in the neighbourhood
+        table, SELF for the site itself, NONE for an unused slot]; nbr
+        (natoms, D) int32: site index of every neighbourhood offset."""
+        offs = {}
+        rows = []
+        for g, cl in enumerate(self.classes):
+            for img, so in cl.images:
+                pos = [(0, 0, 0)] + [tuple(img[int(np.argmax(so == q))])
+                                     for q in range(cl.nslot)]
+                pos += [None] * (4 - len(pos))
+                for r in range(1 + cl.nslot):              # the site at position r
+                    code = 0
+                    for p in range(4):
+                        if p == r:
+                            v = self.SELF
+                        elif pos[p] is None:
+                            v = self.NONE
+                        else:
+                            d = tuple(int(x) for x in np.subtract(pos[p], pos[r]))
+                            v = offs.setdefault(d, len(offs))
+                        code |= v << (8 * p)
+                    rows.append((int(self.cls_off[g]), code))
+        if len(offs) >= self.SELF:
+            raise ValueError(f"{len(offs)} neighbourhood sites do not fit one byte")
+        if len(rows) != self.M:
+            raise ValueError("templates do not cover the incident paths")
+        self.D = len(offs)
+        D = np.array(list(offs.keys()), int)
+        t = np.array(rows, np.int64)
+        self.tpl = np.empty((len(rows), 2), np.int32)
+        self.tpl[:, 0] = t[:, 0]
+        self.tpl[:, 1] = (t[:, 1] & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
+        q = (Xi[:, None, :] + D[None, :, :]) % box
+        self.nbr = look[q[..., 0], q[..., 1], q[..., 2]].astype(np.int32)
+        if (self.nbr < 0).any():
+            raise ValueError("a neighbourhood offset lands off the lattice")
+
+    def template_entries(self, species, site, a=-1, b=-1, nsa=0, nsb=0):
+        """Entries of the paths through `site` from the templates (host check),
+        with the species of a and b replaced by nsa and nsb when given."""
+        sp = np.asarray(species).copy()
+        if a >= 0:
+            sp[a], sp[b] = nsa, nsb
+        out = []
+        mult = [self.nblk, 1, self.nsp, self.nsp ** 2]
+        for off, code in self.tpl:
+            e = int(off)
+            for p in range(4):
+                v = (int(code) >> (8 * p)) & 0xFF
+                if v == self.NONE:
+                    continue
+                st = site if v == self.SELF else int(self.nbr[site, v])
+                e += int(sp[st]) * mult[p]
+            out.append(e)
+        return np.array(out)
+
+    def device(self, what=("records", "inc_rec", "tpl", "nbr")):
+        """Device copies (created on first use) of the per-path records, the
+        per-site incidence records, the templates and the neighbourhoods."""
         if not hasattr(self, "_dev"):
-            self._dev = dict(records=N.to_dev(self.records), inc_rec=N.to_dev(self.inc_rec))
+            self._dev = {}
+        for k in what:
+            if k not in self._dev:
+                self._dev[k] = N.to_dev(getattr(self, k))
         return self._dev
 
 
@@ -286,7 +355,7 @@ class SupercellMS:
         torch = self._torch
         sp = torch.as_tensor(species).to("cuda", torch.int32).contiguous()
         nrep = sp.shape[0]
-        d = self.paths.device()
+        d = self.paths.device(("records",))
         out = torch.empty((nrep, self.nent), dtype=torch.int32, device="cuda")
         N.call("chx_ms_counts", N.ptr(sp), nrep, self.natoms, N.ptr(d["records"]), self.npath,
                self.nsp, self.nblk, N.ptr(out), N.stream())
@@ -312,7 +381,7 @@ class SupercellMS:
         torch = self._torch
         sp = torch.as_tensor(species).to("cuda", torch.int32).contiguous()
         nrep = sp.shape[0]
-        d = self.paths.device()
+        d = self.paths.device(("inc_rec",))
         args = [torch.as_tensor(x).to("cuda", torch.int32).contiguous() for x in (a, b, nsa, nsb)]
         dC = torch.empty((nrep, self.nent), dtype=torch.int32, device="cuda")
         N.call("chx_ms_delta", N.ptr(sp), nrep, self.natoms, N.ptr(d["inc_rec"]), self.M,

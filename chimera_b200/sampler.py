@@ -101,10 +101,10 @@ class LadderSpec:
 class Ladders:
     """Device state and descriptors of a batch of ladders (see module doc)."""
 
-    def __init__(self, specs, precision=FP64, use_table=True, threads=256):
+    def __init__(self, specs, precision=FP64, use_table=True, threads=256, min_blocks=3):
         import torch
         N.require_cuda()
-        self.threads = int(threads)
+        self.threads, self.min_blocks = int(threads), int(min_blocks)
         self.torch = torch
         self.specs = list(specs)
         self.precision = int(precision)
@@ -156,7 +156,8 @@ class Ladders:
         first = np.array([np.argmax(shell == q) for q in range(fm.nshell)])
         r_shell, s2_shell = d0[first], sig2[first]
         pair_tab = ((np.abs(d0 - r_shell[shell]) <= 1e-12 * r_shell[shell])
-                    & (sig2 == s2_shell[shell])).astype(np.uint8)
+                    & (sig2 == s2_shell[shell]))
+        pair_tab = (pair_tab & pair_tab[rev]).astype(np.uint8)   # a pair and its reverse agree
         b = dict(rev=self._t(rev), ideal=self._t(ideal), shift=self._t(shift),
                  sig2=self._t(sig2), pair_tab=self._t(pair_tab))
         L.natoms, L.ncoord, L.npairs, L.nshell, L.nsp, L.nk = (natoms, ncoord, fm.npairs,
@@ -186,10 +187,10 @@ class Ladders:
         # exact multiple scattering
         ms = s.ms
         if ms is not None:
-            d = ms.paths.device()
-            L.ms_nblk, L.ms_M = ms.nblk, ms.M
-            L.ms_inc, L.ms_T = N.dptr(d["inc_rec"]), N.dptr(ms.T)
-            self.keep += [d["inc_rec"], ms.T]
+            d = ms.paths.device(("tpl", "nbr"))
+            L.ms_nblk, L.ms_M, L.ms_D = ms.nblk, ms.paths.tpl.shape[0], ms.paths.D
+            L.ms_tpl, L.ms_nbr, L.ms_T = N.dptr(d["tpl"]), N.dptr(d["nbr"]), N.dptr(ms.T)
+            self.keep += [d["tpl"], d["nbr"], ms.T]
             if self.precision != FP64:
                 b["msT32"] = ms.T.float().contiguous()
                 self.keep.append(b["msT32"])
@@ -197,7 +198,7 @@ class Ladders:
             else:
                 L.ms_T32 = 0
         else:
-            L.ms_nblk, L.ms_M, L.ms_inc, L.ms_T, L.ms_T32 = 0, 0, 0, 0, 0
+            L.ms_nblk, L.ms_M, L.ms_D, L.ms_tpl, L.ms_nbr, L.ms_T, L.ms_T32 = 0, 0, 0, 0, 0, 0, 0
         # pair-interaction prior (method_a_rmc.py:147-157)
         if s.energy_prior is not None:
             V, T_ann = s.energy_prior
@@ -221,7 +222,8 @@ class Ladders:
                  tm_re=self._t(np.ascontiguousarray(tm.real, np.float64)),
                  tm_im=self._t(np.ascontiguousarray(tm.imag if cplx else np.zeros(tm.shape),
                                                     np.float64)),
-                 sm=self._t(sm))
+                 sm=self._t(sm), w2=self._t(1.0 / (sm * sm)),
+                 tnorm=self._t(((np.abs(tm) ** 2) / (sm * sm)).sum(1)))
         if f["extra"] is not None:
             b["extra"] = self._t(np.ascontiguousarray(f["extra"], np.float64))
         L.nchan, L.nkw, L.nwin, L.nfft, L.ncoef = (f["nchan"], f["nkw"], int(win.size),
@@ -231,6 +233,7 @@ class Ladders:
         L.win_bin, L.ft_norm = N.dptr(b["win"]), f["norm"]
         L.chi_extra = N.dptr(b.get("extra"))
         L.tm_re, L.tm_im, L.sm = N.dptr(b["tm_re"]), N.dptr(b["tm_im"]), N.dptr(b["sm"])
+        L.w2, L.tnorm = N.dptr(b["w2"]), N.dptr(b["tnorm"])
         L.cplx, L.profile = int(cplx), int(s.profile_scale)
         self.nfit_of = getattr(self, "nfit_of", []) + [int(s.mask.sum()) * f["nchan"] * (2 if cplx else 1)]
         L.nfit = float(self.nfit_of[-1])
@@ -348,8 +351,8 @@ class Ladders:
         assert 0 < nsteps <= MAX_BLOCK
         N.call("chx_sampler_step", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
                N.ptr(self.slot_ladder), self.nslots, self.precision, int(nsteps),
-               self.threads, N.ptr(self.stepc), N.ptr(self.ticket), N.ptr(self.err),
-               N.stream())
+               self.threads, self.min_blocks, N.ptr(self.stepc), N.ptr(self.ticket),
+               N.ptr(self.err), N.stream())
 
     def exchange_device(self):
         N.call("chx_replica_exchange", N.ptr(self.d_ladders), self.nladders, N.ptr(self.stepc),
@@ -631,10 +634,12 @@ class BatchedSampler:
     accepted moves (checked every `check_every` blocks)."""
 
     def __init__(self, specs, precision=FP32C, exchange_every=25, use_table=True,
-                 reanchor_every=1000, check_every=40, threads=256):
+                 reanchor_every=1000, check_every=40, threads=256, min_blocks=3):
         import torch
         self.torch = torch
-        self.lad = Ladders(specs, precision=precision, use_table=use_table, threads=threads)
+        self.lad = Ladders(specs, precision=precision, use_table=use_table, threads=threads,
+                           min_blocks=min_blocks)
+        self.tuning = None
         self.exchange_every = int(exchange_every)
         self.reanchor_every = int(reanchor_every)
         self.check_every = int(check_every)
@@ -654,6 +659,14 @@ class BatchedSampler:
             ps = pos0[li] if isinstance(pos0, (list, tuple)) else pos0
             self.lad.init_state(li, sp, ps)
         self.lad.refresh_chi2(reset_best=True)
+
+    def autotune(self, reps=3, path=None):
+        """Measure the step kernel's launch shapes on this problem (real
+        steps of the chains) and keep the fastest (chimera_b200.autotune)."""
+        from .autotune import tune
+        self.tuning = tune(self.lad, nsteps=self.exchange_every, reps=reps, path=path)
+        self.steps += self.exchange_every * (reps + 1) * 3
+        return self.tuning
 
     def block(self):
         """One exchange period: exchange_every steps in one launch, then the

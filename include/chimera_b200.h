@@ -210,9 +210,13 @@ typedef struct {
     double s02;
     const double *sstab;             /* (nshell*nsp*nsp, nk) ideal-shell terms, or NULL */
     const float *sstab32;            /* the same table in FP32 (CHX_FP32C), or NULL    */
-    /* exact multiple scattering, ms_nblk == 0 when off */
-    int ms_nblk, ms_M;
-    const int *ms_inc;               /* (natoms, ms_M, 4) records incident on a site */
+    /* exact multiple scattering, ms_nblk == 0 when off. The paths through a
+       site are ms_M shared templates {class entry offset, 4 position bytes:
+       neighbourhood index of the absorber and slots 0-2, 0xFE the site itself,
+       0xFF unused} resolved through the site's row of ms_nbr */
+    int ms_nblk, ms_M, ms_D;
+    const int *ms_tpl;               /* (ms_M, 2) path templates                  */
+    const int *ms_nbr;               /* (natoms, ms_D) neighbourhood site indices */
     const double *ms_T;              /* (nsp*ms_nblk, nk)                         */
     const float *ms_T32;             /* the same table in FP32 (CHX_FP32C), or NULL */
     /* pair-interaction prior, etab NULL when off (method_a_rmc.py:147-157,310-320) */
@@ -229,6 +233,8 @@ typedef struct {
     const double *chi_extra;         /* (nsp, nk) added before the transform, or NULL */
     double ft_norm;
     const double *tm_re, *tm_im, *sm;/* (nchan, nwin) target window and sigma     */
+    const double *w2;                /* (nchan, nwin) 1 / sigma^2                  */
+    const double *tnorm;             /* (nchan) sum |target|^2 / sigma^2           */
     int cplx, profile;
     double nfit;
     /* sampler constants */
@@ -273,12 +279,13 @@ CHX_API int chx_shell_table(const chx_ladder_t *L, const double *rshell, const d
  * device array of nladders descriptors; slot_ladder (nslots): ladder of each
  * slot. d_stepc: device counter; step s of the launch is step *d_stepc + s + 1
  * (the reference's `_stepc`, first step = 1), and the counter advances by
- * nsteps when the launch completes. threads: CTA size, 128 or 256 (0 picks
- * 256). d_err: device error word. */
+ * nsteps when the launch completes. (threads, min_blocks): the launch shape,
+ * CTA size and CTAs kept resident per SM: (128, 6), (256, 3) or (256, 4);
+ * (0, 0) picks (256, 3). d_err: device error word. */
 CHX_API int chx_sampler_step(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
                              int nladders, const int *slot_ladder, int nslots, int precision,
-                             int nsteps, int threads, uint64_t *d_stepc, int *d_ticket,
-                             int *d_err, void *stream);
+                             int nsteps, int threads, int min_blocks, uint64_t *d_stepc,
+                             int *d_ticket, int *d_err, void *stream);
 
 /* chi^2 of every slot's state chi (chi_in NULL) or of chi_in (nslots, nsp, nk)
  * with absorber counts count_in (nslots, nsp) (count NULL: the state's), by

@@ -77,3 +77,50 @@ def test_supercell_paths_and_oracle_counts(classes, nsp):
     chi = np.stack([dC[:, a * sp.nblk:(a + 1) * sp.nblk] @ T[a * sp.nblk:(a + 1) * sp.nblk]
                     for a in range(nsp)], axis=1)
     assert np.allclose(chi, g[key + "chi_delta"], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("nsp", [2, 3])
+def test_templates_give_the_incident_paths_entries(classes, nsp):
+    """Every site's paths, rebuilt from the shared templates and the site's
+    neighbourhood table, carry the same entries as its incidence records,
+    before and after a swap."""
+    from oracle import kernels as K
+    cell = L.CrystalSupercell("fcc", (5, 5, 5), 3.59)
+    sp = MP.SupercellPaths(classes, cell.ideal, cell.H, 3.59, nsp)
+    assert sp.tpl.shape == (sp.M, 2) and sp.nbr.shape == (sp.natoms, sp.D)
+    assert sp.D < 0xFE
+    rng = np.random.default_rng(nsp)
+    species = rng.integers(0, nsp, sp.natoms).astype(np.int32)
+    for site in rng.integers(0, sp.natoms, 4):
+        pids = sp.inc[site]
+        pids = pids[pids < sp.npath]
+        rec = []
+        for pid in pids:
+            e = species[sp.p_abs[pid]] * sp.nblk + sp.cls_off[sp.p_cls[pid]]
+            for q in range(3):
+                if sp.p_slot[pid, q] >= 0:
+                    e += species[sp.p_slot[pid, q]] * nsp ** q
+            rec.append(e)
+        assert np.array_equal(np.sort(sp.template_entries(species, site)), np.sort(rec))
+    # the count change of a swap, from templates, equals the oracle's
+    a, b = 17, int(sp.nbr[17, 3])
+    while species[a] == species[b]:
+        species[b] = (species[b] + 1) % nsp
+    nsa, nsb = int(species[b]), int(species[a])
+    dC = np.zeros(sp.nent)
+    for site, skip_a in ((a, False), (b, True)):
+        old = sp.template_entries(species, site)
+        new = sp.template_entries(species, site, a, b, nsa, nsb)
+        for t, (eo, en) in enumerate(zip(old, new)):
+            code = int(sp.tpl[t, 1])
+            sites = [site if ((code >> 8 * p) & 0xFF) == sp.SELF else
+                     (-1 if ((code >> 8 * p) & 0xFF) == sp.NONE else
+                      int(sp.nbr[site, (code >> 8 * p) & 0xFF])) for p in range(4)]
+            if skip_a and a in sites:
+                continue
+            dC[en] += 1
+            dC[eo] -= 1
+    ref = K.ms_delta(species[None], sp.inc, sp.p_abs, sp.p_cls, sp.p_slot, sp.npath,
+                     sp.cls_off, nsp, sp.nblk, np.array([a], np.int32), np.array([b], np.int32),
+                     np.array([nsa], np.int32), np.array([nsb], np.int32))[0]
+    assert np.array_equal(dC, ref)
