@@ -91,6 +91,7 @@ _SIGS = {
     "chx_sampler_smem_bytes": ([c_p, c_i, c_i], c_i),
     "chx_shell_table": ([c_p, c_p, c_p, c_p, c_p], c_i),
     "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
+    "chx_reanchor": ([c_p, c_p, c_i, c_p, c_i, c_p, c_p, c_p], c_i),
     "chx_replica_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_apply_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_ft_batch": ([c_p, c_i, c_i, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),

@@ -748,6 +748,132 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
     if (tid == 0) out[slot] = s_c2;
 }
 
+
+// ------------------------------------------------------- FP64 re-anchoring
+// A fresh FP64 recompute of a slot's chi(k) from its species, positions and
+// MS entry counts, in the pair-count form: pairs whose two atoms sit on their
+// ideal sites are counted by (shell, pair type) and contracted with the FP64
+// (shell, type) term table (the pair sum of the reference's pair-count model,
+// chimera/shellmodel.py:411-413, which equals the per-pair sum to rounding),
+// displaced pairs take the reference's FP64 term directly (kernels.py:22-29),
+// and the MS part is sum_e C_e T_e in FP64 (mslibrary.py:453-457). Only slots
+// with mask[slot] set are recomputed; their accepted-move counters are reset.
+constexpr int kReanchorChunk = 1024;   // pairs examined per round
+
+template <int NSP>
+__global__ void __launch_bounds__(256) k_reanchor(const chx_ladder_t *__restrict__ Ls,
+                                                  const int *__restrict__ slot_ladder,
+                                                  const uint8_t *__restrict__ mask,
+                                                  int *__restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ chx_ladder_t L;
+    __shared__ int s_ndir;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int slot = blockIdx.x;
+    if (mask && !mask[slot]) return;
+    {
+        const int *src = (const int *)&Ls[slot_ladder[slot]];
+        int *dst = (int *)&L;
+        for (int q = tid; q < (int)(sizeof(chx_ladder_t) / 4); q += blockDim.x) dst[q] = src[q];
+    }
+    __syncthreads();
+    const int c = slot - L.slot0;
+    const int natoms = L.natoms, z = L.ncoord, nk = L.nk, nn = NSP * NSP;
+    const int nbins = L.nshell * nn;
+    const int nwarps = blockDim.x / 32;
+    int *s_hist = (int *)smem;                               // (nwarps, nbins)
+    int *s_dir = s_hist + nwarps * nbins;                    // direct pairs of a chunk
+    uint8_t *s_flag = (uint8_t *)(s_dir + kReanchorChunk);   // 1: the pair is direct
+    uint8_t *s_sp = s_flag + kReanchorChunk;                 // species | moved << 7
+    const int *Sg = L.species + (long)c * natoms;
+    const uint8_t *MVg = L.moved + (long)c * natoms;
+    const double *P = L.pos + (long)c * natoms * 3;
+    for (int q = tid; q < nwarps * nbins; q += blockDim.x) s_hist[q] = 0;
+    for (int i = tid; i < natoms; i += blockDim.x)
+        s_sp[i] = (uint8_t)((Sg[i] & 0x7F) | (MVg[i] ? 0x80 : 0));
+    __syncthreads();
+    const bool tab = L.sstab != nullptr;
+    int *hw = s_hist + warp * nbins;
+    // thread tid owns k = tid and tid + blockDim (nk <= 2 * blockDim)
+    double acc[2][NSP];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int s = 0; s < NSP; ++s) acc[h][s] = 0.0;
+    for (int c0 = 0; c0 < L.npairs; c0 += kReanchorChunk) {
+        const int n = min(kReanchorChunk, L.npairs - c0);
+        for (int q = tid; q < n; q += blockDim.x) {
+            int p = c0 + q, i = p / z, j = L.jidx[p];
+            uint8_t direct = 0;
+            if ((unsigned)j >= (unsigned)natoms) {
+                atomicOr(err, CHX_DEVERR_INDEX);
+            } else {
+                int wi = s_sp[i], wj = s_sp[j];
+                if (tab && L.pair_tab[p] && !((wi | wj) & 0x80))
+                    atomicAdd(&hw[L.shell[p] * nn + (wi & 0x7F) * NSP + (wj & 0x7F)], 1);
+                else
+                    direct = 1;
+            }
+            s_flag[q] = direct;
+        }
+        __syncthreads();
+        if (warp == 0) {                       // in-order list of the chunk's direct pairs
+            int cnt = warp_compact(n, [&](int q) { return s_flag[q] != 0; }, s_dir);
+            if (lane == 0) s_ndir = cnt;
+        }
+        __syncthreads();
+        const int nd = s_ndir;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int ik = tid + h * blockDim.x;
+            if (ik >= nk || nd == 0) continue;
+            KPoint kp{L.ktab[ik], L.lamtab[ik]};
+            for (int q = 0; q < nd; ++q) {
+                int p = c0 + s_dir[q];
+                int i = p / z, j = L.jidx[p];
+                const double *sh3 = L.shift + 3 * (long)p;
+                const double *pi = P + 3 * (long)i, *pj = P + 3 * (long)j;
+                double dx = pj[0] + sh3[0] - pi[0], dy = pj[1] + sh3[1] - pi[1],
+                       dz = pj[2] + sh3[2] - pi[2];
+                double r = sqrt(dx * dx + dy * dy + dz * dz);
+                int t = (s_sp[i] & 0x7F) * NSP + (s_sp[j] & 0x7F);
+                add_by_species<NSP>(acc[h], t / NSP,
+                                    term64(r, t, L.shell[p], L.sig2[p], ik, nk, NSP, kp, L.ftab,
+                                           L.dtab, L.drtab, L.c3tab, L.s2tab, L.s02));
+            }
+        }
+        __syncthreads();
+    }
+    for (int bb = tid; bb < nbins; bb += blockDim.x) {
+        int v = 0;
+        for (int w = 0; w < nwarps; ++w) v += s_hist[w * nbins + bb];
+        s_hist[bb] = v;
+    }
+    __syncthreads();
+    const int nent = L.ms_nblk ? NSP * L.ms_nblk : 0;
+    const int *C = L.ms_C + (long)c * nent;
+    double *CHg = L.chi + (long)c * NSP * nk;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int ik = tid + h * blockDim.x;
+        if (ik >= nk) continue;
+        if (tab)
+            for (int bb = 0; bb < nbins; ++bb) {
+                int n = s_hist[bb];
+                if (n)
+                    add_by_species<NSP>(acc[h], (bb % nn) / NSP,
+                                        (double)n * L.sstab[(long)bb * nk + ik]);
+            }
+        for (int e = 0; e < nent; ++e) {
+            int n = C[e];
+            if (n) add_by_species<NSP>(acc[h], e / L.ms_nblk, (double)n * L.ms_T[(long)e * nk + ik]);
+        }
+#pragma unroll
+        for (int s = 0; s < NSP; ++s) CHg[s * nk + ik] = acc[h][s];
+    }
+    if (tid == 0) L.n_acc[c] = 0;
+}
+
 // ------------------------------------------------------- replica exchange
 // One thread per ladder (method_a_rmc.py:332-373 with the uniforms from a
 // counter stream): rung pairs (i, i+1) from a random parity, d >= 0 or
@@ -994,6 +1120,40 @@ int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladder
 #undef CHX_EV
     set_error("eval_chi2: nsp %d not built", nsp);
     return CHX_ERR_UNSUPPORTED;
+}
+
+int chx_reanchor(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders, int nladders,
+                 const int *slot_ladder, int nslots, const uint8_t *mask, int *d_err,
+                 void *stream) {
+    CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && d_err && nladders > 0 && nslots > 0,
+                "reanchor: bad arguments");
+    int nsp = host_ladders[0].nsp;
+    size_t smem = 0;
+    for (int i = 0; i < nladders; ++i) {
+        const chx_ladder_t &L = host_ladders[i];
+        CHX_REQUIRE(L.nsp == nsp, "reanchor: one launch needs one species count");
+        CHX_REQUIRE(L.nk <= 512, "reanchor: nk %d above 512", L.nk);
+        size_t b = sizeof(int) * ((size_t)8 * L.nshell * nsp * nsp + kReanchorChunk) +
+                   (size_t)kReanchorChunk + (size_t)L.natoms;
+        smem = std::max(smem, b);
+    }
+    CHX_REQUIRE(smem <= 200 * 1024, "reanchor: %zu bytes of shared memory needed", smem);
+    cudaStream_t st = as_stream(stream);
+#define CHX_RA(N)                                                                              \
+    do {                                                                                       \
+        cudaFuncSetAttribute(k_reanchor<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+                             (int)smem);                                                       \
+        k_reanchor<N><<<nslots, 256, smem, st>>>(d_ladders, slot_ladder, mask, d_err);          \
+    } while (0)
+    switch (nsp) {
+        case 2: CHX_RA(2); break;
+        case 3: CHX_RA(3); break;
+        case 4: CHX_RA(4); break;
+        default: set_error("reanchor: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+    }
+#undef CHX_RA
+    CHX_CHECK_LAUNCH("reanchor");
+    return CHX_OK;
 }
 
 int chx_replica_exchange(const chx_ladder_t *d_ladders, int nladders, const uint64_t *round_key,

@@ -334,16 +334,31 @@ class Ladders:
                 b["best_sp"].copy_(b["species"])
                 b["best_pos"].copy_(b["pos"])
 
-    def reanchor(self):
-        """Replace every slot's running chi by an FP64 recompute from its
-        species and positions (and exact MS counts), then its chi^2."""
-        for s, b in zip(self.specs, self.bufs):
-            chi = s.fm.chi_full(b["pos"], b["species"], precision=FP64)
-            if s.ms is not None:
-                chi = chi + s.ms.chi_of(b["ms_C"])
-            b["chi"].copy_(chi)
-            b["n_acc"].zero_()
+    def reanchor(self, mask=None):
+        """Replace the running chi of the slots in `mask` (a (nslots,) bool
+        array; None: all) by an FP64 recompute from their species, positions
+        and exact MS counts, reset their accepted-move counters, and refresh
+        chi^2. With the (shell, type) table this is one chx_reanchor launch
+        (pair-count form); otherwise the full FP64 path sum."""
+        torch = self.torch
+        if self.use_table:
+            m = None if mask is None else torch.as_tensor(mask).to("cuda", torch.uint8).contiguous()
+            N.call("chx_reanchor", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
+                   N.ptr(self.slot_ladder), self.nslots, N.ptr(m) if m is not None else None,
+                   N.ptr(self.err), N.stream())
+            self._reanchor_mask = m
+        else:
+            for s, b in zip(self.specs, self.bufs):
+                chi = s.fm.chi_full(b["pos"], b["species"], precision=FP64)
+                if s.ms is not None:
+                    chi = chi + s.ms.chi_of(b["ms_C"])
+                b["chi"].copy_(chi)
+                b["n_acc"].zero_()
         self.refresh_chi2()
+
+    def accepted_since_anchor(self):
+        """(nslots,) accepted moves since each slot's last re-anchoring."""
+        return self.torch.cat([b["n_acc"] for b in self.bufs])
 
     # --------------------------------------------------------------- steps
     def step(self, nsteps=1):
@@ -697,8 +712,9 @@ class BatchedSampler:
             self.blocks += 1
             self.steps += self.exchange_every
             if self.reanchor_every and self.blocks % self.check_every == 0:
-                if int(max(int(b["n_acc"].max()) for b in self.lad.bufs)) >= self.reanchor_every:
-                    self.lad.reanchor()
+                due = self.lad.accepted_since_anchor() >= self.reanchor_every
+                if bool(due.any()):
+                    self.lad.reanchor(due)
                     self.reanchors += 1
 
     def best(self, li):

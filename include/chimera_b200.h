@@ -295,6 +295,18 @@ CHX_API int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *hos
                           const double *chi_in, const double *count_in, double *out,
                           void *stream);
 
+/* FP64 re-anchoring (no reference counterpart; the reference accumulates its
+ * running chi in FP64 forever, method_a_rmc.py:298): replace the running chi of
+ * every slot with mask[slot] != 0 (mask NULL: every slot) by a fresh FP64
+ * recompute from its species, positions and MS entry counts, in the
+ * pair-count form (pairs on ideal sites counted per (shell, type) and
+ * contracted with the FP64 term table sstab; displaced pairs by the FP64 pair
+ * term, visited in fixed order), and reset its accepted-move counter. Uses
+ * the counted form where sstab is set; nk <= 512. */
+CHX_API int chx_reanchor(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                         int nladders, const int *slot_ladder, int nslots, const uint8_t *mask,
+                         int *d_err, void *stream);
+
 /* Replica exchange decided on the device (method_a_rmc.py:332-373): alternate
  * adjacent rung pairs from a random start parity, accept d >= 0 or
  * u < exp(max(d, -60)) with d = (b_i - b_{i+1})(E_i - E_{i+1}) nfit. The

@@ -66,3 +66,28 @@ def test_fp32c_tracks_full_recompute(cuda, name):
     assert all((np.sort(s) == np.sort(d["species0"])).all() for s in sp)
     assert abs(smp.best_verified - smp.best()[2]) <= 1e-3 * abs(smp.best()[2])
     assert lad.device_error() == 0
+
+
+def test_reanchor_kernel_equals_fp64_recompute(cuda):
+    """The pair-count FP64 re-anchoring of chx_reanchor gives the state's FP64
+    path sum (ideal pairs via the shell table, displaced pairs directly, exact
+    MS counts) to rounding, on the slots it is asked to recompute only."""
+    torch = cuda
+    d = trace_inputs("rmc_trace_ms.npz")
+    d["swap_frac"] = np.float64(0.7)            # make displaced atoms appear
+    smp, fm = device_objects(d, precision=1, reproduce=False)
+    smp.init_state(d["species0"], d["ideal"])
+    smp.run(200, exchange_every=25, log_every=10 ** 9)
+    lad, b = smp.lad, smp.b
+    assert int(b["moved"].sum()) > 0
+    before = b["chi"].clone()
+    mask = np.zeros(lad.nslots, bool)
+    mask[::2] = True
+    lad.reanchor(mask)
+    after = b["chi"].cpu().numpy()
+    full = fm.chi_full(b["pos"], b["species"]).cpu().numpy() + smp.ms.chi_of(b["ms_C"]).cpu().numpy()
+    scale = np.abs(full).max()
+    assert np.abs(after[mask] - full[mask]).max() <= 1e-12 * scale
+    assert np.array_equal(after[~mask], before.cpu().numpy()[~mask])
+    assert (b["n_acc"].cpu().numpy()[mask] == 0).all()
+    assert lad.device_error() == 0
