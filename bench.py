@@ -127,13 +127,15 @@ def peaks():
 
 
 def step_bytes(prob):
-    """Algorithmic bytes one replica's swap attempt reads or writes: the MS
-    incidence records of both sites, the affected pairs' topology, the
-    endpoint species, and the replica's chi row."""
+    """Algorithmic bytes of one swap attempt in the reference's own int32
+    layout: for both sites, the z pair ids (4 B) and neighbour species (1 B),
+    and the M incident MS paths (4 B path id, 4 B absorber/class, 12 B slot
+    ids, 4 B species); the delta chi is fused into the transform, so it is not
+    written back. The kernel reads far less (the MS paths come from shared
+    templates and the species from shared memory): see `traffic`."""
     z = prob.top.ncoord
-    M = prob.ms.M if prob.ms is not None else 0
-    nsp, nk = prob.nsp, prob.k.size
-    return 2 * M * 16 + 4 * z * 45 + 2 * z * 4 + 8 * z * 4 + nsp * nk * 8
+    M = prob.paths.M if prob.paths is not None else 0
+    return 2 * z * (4 + 1) + 2 * M * 24
 
 
 def time_graph(fn, reps):
@@ -238,7 +240,7 @@ def main():
     global NPOS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=1200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=30)
@@ -306,7 +308,9 @@ def main():
     traffic = None
     tp = os.path.join(ROOT, "profiles", "step_traffic.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get("bytes_per_launch")
+        t = json.load(open(tp))
+        # DRAM bytes per replica-step from the capture, scaled to this launch
+        traffic = t["dram_bytes_per_replica_step"] * smp.nslots * EXCH
 
     # ---- end to end through the public API with host buffers
     torch.cuda.synchronize()
@@ -341,7 +345,9 @@ def main():
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "peak_source": src, "kernel": "k_step (fused sampler step)",
                          "launch_us": per_launch * 1e6, "step_us": per_step * 1e6,
-                         "bytes_per_launch": step_bytes(prob) * smp.nslots * EXCH},
+                         "bytes_per_launch": step_bytes(prob) * smp.nslots * EXCH,
+                         "bytes_layout": "reference int32 layout (algorithmic); traffic = "
+                                         "measured DRAM bytes of the same launch (ncu)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": h2d / (e2e_blocks + 1),
