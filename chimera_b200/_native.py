@@ -64,7 +64,18 @@ class Ladder(C.Structure):
         ("species", c_p), ("pos", c_p), ("moved", c_p), ("chi", c_p), ("chi2", c_p),
         ("count", c_p), ("rung_of", c_p), ("slot_of", c_p), ("best_chi2", c_p),
         ("best_sp", c_p), ("best_pos", c_p), ("ms_C", c_p), ("acc_rung", c_p), ("acc_log", c_p), ("n_acc", c_p),
-        ("exch_att", c_p), ("exch_acc", c_p)]
+        ("exch_att", c_p), ("exch_acc", c_p),
+        ("mlp", c_p), ("feat_nbr", c_p), ("feat_D", c_i), ("da_on", c_p), ("da_stat", c_p),
+        ("log_codes", c_p), ("log_y", c_p), ("log_cap", c_i64)]
+
+
+class Mlp(C.Structure):
+    """chx_mlp_t"""
+    _fields_ = [("nsp", c_i), ("D", c_i), ("H", c_i), ("nin", c_i),
+                ("W1", c_p), ("W2", c_p), ("W3", c_p), ("w4", c_p),
+                ("b1", c_p), ("b2", c_p), ("b3", c_p), ("b4", c_p),
+                ("out_scale", C.c_float), ("feat_shift", C.c_float), ("feat_scale", C.c_float),
+                ("nchain", c_i)]
 
 
 # argument types of every entry point, in header order
@@ -96,6 +107,13 @@ _SIGS = {
     "chx_apply_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_ft_batch": ([c_p, c_i, c_i, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),
     "chx_ft_batch_scratch_bytes": ([c_i, c_i, c_i, c_i], c_i64),
+    "chx_mlp_nparam": ([c_i, c_i, c_i, c_i], c_i64),
+    "chx_mlp_bind": ([c_p, c_i, c_i, c_i, c_i, c_p, c_p], c_i),
+    "chx_mlp_predict": ([c_p, c_p, c_p, c_p, c_i, c_p, c_p], c_i),
+    "chx_mlp_work_bytes": ([c_i, c_i], c_i64),
+    "chx_mlp_grad": ([c_p] * 5 + [c_i] + [c_p] * 5, c_i),
+    "chx_mlp_adam": ([c_p] * 5 + [c_i64, C.c_float, C.c_float, C.c_float, C.c_float, c_i, c_p],
+                     c_i),
 }
 
 # entry points declared in include/chimera_b200.h (checked by the tests)
@@ -124,9 +142,9 @@ def lib():
 
 
 def _check_abi(L):
-    got = (L.chx_struct_size(0), L.chx_struct_size(1), L.chx_struct_size(2),
-           L.chx_struct_size(3))
-    want = (C.sizeof(Pairs), C.sizeof(Ladder), Ladder.exch_acc.offset, Ladder.seed.offset)
+    got = tuple(L.chx_struct_size(q) for q in range(6))
+    want = (C.sizeof(Pairs), C.sizeof(Ladder), Ladder.exch_acc.offset, Ladder.seed.offset,
+            C.sizeof(Mlp), Ladder.log_cap.offset)
     if got != want:
         raise ChxError(f"ABI mismatch between chimera_b200.h and the binding: {got} != {want}")
 

@@ -267,6 +267,8 @@ int64_t chx_struct_size(int which) {
         case 1: return (int64_t)sizeof(chx_ladder_t);
         case 2: return (int64_t)offsetof(chx_ladder_t, exch_acc);
         case 3: return (int64_t)offsetof(chx_ladder_t, seed);
+        case 4: return (int64_t)sizeof(chx_mlp_t);
+        case 5: return (int64_t)offsetof(chx_ladder_t, log_cap);
         default: return -1;
     }
 }

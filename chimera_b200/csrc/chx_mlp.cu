@@ -1,0 +1,466 @@
+// chx_mlp.cu -- the swap surrogate's batch kernels: inference (the same
+// per-CTA code the sampler runs), training forward + loss + gradient, Adam.
+//
+// Training works on a batch of B logged swaps. The two dense layers
+// (B x H x H) run on the tensor cores through one strided BF16 GEMM
+// (mma.sync m16n8k16, FP32 accumulation) that serves the forward (H W), the
+// weight gradients (H^T dZ) and the input gradients (dZ W^T). Layer 1 is a
+// gather-sum of W1 rows (its input is one-hot), and its weight gradient a
+// per-site scatter done as one CTA per input site with no atomics. Every
+// reduction runs in a fixed order, so a gradient is reproducible bit for bit.
+// Rounding: weights BF16; activations and the back-propagated dZ rounded to
+// BF16 before they enter a GEMM; everything else FP32.
+#include "chx_mlp.cuh"
+
+namespace chx {
+
+static inline int64_t mlp_nin(int nsp, int D, int nchain) {
+    return (int64_t)nsp * (nsp - 1) / 2 + 2LL * D * (nsp + 1) + nchain;
+}
+
+// ---------------------------------------------------------------- GEMM
+// C[m][n] = sum_k A(m,k) B(k,n) (+ bias[n]); A(m,k) = A[m*sam + k*sak],
+// B(k,n) = B[k*sbk + n*sbn] (BF16 bit patterns); C FP32 with row stride ldc;
+// with Cb, also BF16(relu(C)) (relu != 0) or BF16(C) into Cb (row stride ldc).
+constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
+
+__device__ __forceinline__ uint32_t pack2(uint16_t lo, uint16_t hi) {
+    return (uint32_t)lo | ((uint32_t)hi << 16);
+}
+
+__global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t *__restrict__ A, long sam,
+                                                   long sak, const uint16_t *__restrict__ B,
+                                                   long sbk, long sbn, float *__restrict__ C,
+                                                   long ldc, uint16_t *__restrict__ Cb,
+                                                   const float *__restrict__ bias, int M, int N,
+                                                   int K, int relu) {
+    __shared__ uint16_t sa[GT_M][GT_K + 2];
+    __shared__ uint16_t sb[GT_K][GT_N + 2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;   // the warp's 32 x 32 sub-tile
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+    for (int k0 = 0; k0 < K; k0 += GT_K) {
+        for (int q = tid; q < GT_M * GT_K; q += blockDim.x) {
+            int mm = q / GT_K, kk = q % GT_K, gm = m0 + mm, gk = k0 + kk;
+            sa[mm][kk] = (gm < M && gk < K) ? A[gm * sam + gk * sak] : (uint16_t)0;
+        }
+        for (int q = tid; q < GT_K * GT_N; q += blockDim.x) {
+            int kk = q / GT_N, nn = q % GT_N, gk = k0 + kk, gn = n0 + nn;
+            sb[kk][nn] = (gk < K && gn < N) ? B[gk * sbk + gn * sbn] : (uint16_t)0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int r = wm + i * 16;
+            uint32_t a0 = pack2(sa[r + g][2 * t], sa[r + g][2 * t + 1]);
+            uint32_t a1 = pack2(sa[r + g + 8][2 * t], sa[r + g + 8][2 * t + 1]);
+            uint32_t a2 = pack2(sa[r + g][2 * t + 8], sa[r + g][2 * t + 9]);
+            uint32_t a3 = pack2(sa[r + g + 8][2 * t + 8], sa[r + g + 8][2 * t + 9]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int cc = wn + j * 8 + g;
+                uint32_t b0 = pack2(sb[2 * t][cc], sb[2 * t + 1][cc]);
+                uint32_t b1 = pack2(sb[2 * t + 8][cc], sb[2 * t + 9][cc]);
+                asm volatile(
+                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                    "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+                    : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]),
+                      "+f"(acc[i][j][3])
+                    : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int gm = m0 + wm + i * 16 + g + ((q & 2) ? 8 : 0);
+                const int gn = n0 + wn + j * 8 + 2 * t + (q & 1);
+                if (gm >= M || gn >= N) continue;
+                float v = acc[i][j][q];
+                if (bias) v += bias[gn];
+                C[gm * ldc + gn] = v;
+                if (Cb)
+                    Cb[gm * ldc + gn] =
+                        __bfloat16_as_ushort(__float2bfloat16_rn(relu ? fmaxf(v, 0.f) : v));
+            }
+}
+
+static void gemm(const uint16_t *A, long sam, long sak, const uint16_t *B, long sbk, long sbn,
+                 float *C, long ldc, uint16_t *Cb, const float *bias, int M, int N, int K,
+                 int relu, cudaStream_t st) {
+    dim3 grid((N + GT_N - 1) / GT_N, (M + GT_M - 1) / GT_M);
+    k_gemm_bf16<<<grid, 128, 0, st>>>(A, sam, sak, B, sbk, sbn, C, ldc, Cb, bias, M, N, K, relu);
+}
+
+// ---------------------------------------------------------------- forward
+// Z1[b][o] = b1[o] + f_b W1[nin][o] + sum over the sample's rows of W1[row][o]
+__global__ void k_l1_fwd(chx_mlp_t P, const uint8_t *__restrict__ codes,
+                         const float *__restrict__ lnbeta, const int *__restrict__ chain, int B,
+                         float *__restrict__ Z1, uint16_t *__restrict__ H1b) {
+    const int b = blockIdx.x, H = P.H, D2 = 2 * P.D, ns1 = P.nsp + 1;
+    const int npt = P.nsp * (P.nsp - 1) / 2;
+    if (b >= B) return;
+    const uint8_t *cd = codes + (long)b * (D2 + 1);
+    const float f = (lnbeta[b] - P.feat_shift) * P.feat_scale;
+    const int ch = chain ? chain[b] : -1;
+    const bool has_ch = ch >= 0 && ch < P.nchain;
+    for (int o = threadIdx.x; o < H; o += blockDim.x) {
+        float s = 0.f;
+        for (int k = 0; k <= D2; ++k) {
+            int row = k == 0 ? (int)cd[0] : npt + (k - 1) * ns1 + (int)cd[k];
+            s += bf16f(P.W1[(long)row * H + o]);
+        }
+        if (has_ch) s += bf16f(P.W1[(long)(npt + D2 * ns1 + ch) * H + o]);
+        s = fmaf(f, bf16f(P.W1[(long)P.nin * H + o]), P.b1[o]) + s;
+        Z1[(long)b * H + o] = s;
+        H1b[(long)b * H + o] = __bfloat16_as_ushort(__float2bfloat16_rn(fmaxf(s, 0.f)));
+    }
+}
+
+// y[b] = b4 + sum_i h3[b][i] w4[i], one warp per sample
+__global__ void k_out_fwd(chx_mlp_t P, const uint16_t *__restrict__ H3b, int B,
+                          float *__restrict__ y) {
+    const int b = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (b >= B) return;
+    float s = 0.f;
+    for (int i = lane; i < P.H; i += 32)
+        s = fmaf(bf16f(H3b[(long)b * P.H + i]), bf16f(P.w4[i]), s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[b] = s + P.b4[0];
+}
+
+// ---------------------------------------------------------------- backward
+// dy_b = 2 (y_b - t_b) / B; dZ3 = BF16(dy_b w4[i] [Z3 > 0])
+__global__ void k_out_back(chx_mlp_t P, const float *__restrict__ y, const float *__restrict__ t,
+                           int B, const float *__restrict__ Z3, float *__restrict__ dy,
+                           uint16_t *__restrict__ dZ3) {
+    const int b = blockIdx.x;
+    if (b >= B) return;
+    const float d = 2.f * (y[b] - t[b]) / (float)B;
+    if (threadIdx.x == 0) dy[b] = d;
+    for (int i = threadIdx.x; i < P.H; i += blockDim.x) {
+        long q = (long)b * P.H + i;
+        float v = Z3[q] > 0.f ? d * bf16f(P.w4[i]) : 0.f;
+        dZ3[q] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+    }
+}
+
+// dZ = BF16(dH [Z > 0]), elementwise over n values
+__global__ void k_relu_back(const float *__restrict__ dH, const float *__restrict__ Z, long n,
+                            uint16_t *__restrict__ dZ) {
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    dZ[q] = __bfloat16_as_ushort(__float2bfloat16_rn(Z[q] > 0.f ? dH[q] : 0.f));
+}
+
+// out[o] = sum_b w_b X[b][o] (w NULL: 1), X BF16 (B, H): 32 columns per CTA,
+// 8 row groups, reduced in fixed order
+__global__ void __launch_bounds__(256) k_colsum(const uint16_t *__restrict__ X,
+                                                const float *__restrict__ w, int B, int H,
+                                                float *__restrict__ out) {
+    __shared__ float red[8][33];
+    const int cx = threadIdx.x & 31, ry = threadIdx.x >> 5;
+    const int o = blockIdx.x * 32 + cx;
+    float s = 0.f;
+    if (o < H)
+        for (int b = ry; b < B; b += 8) {
+            float x = bf16f(X[(long)b * H + o]);
+            s = w ? fmaf(w[b], x, s) : s + x;
+        }
+    red[ry][cx] = s;
+    __syncthreads();
+    if (ry == 0 && o < H) {
+        float t = 0.f;
+        for (int r = 0; r < 8; ++r) t += red[r][cx];
+        out[o] = t;
+    }
+}
+
+// gb4 = sum_b dy_b, loss = mean (y - t)^2 (one CTA, fixed order)
+__global__ void __launch_bounds__(256) k_loss(const float *__restrict__ y,
+                                              const float *__restrict__ t,
+                                              const float *__restrict__ dy, int B,
+                                              float *__restrict__ gb4, float *__restrict__ loss) {
+    __shared__ float r1[256], r2[256];
+    float s1 = 0.f, s2 = 0.f;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) {
+        float e = y[b] - t[b];
+        s1 = fmaf(e, e, s1);
+        s2 += dy[b];
+    }
+    r1[threadIdx.x] = s1;
+    r2[threadIdx.x] = s2;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            r1[threadIdx.x] += r1[threadIdx.x + h];
+            r2[threadIdx.x] += r2[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *loss = r1[0] / (float)B;
+        *gb4 = r2[0];
+    }
+}
+
+// gW1: CTA k < 1 + 2D owns input site k: for each sample b the row named by
+// code[b][k] gains dZ1[b][:]. A site's code values are below 8.
+__global__ void __launch_bounds__(256) k_l1_back(chx_mlp_t P, const uint8_t *__restrict__ codes,
+                                                 int B, const uint16_t *__restrict__ dZ1,
+                                                 float *__restrict__ gW1) {
+    const int k = blockIdx.x, H = P.H, D2 = 2 * P.D, ns1 = P.nsp + 1;
+    const int npt = P.nsp * (P.nsp - 1) / 2;
+    const int nv = k == 0 ? npt : ns1, row0 = k == 0 ? 0 : npt + (k - 1) * ns1;
+    for (int o = threadIdx.x; o < H; o += blockDim.x) {
+        float acc[8];
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[v] = 0.f;
+        for (int b = 0; b < B; ++b) {
+            const int v = codes[(long)b * (D2 + 1) + k];
+            const float d = bf16f(dZ1[(long)b * H + o]);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (u == v) acc[u] += d;
+        }
+        for (int v = 0; v < nv && v < 8; ++v) gW1[(long)(row0 + v) * H + o] = acc[v];
+    }
+}
+
+// gW1 chain rows: CTA c sums dZ1 over the run of samples with chain c
+// (chain sorted ascending), in order
+__global__ void __launch_bounds__(256) k_chain_back(chx_mlp_t P, const int *__restrict__ chain,
+                                                    int B, const uint16_t *__restrict__ dZ1,
+                                                    float *__restrict__ gW1) {
+    const int c = blockIdx.x, H = P.H;
+    const int row = P.nsp * (P.nsp - 1) / 2 + 2 * P.D * (P.nsp + 1) + c;
+    int lo = 0, hi = B;            // first sample with chain >= c
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (chain[mid] < c) lo = mid + 1;
+        else hi = mid;
+    }
+    for (int o = threadIdx.x; o < H; o += blockDim.x) {
+        float s = 0.f;
+        for (int b = lo; b < B && chain[b] == c; ++b) s += bf16f(dZ1[(long)b * H + o]);
+        gW1[(long)row * H + o] = s;
+    }
+}
+
+__global__ void k_normfeat(chx_mlp_t P, const float *__restrict__ lnbeta, int B,
+                           float *__restrict__ f) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < B) f[b] = (lnbeta[b] - P.feat_shift) * P.feat_scale;
+}
+
+// ---------------------------------------------------------------- predict
+__global__ void __launch_bounds__(256) k_predict(const chx_mlp_t *__restrict__ Pd,
+                                                 const uint8_t *__restrict__ codes,
+                                                 const float *__restrict__ lnbeta,
+                                                 const int *__restrict__ chain, int B,
+                                                 float *__restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ chx_mlp_t P;
+    if (threadIdx.x == 0) P = *Pd;
+    __syncthreads();
+    const int nsite = 2 * P.D + 1, nw = blockDim.x >> 5;
+    float *part = (float *)smem;
+    float *h = part + nw * P.H;
+    uint8_t *s_codes = (uint8_t *)(h + P.H);
+    for (int b = blockIdx.x; b < B; b += gridDim.x) {
+        for (int k = threadIdx.x; k < nsite; k += blockDim.x)
+            s_codes[k] = codes[(long)b * nsite + k];
+        __syncthreads();
+        float y = mlp_eval_cta(P, s_codes, lnbeta[b], chain ? chain[b] : -1, part, h);
+        if (threadIdx.x == 0) out[b] = y;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- Adam
+__global__ void k_adam(float *__restrict__ w, uint16_t *__restrict__ wb,
+                       const float *__restrict__ g, float *__restrict__ m, float *__restrict__ v,
+                       long n, float lr, float b1, float b2, float eps, float c1, float c2) {
+    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    wb[i] = __bfloat16_as_ushort(__float2bfloat16_rn(wi));
+}
+
+struct MlpOffsets {
+    int64_t W1, b1, W2, b2, W3, b3, w4, b4, n;
+};
+static MlpOffsets mlp_offsets(int nsp, int D, int nchain, int H) {
+    MlpOffsets o;
+    int64_t nin = mlp_nin(nsp, D, nchain);
+    o.W1 = 0;
+    o.b1 = o.W1 + (nin + 1) * H;
+    o.W2 = o.b1 + H;
+    o.b2 = o.W2 + (int64_t)H * H;
+    o.W3 = o.b2 + H;
+    o.b3 = o.W3 + (int64_t)H * H;
+    o.w4 = o.b3 + H;
+    o.b4 = o.w4 + H;
+    o.n = o.b4 + 1;
+    return o;
+}
+
+static bool mlp_shape_ok(int nsp, int D, int nchain, int H) {
+    return nsp >= 2 && nsp <= 7 && D >= 1 && D <= 127 && nchain >= 0 && nchain <= (1 << 20) &&
+           H >= 8 && H <= 256 && H % 8 == 0;
+}
+
+// dynamic shared memory of k_predict for the largest shape (H 256, D 127)
+static size_t predict_smem_bytes() { return (size_t)(8 * 256 + 256) * sizeof(float) + 256; }
+
+}  // namespace chx
+
+using namespace chx;
+
+extern "C" {
+
+int64_t chx_mlp_nparam(int nsp, int D, int nchain, int H) {
+    if (!mlp_shape_ok(nsp, D, nchain, H)) return -1;
+    return mlp_offsets(nsp, D, nchain, H).n;
+}
+
+int chx_mlp_bind(chx_mlp_t *P, int nsp, int D, int nchain, int H, const float *theta,
+                 const uint16_t *theta16) {
+    CHX_REQUIRE(P && theta && theta16, "mlp_bind: null pointer");
+    CHX_REQUIRE(mlp_shape_ok(nsp, D, nchain, H),
+                "mlp_bind: need 2 <= nsp <= 7, 1 <= D <= 127, 0 <= nchain <= 2^20, "
+                "8 <= H <= 256, H % 8 == 0");
+    CHX_REQUIRE(nsp * (nsp - 1) / 2 <= 8, "mlp_bind: at most 8 species pairs");
+    // W1, W2, W3 rows are read as 16-byte words
+    CHX_REQUIRE(((uintptr_t)theta16 & 15) == 0, "mlp_bind: theta16 must be 16-byte aligned");
+    MlpOffsets o = mlp_offsets(nsp, D, nchain, H);
+    CHX_REQUIRE((o.W2 * 2) % 16 == 0 && (o.W3 * 2) % 16 == 0,
+                "mlp_bind: layout misaligned for this H");
+    P->nsp = nsp;
+    P->D = D;
+    P->H = H;
+    P->nchain = nchain;
+    P->nin = (int)mlp_nin(nsp, D, nchain);
+    P->W1 = theta16 + o.W1;
+    P->W2 = theta16 + o.W2;
+    P->W3 = theta16 + o.W3;
+    P->w4 = theta16 + o.w4;
+    P->b1 = theta + o.b1;
+    P->b2 = theta + o.b2;
+    P->b3 = theta + o.b3;
+    P->b4 = theta + o.b4;
+    return CHX_OK;
+}
+
+int chx_mlp_predict(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
+                    const int *chain, int B, float *out, void *stream) {
+    CHX_REQUIRE(P && codes && lnbeta && out && B > 0, "mlp_predict: bad arguments");
+    int grid = B < 148 * 8 ? B : 148 * 8;
+    k_predict<<<grid, 256, predict_smem_bytes(), as_stream(stream)>>>(P, codes, lnbeta, chain, B,
+                                                                      out);
+    CHX_CHECK_LAUNCH("mlp_predict");
+    return CHX_OK;
+}
+
+int64_t chx_mlp_work_bytes(int B, int H) {
+    if (B <= 0 || H <= 0) return -1;
+    const int64_t bh = (int64_t)B * H;
+    return bh * (4 * 4 + 5 * 2) + (int64_t)B * 8 + 12 * 256;
+}
+
+int chx_mlp_grad(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
+                 const int *chain, const float *target, int B, float *y, float *grad,
+                 float *loss, void *work, void *stream) {
+    CHX_REQUIRE(P && codes && lnbeta && target && y && grad && loss && work && B > 0,
+                "mlp_grad: bad arguments");
+    CHX_REQUIRE(mlp_shape_ok(P->nsp, P->D, P->nchain, P->H), "mlp_grad: bad shape");
+    cudaStream_t st = as_stream(stream);
+    const int H = P->H;
+    const long bh = (long)B * H;
+    const MlpOffsets of = mlp_offsets(P->nsp, P->D, P->nchain, H);
+    auto take = [](char *&p, size_t n) {   // 256-byte aligned pieces of work
+        char *r = p;
+        p += (n + 255) / 256 * 256;
+        return r;
+    };
+    char *p = (char *)work;
+    float *Z1 = (float *)take(p, bh * 4), *Z2 = (float *)take(p, bh * 4),
+          *Z3 = (float *)take(p, bh * 4), *dH = (float *)take(p, bh * 4);
+    uint16_t *H1b = (uint16_t *)take(p, bh * 2), *H2b = (uint16_t *)take(p, bh * 2),
+             *H3b = (uint16_t *)take(p, bh * 2);
+    uint16_t *dZa = (uint16_t *)take(p, bh * 2), *dZb = (uint16_t *)take(p, bh * 2);
+    float *dy = (float *)take(p, (size_t)B * 4), *f = (float *)take(p, (size_t)B * 4);
+    if ((int64_t)(p - (char *)work) > chx_mlp_work_bytes(B, H)) {
+        set_error("mlp_grad: work carve-up exceeds chx_mlp_work_bytes");
+        return CHX_ERR_SCRATCH;
+    }
+    const chx_mlp_t Pv = *P;
+    // forward
+    k_l1_fwd<<<B, 256, 0, st>>>(Pv, codes, lnbeta, chain, B, Z1, H1b);
+    gemm(H1b, H, 1, P->W2, H, 1, Z2, H, H2b, P->b2, B, H, H, 1, st);
+    gemm(H2b, H, 1, P->W3, H, 1, Z3, H, H3b, P->b3, B, H, H, 1, st);
+    k_out_fwd<<<(B + 7) / 8, 256, 0, st>>>(Pv, H3b, B, y);
+    // output layer
+    k_out_back<<<B, 256, 0, st>>>(Pv, y, target, B, Z3, dy, dZa);
+    k_loss<<<1, 256, 0, st>>>(y, target, dy, B, grad + of.b4, loss);
+    const int cs = (H + 31) / 32;
+    k_colsum<<<cs, 256, 0, st>>>(H3b, dy, B, H, grad + of.w4);
+    // layer 3: gW3 = H2^T dZ3, gb3, dH2 = dZ3 W3^T
+    gemm(H2b, 1, H, dZa, H, 1, grad + of.W3, H, nullptr, nullptr, H, H, B, 0, st);
+    k_colsum<<<cs, 256, 0, st>>>(dZa, nullptr, B, H, grad + of.b3);
+    gemm(dZa, H, 1, P->W3, 1, H, dH, H, nullptr, nullptr, B, H, H, 0, st);
+    k_relu_back<<<(unsigned)((bh + 255) / 256), 256, 0, st>>>(dH, Z2, bh, dZb);
+    // layer 2
+    gemm(H1b, 1, H, dZb, H, 1, grad + of.W2, H, nullptr, nullptr, H, H, B, 0, st);
+    k_colsum<<<cs, 256, 0, st>>>(dZb, nullptr, B, H, grad + of.b2);
+    gemm(dZb, H, 1, P->W2, 1, H, dH, H, nullptr, nullptr, B, H, H, 0, st);
+    k_relu_back<<<(unsigned)((bh + 255) / 256), 256, 0, st>>>(dH, Z1, bh, dZa);
+    // layer 1
+    k_colsum<<<cs, 256, 0, st>>>(dZa, nullptr, B, H, grad + of.b1);
+    k_normfeat<<<(B + 255) / 256, 256, 0, st>>>(Pv, lnbeta, B, f);
+    k_colsum<<<cs, 256, 0, st>>>(dZa, f, B, H, grad + of.W1 + (int64_t)P->nin * H);
+    k_l1_back<<<2 * P->D + 1, 256, 0, st>>>(Pv, codes, B, dZa, grad + of.W1);
+    if (P->nchain > 0) {
+        if (chain) {
+            k_chain_back<<<P->nchain, 256, 0, st>>>(Pv, chain, B, dZa, grad + of.W1);
+        } else {
+            const int64_t r0 = (int64_t)(P->nin - P->nchain) * H;
+            cudaError_t e = cudaMemsetAsync(grad + of.W1 + r0, 0,
+                                            sizeof(float) * (size_t)P->nchain * H, st);
+            if (e != cudaSuccess) return cuda_fail(e, "mlp_grad memset");
+        }
+    }
+    CHX_CHECK_LAUNCH("mlp_grad");
+    return CHX_OK;
+}
+
+int chx_mlp_adam(float *theta, uint16_t *theta16, const float *grad, float *m, float *v,
+                 int64_t n, float lr, float beta1, float beta2, float eps, int t, void *stream) {
+    CHX_REQUIRE(theta && theta16 && grad && m && v && n > 0 && t >= 1, "mlp_adam: bad arguments");
+    const float c1 = 1.f - powf(beta1, (float)t), c2 = 1.f - powf(beta2, (float)t);
+    k_adam<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(
+        theta, theta16, grad, m, v, (long)n, lr, beta1, beta2, eps, c1, c2);
+    CHX_CHECK_LAUNCH("mlp_adam");
+    return CHX_OK;
+}
+
+}  // extern "C"

@@ -32,6 +32,7 @@
 // The last CTA to finish advances the step counter, so a sequence of blocks
 // is a sequence of identical launches (CUDA-graph capturable).
 #include "chx_device.cuh"
+#include "chx_mlp.cuh"
 
 namespace chx {
 
@@ -42,8 +43,11 @@ constexpr int kMaxSplit = 2;     // threads sharing one bin's taps
 
 // Shared-memory carve-up of one step CTA (all offsets 16-byte aligned).
 struct StepSmem {
-    size_t u, x, tr, dchi, dir, dirv, hist, dn, list, sp, nb, chi, total;
+    size_t u, x, tr, dchi, dir, dirv, hist, dn, list, sp, nb, cd, chi, total;
 };
+
+// salt of the stage-1 uniforms of delayed acceptance
+constexpr uint64_t kDaSalt = 0x6A09E667F3BCC909ULL;
 
 template <typename T>
 static inline size_t al16(size_t n) { return ((n * sizeof(T)) + 15) / 16 * 16; }
@@ -56,8 +60,12 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     int nent = L.ms_nblk ? L.nsp * L.ms_nblk : 0;
     int ndn = L.nshell * L.nsp * L.nsp;
     s.u = o; o += f64 ? al16<double>((size_t)L.nchan * L.ncoef) : al16<float>((size_t)L.nchan * L.ncoef);
-    s.x = o; o += (f64 ? al16<double2>((size_t)kMaxSplit * L.nchan * L.nwin)
-                       : al16<float2>((size_t)kMaxSplit * L.nchan * L.nwin));
+    size_t xs = f64 ? al16<double2>((size_t)kMaxSplit * L.nchan * L.nwin)
+                    : al16<float2>((size_t)kMaxSplit * L.nchan * L.nwin);
+    // the surrogate's scratch (partial sums of every warp + one activation
+    // row, H <= 256) shares the transform's region: they are used in turn
+    if (L.mlp) xs = std::max(xs, al16<float>((size_t)(kStepThreads / 32 + 1) * 256));
+    s.x = o; o += xs;
     s.tr = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.dchi = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.dir = o; o += al16<PairRec>((size_t)2 * maxaff);
@@ -67,6 +75,7 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     s.list = o; o += al16<int>((size_t)(2 * maxaff + 2 * ndn + 2 * nent + 64));
     s.sp = o; o += al16<uint8_t>((size_t)L.natoms);
     s.nb = o; o += al16<uint16_t>((size_t)2 * std::max(L.ms_D, 1));
+    s.cd = o; o += al16<uint8_t>((size_t)((L.mlp || L.log_cap > 0) ? 2 * L.feat_D + 1 : 1));
     s.chi = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.total = o;
     return s;
@@ -342,6 +351,88 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real
     __syncthreads();
 }
 
+// Stage 1 of delayed acceptance for a swap of a and b (species differ),
+// run by every thread of the step CTA: the surrogate's input (sites lo < hi,
+// their neighbourhoods in the feature order, code NSP for lo and hi
+// themselves) into s_codes and the orientation sign into *s_sigma; with the
+// screen on, the prediction d^ (*s_dhat), the exact prior change, and the
+// stage-1 test min(1, exp(-beta nfit d^ - E)) with its own uniform stream.
+// Returns 1 when the screen rejects the move (then recorded as rejected).
+template <int NSP>
+__device__ __noinline__ int da_stage1(const chx_ladder_t &L, const chx_mlp_t &M,
+                                      const uint8_t *s_sp, uint8_t *s_codes, float *s_mpart,
+                                      float *s_mh, double *s_de, uint64_t step, int rung, int st,
+                                      int a, int b, int nsa, int nsb, bool da_on, float lnb,
+                                      float *s_sigma, double *s_dhat, double *s_dast,
+                                      int *s_skip, int *err) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int natoms = L.natoms, z = L.ncoord, nn = NSP * NSP;
+    auto spc = [s_sp](int i) { return (int)(s_sp[i] & 0x7F); };
+    {
+        const int lo = a < b ? a : b, hi = a < b ? b : a, D = L.feat_D;
+        for (int k = tid; k < 2 * D; k += blockDim.x) {
+            const int half = k >= D;
+            const int site = __ldg(&L.feat_nbr[(long)(half ? hi : lo) * D + (k - half * D)]);
+            int code = NSP;
+            if ((unsigned)site >= (unsigned)natoms) atomicOr(err, CHX_DEVERR_INDEX);
+            else if (site != a && site != b) code = spc(site);
+            s_codes[1 + k] = (uint8_t)code;
+        }
+        if (tid == 0) {
+            const int p = spc(lo), q = spc(hi);
+            s_codes[0] = (uint8_t)pair_row(p, q, NSP);
+            *s_sigma = p < q ? 1.f : -1.f;
+        }
+        __syncthreads();
+    }
+    if (!da_on) return 0;
+    const float net = mlp_eval_cta(M, s_codes, lnb, L.slot0 + rung, s_mpart, s_mh);
+    if (L.etab) {   // exact prior change of the swap, in both stages
+        double de1 = 0.0;
+        for (int q = tid; q < 4 * z; q += blockDim.x) {
+            const int blk = q / z, o = q - blk * z;
+            const int site = (blk < 2) ? a : b, pf = site * z + o;
+            const int jn = L.jidx[pf];
+            if ((unsigned)jn >= (unsigned)natoms) continue;   // flagged by the pair phase
+            if (blk >= 2 && jn == a) continue;
+            const int i = (blk & 1) ? jn : site, j = (blk & 1) ? site : jn;
+            const int si = spc(i), sj = spc(j);
+            const int ni_ = (i == a) ? nsa : ((i == b) ? nsb : si);
+            const int nj_ = (j == a) ? nsa : ((j == b) ? nsb : sj);
+            const int sh = L.shell[pf];
+            de1 += L.etab[sh * nn + ni_ * NSP + nj_] - L.etab[sh * nn + si * NSP + sj];
+        }
+        de1 = warp_sum(de1);
+        if (lane == 0) s_de[warp] = de1;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const double beta = L.beta_rung[rung];
+        const double dh = (double)*s_sigma * (double)M.out_scale * (double)net;
+        double x1 = beta * dh * L.nfit;
+        if (L.etab) {
+            double d = 0.0;
+            for (int w = 0; w < (int)(blockDim.x / 32); ++w) d += s_de[w];
+            x1 += L.energy_beta * d;
+        }
+        const uint64_t h = splitmix64(splitmix64(L.seed ^ kDaSalt) ^
+                                      (step * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)rung << 32));
+        const double u1 = u01(splitmix64(h));
+        const int pass = (x1 <= 0.0) || (u1 < exp(-fmin(x1, 60.0)));
+        *s_dhat = dh;
+        *s_skip = !pass;
+        s_dast[0] += 1.0;
+        if (pass) {
+            s_dast[1] += 1.0;
+        } else {
+            L.acc_rung[rung] = 0;
+            if (L.acc_log) L.acc_log[(long)st * L.nrep + rung] = 0;
+        }
+    }
+    __syncthreads();
+    return *s_skip;
+}
+
 template <int NSP, int PREC, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restrict__ Ls,
                                                          const int *__restrict__ slot_ladder,
@@ -359,6 +450,11 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     __shared__ double s_num[32], s_den[32], s_sq[40], s_scale[8], s_de[NT / 32];
     __shared__ double s_c2;
     __shared__ int s_msb[NSP + 1];
+    __shared__ chx_mlp_t s_mlp;
+    __shared__ double s_dhat, s_dast[4];
+    __shared__ float s_sigma;
+    __shared__ int s_daon, s_skip;
+    __shared__ long long s_logi;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int slot = blockIdx.x;
@@ -389,11 +485,17 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     uint8_t *s_sp = (uint8_t *)(smem + so.sp);
     uint16_t *s_nb = (uint16_t *)(smem + so.nb);
     double *s_chi = (double *)(smem + so.chi);
+    uint8_t *s_codes = (uint8_t *)(smem + so.cd);
+    float *s_mpart = (float *)(smem + so.x);       // surrogate scratch, shares the
+    float *s_mh = s_mpart + (NT / 32) * 256;       // transform's region
     auto spc = [s_sp](int i) { return (int)(s_sp[i] & 0x7F); };
 
     if (tid == 0) {
         s_base = *(volatile uint64_t *)stepc;
         s_rung = L.rung_of[c];
+        s_daon = L.mlp != nullptr && L.da_on != nullptr && *L.da_on != 0;
+        if (s_daon) s_mlp = *L.mlp;
+        for (int q = 0; q < 4; ++q) s_dast[q] = 0.0;
     }
     if (tid <= NSP) s_msb[tid] = 0;
     for (int i = tid; i < natoms; i += blockDim.x)
@@ -403,6 +505,9 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     __syncthreads();
     const bool use_tab = (PREC != CHX_FP64) && L.sstab32 != nullptr;
     const float *msT32 = L.ms_T32;
+    const bool da_on = s_daon != 0;
+    const bool log_on = L.log_cap > 0 && L.log_codes != nullptr && L.log_y != nullptr;
+    const float lnb = logf((float)L.beta_rung[s_rung]);
 
     for (int st = 0; st < nsteps; ++st) {
         // ---- 1. proposal (one thread)
@@ -415,6 +520,18 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         for (int e = tid; e < ndn; e += blockDim.x) s_dn[e] = 0;
         __syncthreads();
         const int a = prop.a, b = prop.b, nsa = prop.nsa, nsb = prop.nsb, swp = prop.swap;
+
+        // ---- 1b. delayed acceptance, stage 1 (features, prediction, screen)
+        const bool feat = swp && (da_on || log_on) && spc(a) != spc(b);
+        int skip = 0;
+        if (feat)
+            skip = da_stage1<NSP>(L, s_mlp, s_sp, s_codes, s_mpart, s_mh, s_de, s_step, s_rung, st,
+                                  a, b, nsa, nsb, da_on, lnb, &s_sigma, &s_dhat, s_dast, &s_skip,
+                                  err);
+        if (skip) {   // rejected by the screen: the state is unchanged
+            __syncthreads();
+            continue;
+        }
 
         // ---- 2. affected pairs: old/new terms, table counts or direct records.
         // Pair q of block blk is site -> neighbour (even blocks) or
@@ -640,10 +757,24 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             double c2 = s_c2;
             int rung = s_rung;
             double x = L.beta_rung[rung] * (c2 - L.chi2[c]) * L.nfit;
-            if (L.etab) {
+            if (feat && da_on) {
+                // stage 2 of delayed acceptance: the surrogate's error alone
+                // (the prior's change cancels between the two stages)
+                x -= L.beta_rung[rung] * s_dhat * L.nfit;
+                s_dast[3] += x <= 0.0 ? 1.0 : exp(-fmin(x, 60.0));   // stage-2 probability
+            } else if (L.etab) {
                 double d = 0.0;
                 for (int w = 0; w < (int)(blockDim.x / 32); ++w) d += s_de[w];
                 x += L.energy_beta * d;
+            }
+            if (feat && log_on) {
+                const long long li = (long long)(((s_step - 1) * (uint64_t)L.nrep + (uint64_t)c) %
+                                                 (uint64_t)L.log_cap);
+                L.log_y[4 * li] = s_sigma * (float)(c2 - L.chi2[c]);
+                L.log_y[4 * li + 1] = lnb;
+                L.log_y[4 * li + 2] = (float)(L.slot0 + rung);    // chain: ladder and rung
+                L.log_y[4 * li + 3] = (float)s_step;
+                s_logi = li;
             }
             double u;
             long ui = (long)(s_step - 1);
@@ -656,11 +787,18 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 u = u01(splitmix64(h));
             }
             int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
+            if (feat && da_on && acc) s_dast[2] += 1.0;
             s_acc = acc;
             L.acc_rung[rung] = (uint8_t)acc;
             if (L.acc_log) L.acc_log[(long)st * L.nrep + rung] = (uint8_t)acc;
         }
         __syncthreads();
+
+        if (feat && log_on) {
+            const int nsite = 2 * L.feat_D + 1;
+            uint8_t *dst = L.log_codes + s_logi * nsite;
+            for (int k = tid; k < nsite; k += blockDim.x) dst[k] = s_codes[k];
+        }
 
         // ---- 7. commit
         if (s_acc) {
@@ -697,6 +835,8 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         __syncthreads();
     }  // steps
     for (int q = tid; q < NSP * nk; q += blockDim.x) CHg[q] = s_chi[q];
+    if (da_on && tid == 0 && L.da_stat)
+        for (int q = 0; q < 4; ++q) L.da_stat[(long)c * 4 + q] += s_dast[q];
     __syncthreads();
 
     // ---- the last CTA of the launch advances the step counter
@@ -992,15 +1132,20 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
                         L.nkw <= 3 && L.nchan == L.nsp * L.nkw && (L.nfft & (L.nfft - 1)) == 0 &&
                         L.natoms < (1 << 20) && L.nwin > 0,
                     "sampler: ladder %d outside the built limits", i);
+        CHX_REQUIRE(!L.mlp || (L.da_on && L.da_stat),
+                    "sampler: ladder %d has a surrogate but no da_on word or da_stat", i);
+        CHX_REQUIRE(!(L.mlp || L.log_cap > 0) ||
+                        (L.feat_nbr && L.feat_D > 0 && L.feat_D <= 127 &&
+                         (L.log_cap == 0 || (L.log_codes && L.log_y && L.log_cap > 0))),
+                    "sampler: ladder %d has an incomplete surrogate feature set or swap log", i);
         StepSmem s = step_smem(L, precision);
         // field sizes of this ladder, then the running maximum of each
-        // field sizes of this ladder, then the running maximum of each
-        size_t f[12] = {s.x - s.u, s.tr - s.x, s.dchi - s.tr, s.dir - s.dchi, s.dirv - s.dir,
+        size_t f[13] = {s.x - s.u, s.tr - s.x, s.dchi - s.tr, s.dir - s.dchi, s.dirv - s.dir,
                         s.hist - s.dirv, s.dn - s.hist, s.list - s.dn, s.sp - s.list,
-                        s.nb - s.sp, s.chi - s.nb, s.total - s.chi};
-        size_t *g[12] = {&mx.u, &mx.x, &mx.tr, &mx.dchi, &mx.dir, &mx.dirv, &mx.hist, &mx.dn,
-                         &mx.list, &mx.sp, &mx.nb, &mx.chi};
-        for (int q = 0; q < 12; ++q) *g[q] = std::max(*g[q], f[q]);
+                        s.nb - s.sp, s.cd - s.nb, s.chi - s.cd, s.total - s.chi};
+        size_t *g[13] = {&mx.u, &mx.x, &mx.tr, &mx.dchi, &mx.dir, &mx.dirv, &mx.hist, &mx.dn,
+                         &mx.list, &mx.sp, &mx.nb, &mx.cd, &mx.chi};
+        for (int q = 0; q < 13; ++q) *g[q] = std::max(*g[q], f[q]);
     }
     // mx holds field sizes; turn them into offsets
     StepSmem o;
@@ -1016,6 +1161,7 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
     o.list = at; at += mx.list;
     o.sp = at; at += mx.sp;
     o.nb = at; at += mx.nb;
+    o.cd = at; at += mx.cd;
     o.chi = at; at += mx.chi;
     o.total = at;
     CHX_REQUIRE(at <= 220 * 1024, "sampler: %zu bytes of shared memory needed", at);

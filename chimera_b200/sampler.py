@@ -276,11 +276,16 @@ class Ladders:
         return b
 
     def _upload(self):
+        """Copy the host descriptors to the device, into the same buffer once
+        it exists (so a captured graph keeps a valid address)."""
         import torch
         raw = bytes(C.string_at(C.addressof(self.host), C.sizeof(self.host)))
-        dev = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to("cuda")
-        self.d_ladders = dev
-        return dev
+        src = torch.frombuffer(bytearray(raw), dtype=torch.uint8)
+        if getattr(self, "d_ladders", None) is None or self.d_ladders.numel() != src.numel():
+            self.d_ladders = src.to("cuda")
+        else:
+            self.d_ladders.copy_(src)
+        return self.d_ladders
 
     def set_field(self, li, name, value):
         setattr(self.host[li], name, value)
@@ -380,6 +385,104 @@ class Ladders:
 
     def device_error(self):
         return int(self.err.item())
+
+    # ------------------------------------------------ surrogate and swap log
+    def feature_table(self, li):
+        """Ladder li's (natoms, D) feature neighbourhoods (built once)."""
+        b, L = self.bufs[li], self.host[li]
+        if "feat_nbr" not in b:
+            from .surrogate import feature_neighbours
+            fm = self.specs[li].fm
+            nbr = feature_neighbours(_host(fm.cell.ideal), fm.i_idx, fm.j_idx,
+                                     _host(fm.d_shift), L.ncoord)
+            b["feat_nbr"] = self._t(nbr)
+            b["feat_nbr_host"] = nbr
+            L.feat_nbr, L.feat_D = N.dptr(b["feat_nbr"]), int(nbr.shape[1])
+        return b["feat_nbr_host"]
+
+    def _da_buffers(self, li):
+        b = self.bufs[li]
+        if "da_on" not in b:
+            b["da_on"] = self._t(np.zeros(1, np.int32))
+            b["da_stat"] = self._t(np.zeros((self.specs[li].nrep, 4)))
+            L = self.host[li]
+            L.da_on, L.da_stat = N.dptr(b["da_on"]), N.dptr(b["da_stat"])
+        return b
+
+    def attach_surrogate(self, sur, ladders=None, on=True):
+        """Screen the swaps of the given ladders (default all) with `sur`
+        (a surrogate.SwapSurrogate), screening on or off. Changes the step
+        kernel's shared-memory plan: recapture graphs afterwards."""
+        for li in (range(self.nladders) if ladders is None else ladders):
+            self.feature_table(li)
+            assert sur.D == self.host[li].feat_D and sur.nsp == self.nsp, "surrogate shape"
+            b = self._da_buffers(li)
+            b["da_on"].fill_(1 if on else 0)
+            self.host[li].mlp = sur.device_ptr
+        self._surrogate = sur
+        self._upload()
+
+    def detach_surrogate(self):
+        for li in range(self.nladders):
+            self.host[li].mlp = 0
+        self._upload()
+
+    def set_screening(self, li, on):
+        """Switch ladder li's screen on or off (a device word: no re-plan,
+        captured graphs stay valid)."""
+        self._da_buffers(li)["da_on"].fill_(1 if on else 0)
+
+    def screening_on(self):
+        return [bool(int(b["da_on"].item())) if "da_on" in b else False for b in self.bufs]
+
+    def da_stats(self, reset=False):
+        """(nladders, 4) summed over each ladder's slots: moves screened,
+        moves passed to the exact stage, moves accepted there, and the sum of
+        the stage-2 acceptance probabilities of the passed moves."""
+        out = np.zeros((self.nladders, 4))
+        for li, b in enumerate(self.bufs):
+            if "da_stat" in b:
+                out[li] = _host(b["da_stat"]).sum(0)
+                if reset:
+                    b["da_stat"].zero_()
+        return out
+
+    def enable_log(self, cap, ladders=None):
+        """Log the swaps of the given ladders (default all) that are evaluated
+        exactly: features, sigma * d, ln beta, chain and step into a ring of
+        `cap` entries each."""
+        torch = self.torch
+        for li in (range(self.nladders) if ladders is None else ladders):
+            self.feature_table(li)
+            b, L = self.bufs[li], self.host[li]
+            b["log_codes"] = torch.zeros((int(cap), 2 * L.feat_D + 1), dtype=torch.uint8,
+                                         device="cuda")
+            b["log_y"] = torch.full((int(cap), 4), float("nan"), dtype=torch.float32,
+                                    device="cuda")
+            self.keep += [b["log_codes"], b["log_y"]]
+            L.log_codes, L.log_y, L.log_cap = N.dptr(b["log_codes"]), N.dptr(b["log_y"]), int(cap)
+        self._upload()
+
+    def disable_log(self):
+        for L in self.host:
+            L.log_cap = 0
+        self._upload()
+
+    def swap_log(self, ladders=None, extra=False):
+        """(codes, lnbeta, y) of the logged swaps (device tensors); with
+        extra, also (chain, step) of each."""
+        torch = self.torch
+        cs, rows = [], []
+        for li in (range(self.nladders) if ladders is None else ladders):
+            b = self.bufs[li]
+            if "log_y" not in b:
+                continue
+            ok = torch.isfinite(b["log_y"][:, 0])
+            cs.append(b["log_codes"][ok])
+            rows.append(b["log_y"][ok])
+        y = torch.cat(rows)
+        out = (torch.cat(cs), y[:, 1].contiguous(), y[:, 0].contiguous())
+        return out + (y[:, 2].long(), y[:, 3].long()) if extra else out
 
 
 class RMCSampler:
@@ -711,11 +814,60 @@ class BatchedSampler:
             self.graph.replay()
             self.blocks += 1
             self.steps += self.exchange_every
-            if self.reanchor_every and self.blocks % self.check_every == 0:
-                due = self.lad.accepted_since_anchor() >= self.reanchor_every
-                if bool(due.any()):
-                    self.lad.reanchor(due)
-                    self.reanchors += 1
+            if self.blocks % self.check_every == 0:
+                if self.reanchor_every:
+                    due = self.lad.accepted_since_anchor() >= self.reanchor_every
+                    if bool(due.any()):
+                        self.lad.reanchor(due)
+                        self.reanchors += 1
+                if self.surrogate is not None:
+                    self._check_screen()
+
+    # ------------------------------------------------- delayed acceptance
+    surrogate = None
+    da_max_err = 0.8        # screening error above which a ladder stops screening
+    fallbacks = 0
+
+    def learn(self, blocks=40, epochs=4, H=256, lr=1e-3, seed=0, batch=4096, cap=None):
+        """Log the swaps of `blocks` exchange periods of plain steps, train a
+        surrogate on them (chimera_b200.surrogate) with one input row per
+        chain (ladder and rung), and switch every ladder to delayed
+        acceptance. Returns the training report."""
+        from .surrogate import SwapSurrogate
+        lad = self.lad
+        cap = int(cap or self.exchange_every * blocks * max(s.nrep for s in lad.specs))
+        lad.enable_log(cap)
+        self.graph = None
+        self.run_blocks(blocks)
+        codes, lnb, y, chain, _ = lad.swap_log(extra=True)
+        lad.disable_log()
+        D = lad.host[0].feat_D
+        if self.surrogate is None or self.surrogate.H != H or self.surrogate.nchain != lad.nslots:
+            self.surrogate = SwapSurrogate(lad.nsp, D, H=H, nchain=lad.nslots, seed=seed)
+        rep = self.surrogate.fit(codes, lnb, y, chain=chain, epochs=epochs, lr=lr, seed=seed,
+                                 batch=batch)
+        lad.attach_surrogate(self.surrogate)
+        lad.da_stats(reset=True)
+        self.graph = None
+        self.train_report = rep
+        return rep
+
+    def _check_screen(self):
+        """Ladders whose screening error since the last check exceeds
+        da_max_err go back to plain steps. The screening error is the mean
+        stage-2 rejection probability of the moves the screen let through,
+        1 - mean min(1, exp(-beta nfit (d - d^))): 0 for an exact screen,
+        the plain rejection rate for a screen that passes everything, the
+        share of exact evaluations the screen could have saved."""
+        st = self.lad.da_stats(reset=True)
+        on = self.lad.screening_on()
+        for li in range(self.lad.nladders):
+            if on[li] and st[li, 1] > 0:
+                err = 1.0 - st[li, 3] / st[li, 1]
+                if err > self.da_max_err:
+                    self.lad.set_screening(li, False)
+                    self.fallbacks += 1
+        self.last_screen = st
 
     def best(self, li):
         b = self.lad.bufs[li]

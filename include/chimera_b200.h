@@ -52,7 +52,8 @@ extern "C" {
 CHX_API int chx_version(void);
 /* sizeof / offsetof of the ABI structs, for binding self-checks:
  * 0 sizeof(chx_pairs_t), 1 sizeof(chx_ladder_t),
- * 2 offsetof(chx_ladder_t, exch_acc), 3 offsetof(chx_ladder_t, seed) */
+ * 2 offsetof(chx_ladder_t, exch_acc), 3 offsetof(chx_ladder_t, seed),
+ * 4 sizeof(chx_mlp_t), 5 offsetof(chx_ladder_t, log_cap) */
 CHX_API int64_t chx_struct_size(int which);
 CHX_API int chx_last_error(char *buf, int n);
 
@@ -197,6 +198,59 @@ CHX_API int chx_ms_chi_of(const int *counts, const double *T, int nconf, int nsp
  *    never moves, and every rung keeps its own proposal and acceptance
  *    streams (keyed by rung), exactly as when the reference moves the state.
  * ------------------------------------------------------------------------ */
+/* The swap surrogate (A11, no reference counterpart): a BF16 MLP with FP32
+ * accumulation, 3 hidden ReLU layers of H units, one linear output.
+ * Input of a swap of sites lo < hi with species p = S[lo] != q = S[hi]:
+ * one-hot row 0..npt-1 the unordered species pair {p, q} (npt =
+ * nsp(nsp-1)/2), then for k < 2D (the D neighbours of lo, then of hi, in the
+ * feature order) the row npt + k (nsp + 1) + code, code the neighbour's
+ * species or nsp where the neighbour is lo or hi; then, when nchain > 0, the
+ * row npt + 2D (nsp + 1) + chain of the chain the move belongs to (chain =
+ * slot0 + rung in the sampler: ladder and temperature, constant within a
+ * step, so a move and its reverse still share the input); plus the scalar
+ * feature (ln beta - feat_shift) * feat_scale on row nin. Prediction
+ * d^ = sigma * out_scale * net, sigma = +1 if p < q else -1: a swap and its
+ * reverse have the same input and opposite predictions, which keeps the
+ * two-stage acceptance exact.
+ * Parameters live in one FP32 buffer (the masters) and a BF16 copy with the
+ * same layout: W1 (nin+1, H) | b1 (H) | W2 (H, H) | b2 | W3 (H, H) | b3 |
+ * w4 (H) | b4 (1); row-major [in][out]; compute reads BF16 weights and FP32
+ * biases. */
+typedef struct chx_mlp {
+    int nsp, D, H, nin;              /* nin = npt + 2 D (nsp + 1) + nchain      */
+    const uint16_t *W1, *W2, *W3, *w4;   /* BF16 bit patterns */
+    const float *b1, *b2, *b3, *b4;
+    float out_scale, feat_shift, feat_scale;
+    int nchain;                      /* chain rows (0: no chain input)          */
+} chx_mlp_t;
+
+/* Parameter count of the layout above. */
+CHX_API int64_t chx_mlp_nparam(int nsp, int D, int nchain, int H);
+/* Fill the descriptor's pointers for a parameter buffer theta (FP32) and its
+ * BF16 copy theta16 (device pointers, same layout). */
+CHX_API int chx_mlp_bind(chx_mlp_t *P, int nsp, int D, int nchain, int H, const float *theta,
+                         const uint16_t *theta16);
+/* Surrogate output for B samples, the same code the sampler step runs:
+ * codes (B, 1 + 2D) as above (code[0] the pair row), lnbeta (B), chain (B)
+ * (NULL: no chain row); out (B) the network output net (before sigma and
+ * out_scale). P is a device pointer. */
+CHX_API int chx_mlp_predict(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
+                            const int *chain, int B, float *out, void *stream);
+/* Training forward (tensor-core GEMMs over the batch), loss and gradient:
+ * loss = mean (net - target)^2; grad (nparam, FP32) overwritten; y (B) the
+ * batch outputs; chain (B) sorted ascending (the chain rows' gradient is
+ * summed per run of equal chains, in order), or NULL; work:
+ * chx_mlp_work_bytes(B, H). P is a HOST descriptor. */
+CHX_API int64_t chx_mlp_work_bytes(int B, int H);
+CHX_API int chx_mlp_grad(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
+                         const int *chain, const float *target, int B, float *y, float *grad,
+                         float *loss, void *work, void *stream);
+/* One Adam step (bias-corrected, step number t >= 1) on the FP32 masters,
+ * then the BF16 copy: theta -= lr * mhat / (sqrt(vhat) + eps). */
+CHX_API int chx_mlp_adam(float *theta, uint16_t *theta16, const float *grad, float *m, float *v,
+                         int64_t n, float lr, float beta1, float beta2, float eps, int t,
+                         void *stream);
+
 typedef struct {
     /* topology and tables of this ladder's supercell */
     int natoms, ncoord, npairs, nshell, nsp, nk;
@@ -263,6 +317,27 @@ typedef struct {
                                         launch, by rung, or NULL                     */
     int *n_acc;                      /* (nrep) accepted moves per slot            */
     int *exch_att, *exch_acc;        /* (nrep) exchange bookkeeping per rung pair */
+    /* delayed acceptance (no reference counterpart; mlp NULL when off): a
+       surrogate predicts each swap's chi^2 change d^ from the species around
+       the two sites; stage 1 accepts with min(1, exp(-beta nfit d^ - E)),
+       E the exact prior change, and only a move that passes is evaluated
+       exactly and accepted with min(1, exp(-beta nfit (d - d^))). */
+    const struct chx_mlp *mlp;       /* device descriptor of the surrogate, or NULL */
+    const int *feat_nbr;             /* (natoms, feat_D) neighbours of each site in
+                                        one translation-invariant order            */
+    int feat_D;
+    const int *da_on;                /* (1) device word: 1 screens, 0 plain steps  */
+    double *da_stat;                 /* (nrep, 4) per slot: moves screened, moves
+                                        passed to the exact stage, moves accepted
+                                        there, sum of the stage-2 acceptance
+                                        probability min(1, exp(-beta nfit (d - d^))) */
+    /* swap log for training the surrogate, log_cap 0 when off: every swap
+       evaluated exactly writes its features and sigma*d at entry
+       ((step - 1) * nrep + slot) mod log_cap */
+    uint8_t *log_codes;              /* (log_cap, 1 + 2 feat_D)                  */
+    float *log_y;                    /* (log_cap, 4): sigma * d, ln beta, chain
+                                        (slot0 + rung), step                     */
+    int64_t log_cap;
 } chx_ladder_t;
 
 /* Bytes of dynamic shared memory the step kernel needs for these ladders. */

@@ -222,6 +222,9 @@ class PlainSampler:
             x = x + p.energy_beta * (d * valid).sum(axis=1)
         u = self.urng.random(n)
         acc = (x <= 0) | (u < np.exp(-np.minimum(x, 60.0)))
+        # the step's proposals and exact chi^2 changes, by rung (read by tests)
+        self.last = dict(a=a.copy(), b=b.copy(), swap=isswap.copy(), species=self.species.copy(),
+                         d=c2 - self.chi2)
         accb = acc.astype(np.uint8)
         if dC is not None:
             self.C = self.C + dC * acc[:, None]
