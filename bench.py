@@ -330,6 +330,13 @@ def main():
     d2h = NPOS * (prob.cell.natoms * 4 + 8)
     e2e_val = smp2.nslots * EXCH * (e2e_blocks + 1) / e2e_dt
     err = smp.lad.device_error()
+    best_all = np.array([[b[1]] for b in best])
+    if world > 1:
+        # the one collective of the sharded run: per-ladder summaries (ladders
+        # rank * NPOS + i live on rank `rank`), after the timed region
+        from chimera_b200.shard import gather_summaries
+        parts = [[r * NPOS + i for i in range(NPOS)] for r in range(world)]
+        best_all = gather_summaries(best_all, world * NPOS, parts)
 
     if rank == 0:
         cpu = None
@@ -359,7 +366,8 @@ def main():
             "device_error": err,
             "reanchors": smp.reanchors,
             "autotune": tuning,
-            "best_chi2_min": min(b[1] for b in best),
+            "best_chi2_min": float(np.nanmin(best_all)),
+            "ladders": int(best_all.shape[0]),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

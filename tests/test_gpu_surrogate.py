@@ -245,3 +245,30 @@ def test_bad_screen_falls_back_to_plain_steps(cuda):
     assert bs.fallbacks >= 1
     assert bs.lad.screening_on() == [False, False]
     assert bs.lad.device_error() == 0
+
+
+def test_learned_screen_saves_exact_evaluations(cuda):
+    """After learning from its own logged swaps (one input row per chain),
+    the screen sends a third or more of the swaps of a warm ladder back
+    before the exact path sum, transform and chi^2, with a screening error
+    below the fallback threshold, so every ladder keeps screening."""
+    from chimera_b200 import configs
+    from chimera_b200.sampler import BatchedSampler, LadderSpec
+    prob = configs.Problem(ncell=(10, 10, 10))
+    specs = []
+    for p in range(16):
+        pos = prob.position(p)
+        specs.append(LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R, nrep=32,
+                                tmin=0.05, tmax=0.5, seed=p, swap_frac=1.0, ms_library=prob.ms))
+    bs = BatchedSampler(specs, precision=1, exchange_every=25, reanchor_every=0, check_every=10)
+    bs.init_state([prob.random_config(p) for p in range(16)], prob.cell.ideal)
+    bs.run_blocks(20)
+    rep = bs.learn(blocks=40, epochs=8, H=64)
+    assert rep["rmse_d"] < 0.7 * rep["std_d"], rep
+    bs.run_blocks(20)
+    st = bs.last_screen.sum(0)
+    passed, err = st[1] / st[0], 1.0 - st[3] / st[1]
+    print(f"pass {passed:.3f} screening error {err:.3f} fit {rep['rmse_d'] / rep['std_d']:.3f}")
+    assert passed < 0.75 and err < bs.da_max_err
+    assert all(bs.lad.screening_on()) and bs.fallbacks == 0
+    assert bs.lad.device_error() == 0
