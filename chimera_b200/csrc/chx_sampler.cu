@@ -433,7 +433,9 @@ __device__ __noinline__ int da_stage1(const chx_ladder_t &L, const chx_mlp_t &M,
     return *s_skip;
 }
 
-template <int NSP, int PREC, int NT, int MINB>
+// DA: built with the delayed-acceptance screen and the swap log (a ladder of
+// the launch has a surrogate or a log); without it those paths compile away.
+template <int NSP, int PREC, int NT, int MINB, bool DA>
 __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restrict__ Ls,
                                                          const int *__restrict__ slot_ladder,
                                                          int nslots, int nsteps, StepSmem so,
@@ -493,7 +495,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     if (tid == 0) {
         s_base = *(volatile uint64_t *)stepc;
         s_rung = L.rung_of[c];
-        s_daon = L.mlp != nullptr && L.da_on != nullptr && *L.da_on != 0;
+        s_daon = DA && L.mlp != nullptr && L.da_on != nullptr && *L.da_on != 0;
         if (s_daon) s_mlp = *L.mlp;
         for (int q = 0; q < 4; ++q) s_dast[q] = 0.0;
     }
@@ -505,8 +507,8 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     __syncthreads();
     const bool use_tab = (PREC != CHX_FP64) && L.sstab32 != nullptr;
     const float *msT32 = L.ms_T32;
-    const bool da_on = s_daon != 0;
-    const bool log_on = L.log_cap > 0 && L.log_codes != nullptr && L.log_y != nullptr;
+    const bool da_on = DA && s_daon != 0;
+    const bool log_on = DA && L.log_cap > 0 && L.log_codes != nullptr && L.log_y != nullptr;
     const float lnb = logf((float)L.beta_rung[s_rung]);
 
     for (int st = 0; st < nsteps; ++st) {
@@ -1077,31 +1079,45 @@ __global__ void k_shell_table(chx_ladder_t L, const double *__restrict__ rshell,
     }
 }
 
-template <int NSP, int PREC, int NT, int MINB>
+template <int NSP, int PREC, int NT, int MINB, bool DA>
 static int launch_step_nt(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
                           int nsteps, const StepSmem &so, size_t smem, uint64_t *d_stepc,
                           int *d_ticket, int *d_err, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_step<NSP, PREC, NT, MINB>,
+    cudaError_t e = cudaFuncSetAttribute(k_step<NSP, PREC, NT, MINB, DA>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(e, "sampler_step attribute");
-    k_step<NSP, PREC, NT, MINB><<<nslots, NT, smem, st>>>(d_ladders, slot_ladder, nslots, nsteps,
-                                                          so, d_stepc, d_ticket, d_err);
+    k_step<NSP, PREC, NT, MINB, DA><<<nslots, NT, smem, st>>>(d_ladders, slot_ladder, nslots,
+                                                              nsteps, so, d_stepc, d_ticket,
+                                                              d_err);
     CHX_CHECK_LAUNCH("sampler_step");
     return CHX_OK;
+}
+
+template <int NSP, int PREC, bool DA>
+static int launch_step_da(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
+                          int nsteps, int threads, int min_blocks, const StepSmem &so,
+                          size_t smem, uint64_t *d_stepc, int *d_ticket, int *d_err,
+                          cudaStream_t st) {
+    if (threads == 128)
+        return launch_step_nt<NSP, PREC, 128, 6, DA>(d_ladders, slot_ladder, nslots, nsteps, so,
+                                                     smem, d_stepc, d_ticket, d_err, st);
+    if (min_blocks == 4)
+        return launch_step_nt<NSP, PREC, 256, 4, DA>(d_ladders, slot_ladder, nslots, nsteps, so,
+                                                     smem, d_stepc, d_ticket, d_err, st);
+    return launch_step_nt<NSP, PREC, 256, 3, DA>(d_ladders, slot_ladder, nslots, nsteps, so,
+                                                 smem, d_stepc, d_ticket, d_err, st);
 }
 
 template <int NSP, int PREC>
 static int launch_step(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
                        int nsteps, int threads, int min_blocks, const StepSmem &so, size_t smem,
-                       uint64_t *d_stepc, int *d_ticket, int *d_err, cudaStream_t st) {
-    if (threads == 128)
-        return launch_step_nt<NSP, PREC, 128, 6>(d_ladders, slot_ladder, nslots, nsteps, so,
-                                                 smem, d_stepc, d_ticket, d_err, st);
-    if (min_blocks == 4)
-        return launch_step_nt<NSP, PREC, 256, 4>(d_ladders, slot_ladder, nslots, nsteps, so,
-                                                 smem, d_stepc, d_ticket, d_err, st);
-    return launch_step_nt<NSP, PREC, 256, 3>(d_ladders, slot_ladder, nslots, nsteps, so, smem,
-                                             d_stepc, d_ticket, d_err, st);
+                       uint64_t *d_stepc, int *d_ticket, int *d_err, bool da, cudaStream_t st) {
+    if (da)
+        return launch_step_da<NSP, PREC, true>(d_ladders, slot_ladder, nslots, nsteps, threads,
+                                               min_blocks, so, smem, d_stepc, d_ticket, d_err,
+                                               st);
+    return launch_step_da<NSP, PREC, false>(d_ladders, slot_ladder, nslots, nsteps, threads,
+                                            min_blocks, so, smem, d_stepc, d_ticket, d_err, st);
 }
 
 template <int NSP, int PREC>
@@ -1217,9 +1233,12 @@ int chx_sampler_step(const chx_ladder_t *d_ladders, const chx_ladder_t *host_lad
     if (rc != CHX_OK) return rc;
     cudaStream_t st = as_stream(stream);
     int nsp = host_ladders[0].nsp;
+    bool da = false;
+    for (int i = 0; i < nladders; ++i)
+        da = da || host_ladders[i].mlp != nullptr || host_ladders[i].log_cap > 0;
 #define CHX_STEP(N, PR) \
     launch_step<N, PR>(d_ladders, slot_ladder, nslots, nsteps, threads, min_blocks, so, smem, \
-                       d_stepc, d_ticket, d_err, st)
+                       d_stepc, d_ticket, d_err, da, st)
     if (precision == CHX_FP64) {
         switch (nsp) {
             case 2: return CHX_STEP(2, CHX_FP64);
