@@ -1,14 +1,302 @@
-// chx_ft_tc.cu -- split-BF16 FT contraction on the tcgen05 tensor cores.
+// chx_ft_tc.cu -- the windowed FT contraction out = chi . B on the tcgen05
+// tensor cores (A5, precision 2 of chx_ft_batch).
+//
+// Each FP64 operand x is split into two BF16 numbers, x_hi = bf16(x) and
+// x_lo = bf16(x - x_hi); a product a.b is taken as a_hi b_hi + a_hi b_lo +
+// a_lo b_hi (the a_lo b_lo term is below 2^-16 of it), three BF16 MMAs with
+// FP32 accumulation in tensor memory, which keeps about 16 significant bits
+// per product where one BF16 product keeps 8.
+//
+// Layout. A pre-pass (k_tc_split) writes the hi and lo parts of chi (rows x nk)
+// and of the transposed basis (2 nR x nk) into scratch as 128 x 64 tiles,
+// each 16 KB tile already in the no-swizzle K-major shared-memory layout the
+// MMA reads: 8 x 16-byte core matrices, 128 B apart along K and 1 KB apart
+// along rows. The main kernel (k_ft_tc, one 128 x 128 output tile per CTA)
+// streams the four tiles of each 64-wide K chunk into a two-stage shared
+// ring with bulk-async copies (cp.async.bulk, no multicast) completing on an
+// mbarrier; one thread issues the 4 x 3 MMAs (128 x 128 x 16 each) of the
+// chunk into one 128 x 128 FP32 accumulator in tensor memory and commits them
+// to the stage's mbarrier before the stage is refilled. Four warps then read
+// the accumulator (lane = row) with tcgen05.ld and write FP64.
+//
+// Every wait is bounded (kTcSpin polls); a wait that runs out sets the error
+// word in the first 4 bytes of scratch (CHX_DEVERR_INDEX), waits (bounded)
+// for the copies and MMAs it started, frees its tensor memory and returns.
+#include <cuda_bf16.h>
 #include "chx_common.cuh"
 
 namespace chx {
 
-int64_t ft_batch_tc_scratch(int rows, int nk, int nR) { return 0; }
+constexpr int kTcM = 128, kTcN = 128, kTcK = 64;        // CTA tile; MMA 128 x 128 x 16
+constexpr uint32_t kTcTile = kTcM * kTcK * 2;           // one operand tile, 16 KB
+constexpr uint32_t kTcStage = 4 * kTcTile;              // A_hi, A_lo, B_hi, B_lo
+constexpr int kTcStages = 2;
+constexpr uint32_t kTcLBO = 128, kTcSBO = 1024;         // core-matrix strides (bytes)
+constexpr int kTcSpin = 1 << 24;
+constexpr int kTcTmemCols = 128;                        // FP32 accumulator columns
+constexpr size_t kTcSmem = (size_t)kTcStages * kTcStage + 1024;
+
+static_assert(kTcM == kTcN, "A and B tiles share one layout");
+
+// byte offset of element (r, k) inside one 128 x 64 operand tile
+__host__ __device__ __forceinline__ uint32_t tc_tile_off(int r, int k) {
+    return (uint32_t)((r >> 3) * kTcSBO + (k >> 3) * kTcLBO + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint32_t tc_smem(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// shared-memory matrix descriptor: start address, leading (K) and stride
+// (row-group) byte offsets, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+    return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)(kTcLBO >> 4) << 16) |
+           ((uint64_t)(kTcSBO >> 4) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major,
+// N = 128, M = 128
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
+                              ((uint32_t)(kTcM >> 4) << 24);
+
+__device__ __forceinline__ void tc_mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool tc_mbar_wait(uint64_t *bar, uint32_t parity) {
+    const uint32_t a = tc_smem(bar);
+    for (int it = 0; it < kTcSpin; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_load_tile(void *dst, const void *src, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(tc_smem(dst)),
+        "l"(src), "r"(kTcTile), "r"(tc_smem(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_expect(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem),
+        "l"(da), "l"(db), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            tc_smem(bar))
+        : "memory");
+}
+
+// hi / lo BF16 parts of X (R x C, element (r, c) at X[r*sr + c*sc]) zero-padded
+// to Rp x Kp, written as 128 x 64 tiles (tile (rt, kt) at (rt * Kp/64 + kt))
+__global__ void k_tc_split(const double *__restrict__ X, int R, int C, long sr, long sc, int Rp,
+                           int Kp, uint8_t *__restrict__ hi, uint8_t *__restrict__ lo) {
+    const long n = (long)Rp * Kp;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+         q += (long)gridDim.x * blockDim.x) {
+        const int r = (int)(q / Kp), k = (int)(q % Kp);
+        const double x = (r < R && k < C) ? X[r * sr + k * sc] : 0.0;
+        const __nv_bfloat16 h = __double2bfloat16(x);
+        const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+        const long off = ((long)(r / kTcM) * (Kp / kTcK) + k / kTcK) * kTcTile +
+                         tc_tile_off(r % kTcM, k % kTcK);
+        *(__nv_bfloat16 *)(hi + off) = h;
+        *(__nv_bfloat16 *)(lo + off) = l;
+    }
+}
+
+__global__ void __launch_bounds__(128, 1) k_ft_tc(const uint8_t *__restrict__ Ahi,
+                                                  const uint8_t *__restrict__ Alo,
+                                                  const uint8_t *__restrict__ Bhi,
+                                                  const uint8_t *__restrict__ Blo, int nkt,
+                                                  int rows, int ncol, double *__restrict__ out,
+                                                  int *__restrict__ err) {
+    extern __shared__ uint8_t tc_raw[];
+    __shared__ __align__(8) uint64_t full[kTcStages], freed[kTcStages], done;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    uint8_t *ring = (uint8_t *)(((uintptr_t)tc_raw + 1023) & ~(uintptr_t)1023);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nt = blockIdx.x, mt = blockIdx.y;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         tc_smem(&s_tmem)),
+                     "r"(kTcTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            tc_mbar_init(&full[s]);
+            tc_mbar_init(&freed[s]);
+        }
+        tc_mbar_init(&done);
+        s_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+
+    if (tid == 0) {
+        const long tstride = (long)nkt * kTcTile;            // one row of tiles
+        const uint8_t *a_hi = Ahi + mt * tstride, *a_lo = Alo + mt * tstride;
+        const uint8_t *b_hi = Bhi + nt * tstride, *b_lo = Blo + nt * tstride;
+        int loads[kTcStages] = {0, 0}, waits[kTcStages] = {0, 0};
+        auto load = [&](int kt, int s) {
+            uint8_t *st = ring + (size_t)s * kTcStage;
+            tc_expect(&full[s], kTcStage);
+            tc_load_tile(st, a_hi + (long)kt * kTcTile, &full[s]);
+            tc_load_tile(st + kTcTile, a_lo + (long)kt * kTcTile, &full[s]);
+            tc_load_tile(st + 2 * kTcTile, b_hi + (long)kt * kTcTile, &full[s]);
+            tc_load_tile(st + 3 * kTcTile, b_lo + (long)kt * kTcTile, &full[s]);
+            ++loads[s];
+        };
+        for (int s = 0; s < kTcStages && s < nkt; ++s) load(s, s);
+        bool ok = true;
+        for (int kt = 0; kt < nkt && ok; ++kt) {
+            const int s = kt & 1;
+            const uint32_t par = (uint32_t)((kt >> 1) & 1);
+            if (!tc_mbar_wait(&full[s], par)) {
+                ok = false;
+                break;
+            }
+            ++waits[s];
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = tc_smem(ring + (size_t)s * kTcStage);
+#pragma unroll
+            for (int kk = 0; kk < kTcK / 16; ++kk) {
+                const uint32_t ko = kk * 2 * kTcLBO;   // 16 K values = two core matrices
+                const uint64_t ahi = tc_desc(base + ko), alo = tc_desc(base + kTcTile + ko);
+                const uint64_t bhi = tc_desc(base + 2 * kTcTile + ko),
+                               blo = tc_desc(base + 3 * kTcTile + ko);
+                tc_mma(tmem, ahi, bhi, (kt | kk) != 0);
+                tc_mma(tmem, ahi, blo, 1u);
+                tc_mma(tmem, alo, bhi, 1u);
+            }
+            tc_commit(&freed[s]);
+            if (kt + kTcStages < nkt) {
+                if (!tc_mbar_wait(&freed[s], par)) {
+                    ok = false;
+                    break;
+                }
+                load(kt + kTcStages, s);
+            }
+        }
+        tc_commit(&done);
+        if (!ok) {
+            s_fail = 1;
+            // copies still owed to a stage: wait for them (bounded) before leaving
+            for (int s = 0; s < kTcStages; ++s)
+                for (int w = waits[s]; w < loads[s]; ++w)
+                    if (!tc_mbar_wait(&full[s], (uint32_t)(w & 1))) break;
+        }
+        if (!tc_mbar_wait(&done, 0)) s_fail = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (!s_fail) {
+        const int row = mt * kTcM + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < kTcN; c0 += 32) {
+            uint32_t v[32];
+            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+                "%10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, "
+                "%26, %27, %28, %29, %30, %31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+                  "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                  "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                  "=r"(v[30]), "=r"(v[31])
+                : "r"(ta)
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < rows) {
+                double *o = out + (long)row * ncol + nt * kTcN + c0;
+                const int lim = ncol - (nt * kTcN + c0);
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    if (j < lim) o[j] = (double)__uint_as_float(v[j]);
+            }
+        }
+    } else if (tid == 0) {
+        atomicOr(err, CHX_DEVERR_INDEX);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTcTmemCols)
+                     : "memory");
+}
+
+struct TcPlan {
+    int Mp, Np, Kp;
+    size_t a_bytes, b_bytes, total;
+};
+static TcPlan tc_plan(int rows, int nk, int nR) {
+    TcPlan p;
+    p.Mp = (rows + kTcM - 1) / kTcM * kTcM;
+    p.Np = (2 * nR + kTcN - 1) / kTcN * kTcN;
+    p.Kp = (nk + kTcK - 1) / kTcK * kTcK;
+    p.a_bytes = (size_t)p.Mp * p.Kp * 2;
+    p.b_bytes = (size_t)p.Np * p.Kp * 2;
+    p.total = 256 + 2 * p.a_bytes + 2 * p.b_bytes;
+    return p;
+}
+
+int64_t ft_batch_tc_scratch(int rows, int nk, int nR) { return (int64_t)tc_plan(rows, nk, nR).total; }
 
 int ft_batch_tc(const double *chi, int rows, int nk, const double *basis, int nR, double *out,
                 void *scratch, int64_t scratch_bytes, cudaStream_t st) {
-    set_error("ft_batch: tensor-core path not built yet");
-    return CHX_ERR_UNSUPPORTED;
+    const TcPlan p = tc_plan(rows, nk, nR);
+    CHX_REQUIRE(scratch && scratch_bytes >= (int64_t)p.total,
+                "ft_batch: split-BF16 path needs %zu bytes of scratch", p.total);
+    CHX_REQUIRE(((uintptr_t)scratch & 255) == 0, "ft_batch: scratch must be 256-byte aligned");
+    uint8_t *base = (uint8_t *)scratch;
+    int *err = (int *)base;
+    uint8_t *ahi = base + 256, *alo = ahi + p.a_bytes, *bhi = alo + p.a_bytes,
+            *bl = bhi + p.b_bytes;
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "ft_batch memset");
+    const int ncol = 2 * nR;
+    k_tc_split<<<592, 256, 0, st>>>(chi, rows, nk, nk, 1, p.Mp, p.Kp, ahi, alo);
+    k_tc_split<<<592, 256, 0, st>>>(basis, ncol, nk, 1, ncol, p.Np, p.Kp, bhi, bl);
+    e = cudaFuncSetAttribute(k_ft_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc attribute");
+    dim3 grid(p.Np / kTcN, p.Mp / kTcM);
+    k_ft_tc<<<grid, 128, kTcSmem, st>>>(ahi, alo, bhi, bl, p.Kp / kTcK, rows, ncol, out, err);
+    CHX_CHECK_LAUNCH("ft_batch tc");
+    return CHX_OK;
 }
 
 }  // namespace chx

@@ -1,0 +1,54 @@
+"""The windowed FT contraction chx_ft_batch (A5) in its three precisions:
+FP64 and FP32 SIMT tiles, split-BF16 on the tcgen05 tensor cores."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+# tolerance relative to the largest |chi(R)| of the case
+TOL = {0: 1e-12, 1: 2e-6, 2: 1e-4}
+
+
+@pytest.mark.parametrize("precision", [0, 1, 2])
+@pytest.mark.parametrize("grid", ["model", "uniform", "shifted"])
+def test_transform_matches_reference_goldens(cuda, grid, precision):
+    """chi(R) of the reference's FourierTransform (first 256 bins) for every
+    k grid and k weight of the goldens."""
+    from chimera_b200.fourier import FourierTransform
+    g = golden("fourier.npz")
+    for kw in (1, 2, 3):
+        key = f"{grid}_w{kw}"
+        f = FourierTransform(g[key + "_k"], 3.0, 13.0, kw)
+        z = f.to_R(g[key + "_chi"], bins=np.arange(256), precision=precision)
+        want = g[key + "_R256"]
+        assert np.abs(z - want).max() <= TOL[precision] * np.abs(want).max(), key
+
+
+def test_split_bf16_batch_of_the_series_configuration(cuda):
+    """4,096 spectra x 241 k points onto 200 R points (the series-point
+    configuration's per-weight batch): the tensor-core contraction against the
+    FP64 one, on rows that are not a multiple of the 128-row tile and a column
+    count (400) that is not a multiple of 128."""
+    import torch
+    from chimera_b200.fourier import FourierTransform, apply_basis
+    from chimera_b200.tables import uniform_k
+    k = uniform_k()
+    f = FourierTransform(k, 3.0, 13.0, 2, window="kaiser")
+    B = f.basis(np.arange(46, 246))
+    rng = np.random.default_rng(4)
+    for rows in (4096, 1000):
+        chi = rng.normal(0, 1, (rows, k.size)) * np.exp(-0.1 * k)[None]
+        x = torch.from_numpy(chi).cuda()
+        z0 = apply_basis(x, B, 0).cpu().numpy()
+        z2 = apply_basis(x, B, 2).cpu().numpy()
+        z1 = apply_basis(x, B, 1).cpu().numpy()
+        scale = np.abs(z0).max()
+        e2 = np.abs(z2 - z0).max() / scale
+        e1 = np.abs(z1 - z0).max() / scale
+        print(f"rows {rows}: split-BF16 max err {e2:.2e}, FP32 {e1:.2e} (of max |chi(R)|)")
+        assert e2 <= TOL[2] and e1 <= TOL[1]
+        # per-bin relative error stays small where chi(R) is not tiny
+        big = np.abs(z0) > 0.05 * scale
+        assert (np.abs(z2 - z0)[big] / np.abs(z0)[big]).max() <= 5e-3
