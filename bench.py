@@ -236,6 +236,70 @@ def _ref_worker(arg):
     return {"attempts": steps * NREP, "seconds": steps * NREP / r["value"]}
 
 
+def bench_ft(args):
+    """The windowed FT contraction of the series-point configuration: 4,096
+    spectra x 3 k weights, 241 k points onto 200 R points, per precision
+    (0 FP64 SIMT, 1 FP32 SIMT, 2 split-BF16 tcgen05), inputs resident, L2
+    flushed (256 MB write) before every timed call; one JSON line."""
+    import ctypes as C
+    import torch
+    from chimera_b200 import _native as N
+    from chimera_b200.fourier import FourierTransform
+    from chimera_b200.tables import uniform_k
+    N.lib()
+    k = uniform_k()
+    f = FourierTransform(k, 3.0, 13.0, 2, window="kaiser")
+    B = f.basis(np.arange(46, 246))
+    rows, nk, nR = 4096 * 3, k.size, B.shape[1]
+    ncol = 2 * nR
+    rng = np.random.default_rng(0)
+    x = torch.from_numpy(rng.normal(0, 1, (rows, nk)) * np.exp(-0.1 * k)[None]).cuda()
+    Bd = torch.from_numpy(np.ascontiguousarray(np.stack([B.real, B.imag], -1).reshape(nk, -1))).cuda()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    s = torch.cuda.current_stream()
+    res = {}
+    ref = None
+    for prec in (0, 1, 2):
+        out = torch.empty((rows, ncol), dtype=torch.float64, device="cuda")
+        nsc = int(N.lib().chx_ft_batch_scratch_bytes(rows, nk, nR, prec))
+        scr = torch.empty(max(nsc, 1), dtype=torch.uint8, device="cuda")
+
+        def call():
+            N.call("chx_ft_batch", N.ptr(x), rows, nk, N.ptr(Bd), nR, prec, N.ptr(out),
+                   N.ptr(scr), nsc, N.stream())
+        for _ in range(max(3, args.warmup)):
+            call()
+        ts = []
+        for _ in range(max(5, min(args.steps, 50))):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            call()
+            b.record(s)
+            b.synchronize()
+            ts.append(a.elapsed_time(b) * 1e-3)
+        t = float(np.median(ts))
+        if ref is None:
+            ref = out.clone()
+        err = float((out - ref).abs().max() / ref.abs().max())
+        byts = (rows * nk + nk * ncol + rows * ncol) * 8
+        res[str(prec)] = {"us": t * 1e6, "GB_per_s": byts / t / 1e9,
+                          "useful_TFLOP_per_s": 2.0 * rows * nk * ncol / t / 1e12,
+                          "max_err_vs_fp64": err}
+    hbm, src = peaks()
+    tc = res["2"]
+    line = {"metric": "windowed FT contraction chi(k) -> chi(R)", "kernel": "chx_ft_batch",
+            "config": {"workload": "4,096 spectra x 3 k weights, 241 k -> 200 R points",
+                       "rows": rows, "nk": nk, "nR": nR, "l2": "flushed before each call"},
+            "precisions": {"0": "FP64 SIMT", "1": "FP32 SIMT", "2": "split-BF16 tcgen05"},
+            "results": res,
+            "roofline": {"bound": "hbm", "achieved": tc["GB_per_s"], "peak": hbm,
+                         "unit": "GB/s", "frac": tc["GB_per_s"] / hbm, "peak_source": src,
+                         "bytes": "chi + basis read, chi(R) written, FP64"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global NPOS
     ap = argparse.ArgumentParser()
@@ -248,10 +312,14 @@ def main():
     ap.add_argument("--positions", type=int, default=16,
                     help="ladders per GPU (fewer for a small profiling case)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--kernel", default="sampler", choices=["sampler", "ft"],
+                    help="ft: time the windowed FT contraction (chx_ft_batch) instead")
     args = ap.parse_args()
     NPOS = args.positions
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel == "ft":
+        return bench_ft(args)
 
     import torch
     import torch.distributed as dist

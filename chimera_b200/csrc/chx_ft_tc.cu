@@ -7,17 +7,22 @@
 // FP32 accumulation in tensor memory, which keeps about 16 significant bits
 // per product where one BF16 product keeps 8.
 //
-// Layout. A pre-pass (k_tc_split) writes the hi and lo parts of chi (rows x nk)
-// and of the transposed basis (2 nR x nk) into scratch as 128 x 64 tiles,
-// each 16 KB tile already in the no-swizzle K-major shared-memory layout the
-// MMA reads: 8 x 16-byte core matrices, 128 B apart along K and 1 KB apart
-// along rows. The main kernel (k_ft_tc, one 128 x 128 output tile per CTA)
-// streams the four tiles of each 64-wide K chunk into a two-stage shared
-// ring with bulk-async copies (cp.async.bulk, no multicast) completing on an
-// mbarrier; one thread issues the 4 x 3 MMAs (128 x 128 x 16 each) of the
-// chunk into one 128 x 128 FP32 accumulator in tensor memory and commits them
-// to the stage's mbarrier before the stage is refilled. Four warps then read
-// the accumulator (lane = row) with tcgen05.ld and write FP64.
+// Layout. The basis (2 nR x nk, transposed) is split by a pre-pass
+// (k_tc_split) into hi and lo 128 x 32 tiles in scratch, each 8 KB tile
+// already in the no-swizzle K-major shared-memory layout the MMA reads:
+// 8 x 16-byte core matrices, 128 B apart along K and 512 B apart along rows.
+// The main kernel (k_ft_tc, one 128 x 128 output tile per CTA, three CTAs per
+// SM) runs a two-stage ring over 32-wide K chunks: one thread brings the
+// chunk's basis tiles in with bulk-async copies (cp.async.bulk, no
+// multicast) completing on an mbarrier while all 128 threads read the chunk
+// of chi (FP64, any row alignment) and write its hi and lo parts straight
+// into the same layout (each warp load 256 contiguous bytes of one row);
+// one thread then issues the 2 x 3 MMAs (128 x 128 x 16
+// each) into one 128 x 128 FP32 accumulator in tensor memory and commits them
+// to the stage's mbarrier, and the threads move on to the next chunk while
+// the tensor core works. Four warps finally read the accumulator (lane =
+// row) with tcgen05.ld, turn each 32 x 32 block around in shared memory and
+// write FP64 rows with coalesced stores.
 //
 // Every wait is bounded (kTcSpin polls); a wait that runs out sets the error
 // word in the first 4 bytes of scratch (CHX_DEVERR_INDEX), waits (bounded)
@@ -27,18 +32,17 @@
 
 namespace chx {
 
-constexpr int kTcM = 128, kTcN = 128, kTcK = 64;        // CTA tile; MMA 128 x 128 x 16
-constexpr uint32_t kTcTile = kTcM * kTcK * 2;           // one operand tile, 16 KB
-constexpr uint32_t kTcStage = 4 * kTcTile;              // A_hi, A_lo, B_hi, B_lo
+constexpr int kTcM = 128, kTcN = 128, kTcK = 32;        // CTA tile; MMA 128 x 128 x 16
+constexpr uint32_t kTcTileA = kTcM * kTcK * 2;          // chi operand tile, 8 KB
+constexpr uint32_t kTcTileB = kTcN * kTcK * 2;          // basis operand tile, 16 KB
+constexpr uint32_t kTcStage = 2 * kTcTileA + 2 * kTcTileB;   // A_hi, A_lo, B_hi, B_lo
 constexpr int kTcStages = 2;
-constexpr uint32_t kTcLBO = 128, kTcSBO = 1024;         // core-matrix strides (bytes)
+constexpr uint32_t kTcLBO = 128, kTcSBO = (kTcK / 8) * 128;   // core-matrix strides (bytes)
 constexpr int kTcSpin = 1 << 24;
-constexpr int kTcTmemCols = 128;                        // FP32 accumulator columns
+constexpr int kTcTmemCols = kTcN;                       // FP32 accumulator columns
 constexpr size_t kTcSmem = (size_t)kTcStages * kTcStage + 1024;
 
-static_assert(kTcM == kTcN, "A and B tiles share one layout");
-
-// byte offset of element (r, k) inside one 128 x 64 operand tile
+// byte offset of element (r, k) inside one operand tile of 32 K values
 __host__ __device__ __forceinline__ uint32_t tc_tile_off(int r, int k) {
     return (uint32_t)((r >> 3) * kTcSBO + (k >> 3) * kTcLBO + (r & 7) * 16 + (k & 7) * 2);
 }
@@ -82,7 +86,7 @@ __device__ __forceinline__ void tc_load_tile(void *dst, const void *src, uint64_
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
             "r"(tc_smem(dst)),
-        "l"(src), "r"(kTcTile), "r"(tc_smem(bar))
+        "l"(src), "r"(kTcTileB), "r"(tc_smem(bar))
         : "memory");
 }
 
@@ -110,7 +114,7 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
 }
 
 // hi / lo BF16 parts of X (R x C, element (r, c) at X[r*sr + c*sc]) zero-padded
-// to Rp x Kp, written as 128 x 64 tiles (tile (rt, kt) at (rt * Kp/64 + kt))
+// to Rp x Kp, written as 128 x 32 tiles (tile (rt, kt) at (rt * Kp/32 + kt))
 __global__ void k_tc_split(const double *__restrict__ X, int R, int C, long sr, long sc, int Rp,
                            int Kp, uint8_t *__restrict__ hi, uint8_t *__restrict__ lo) {
     const long n = (long)Rp * Kp;
@@ -120,18 +124,17 @@ __global__ void k_tc_split(const double *__restrict__ X, int R, int C, long sr, 
         const double x = (r < R && k < C) ? X[r * sr + k * sc] : 0.0;
         const __nv_bfloat16 h = __double2bfloat16(x);
         const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
-        const long off = ((long)(r / kTcM) * (Kp / kTcK) + k / kTcK) * kTcTile +
-                         tc_tile_off(r % kTcM, k % kTcK);
+        const long off = ((long)(r / kTcN) * (Kp / kTcK) + k / kTcK) * kTcTileB +
+                         tc_tile_off(r % kTcN, k % kTcK);
         *(__nv_bfloat16 *)(hi + off) = h;
         *(__nv_bfloat16 *)(lo + off) = l;
     }
 }
 
-__global__ void __launch_bounds__(128, 1) k_ft_tc(const uint8_t *__restrict__ Ahi,
-                                                  const uint8_t *__restrict__ Alo,
-                                                  const uint8_t *__restrict__ Bhi,
+__global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi, int rows,
+                                                  int nk, const uint8_t *__restrict__ Bhi,
                                                   const uint8_t *__restrict__ Blo, int nkt,
-                                                  int rows, int ncol, double *__restrict__ out,
+                                                  int ncol, double *__restrict__ out,
                                                   int *__restrict__ err) {
     extern __shared__ uint8_t tc_raw[];
     __shared__ __align__(8) uint64_t full[kTcStages], freed[kTcStages], done;
@@ -162,59 +165,75 @@ __global__ void __launch_bounds__(128, 1) k_ft_tc(const uint8_t *__restrict__ Ah
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
 
-    if (tid == 0) {
-        const long tstride = (long)nkt * kTcTile;            // one row of tiles
-        const uint8_t *a_hi = Ahi + mt * tstride, *a_lo = Alo + mt * tstride;
-        const uint8_t *b_hi = Bhi + nt * tstride, *b_lo = Blo + nt * tstride;
-        int loads[kTcStages] = {0, 0}, waits[kTcStages] = {0, 0};
-        auto load = [&](int kt, int s) {
-            uint8_t *st = ring + (size_t)s * kTcStage;
-            tc_expect(&full[s], kTcStage);
-            tc_load_tile(st, a_hi + (long)kt * kTcTile, &full[s]);
-            tc_load_tile(st + kTcTile, a_lo + (long)kt * kTcTile, &full[s]);
-            tc_load_tile(st + 2 * kTcTile, b_hi + (long)kt * kTcTile, &full[s]);
-            tc_load_tile(st + 3 * kTcTile, b_lo + (long)kt * kTcTile, &full[s]);
-            ++loads[s];
-        };
-        for (int s = 0; s < kTcStages && s < nkt; ++s) load(s, s);
-        bool ok = true;
-        for (int kt = 0; kt < nkt && ok; ++kt) {
-            const int s = kt & 1;
-            const uint32_t par = (uint32_t)((kt >> 1) & 1);
-            if (!tc_mbar_wait(&full[s], par)) {
-                ok = false;
-                break;
-            }
-            ++waits[s];
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t base = tc_smem(ring + (size_t)s * kTcStage);
+    const long tstride = (long)nkt * kTcTileB;               // one row of basis tiles
+    const uint8_t *b_hi = Bhi + nt * tstride, *b_lo = Blo + nt * tstride;
+    const int row0 = mt * kTcM;
+    int issued[kTcStages] = {0, 0}, landed[kTcStages] = {0, 0};
+    for (int kt = 0; kt < nkt; ++kt) {
+        const int s = kt & 1;
+        const uint32_t par = (uint32_t)((kt >> 1) & 1);
+        uint8_t *st = ring + (size_t)s * kTcStage;
+        // the stage's previous MMAs (chunk kt - 2) must be done before it is refilled
+        if (kt >= kTcStages && !s_fail) {
+            if (tid == 0 && !tc_mbar_wait(&freed[s], par ^ 1)) s_fail = 1;
+        }
+        __syncthreads();
+        if (s_fail) break;
+        if (tid == 0) {
+            tc_expect(&full[s], 2 * kTcTileB);
+            tc_load_tile(st + 2 * kTcTileA, b_hi + (long)kt * kTcTileB, &full[s]);
+            tc_load_tile(st + 2 * kTcTileA + kTcTileB, b_lo + (long)kt * kTcTileB, &full[s]);
+            ++issued[s];
+        }
+        // chi chunk, 128 rows x 32 k: lane = k, warp w takes rows w, w + 4, ...,
+        // so every warp load reads 256 contiguous bytes of one row
+        {
+            const int gk = kt * kTcK + lane;
+            const bool kin = gk < nk;
+            double v[kTcM / 4];
 #pragma unroll
-            for (int kk = 0; kk < kTcK / 16; ++kk) {
-                const uint32_t ko = kk * 2 * kTcLBO;   // 16 K values = two core matrices
-                const uint64_t ahi = tc_desc(base + ko), alo = tc_desc(base + kTcTile + ko);
-                const uint64_t bhi = tc_desc(base + 2 * kTcTile + ko),
-                               blo = tc_desc(base + 3 * kTcTile + ko);
-                tc_mma(tmem, ahi, bhi, (kt | kk) != 0);
-                tc_mma(tmem, ahi, blo, 1u);
-                tc_mma(tmem, alo, bhi, 1u);
+            for (int i = 0; i < kTcM / 4; ++i) {
+                const int grow = row0 + warp + 4 * i;
+                v[i] = (kin && grow < rows) ? __ldg(chi + (long)grow * nk + gk) : 0.0;
             }
-            tc_commit(&freed[s]);
-            if (kt + kTcStages < nkt) {
-                if (!tc_mbar_wait(&freed[s], par)) {
-                    ok = false;
-                    break;
+#pragma unroll
+            for (int i = 0; i < kTcM / 4; ++i) {
+                const __nv_bfloat16 h = __double2bfloat16(v[i]);
+                const __nv_bfloat16 l = __double2bfloat16(v[i] - (double)__bfloat162float(h));
+                const uint32_t off = tc_tile_off(warp + 4 * i, lane);
+                *(__nv_bfloat16 *)(st + off) = h;
+                *(__nv_bfloat16 *)(st + kTcTileA + off) = l;
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            if (!tc_mbar_wait(&full[s], par)) {
+                s_fail = 1;
+            } else {
+                ++landed[s];
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t base = tc_smem(st);
+#pragma unroll
+                for (int kk = 0; kk < kTcK / 16; ++kk) {
+                    const uint32_t ko = kk * 2 * kTcLBO;   // 16 K values = two core matrices
+                    const uint64_t ahi = tc_desc(base + ko), alo = tc_desc(base + kTcTileA + ko);
+                    const uint64_t bhi = tc_desc(base + 2 * kTcTileA + ko),
+                                   blo = tc_desc(base + 2 * kTcTileA + kTcTileB + ko);
+                    tc_mma(tmem, ahi, bhi, (kt | kk) != 0);
+                    tc_mma(tmem, ahi, blo, 1u);
+                    tc_mma(tmem, alo, bhi, 1u);
                 }
-                load(kt + kTcStages, s);
+                tc_commit(&freed[s]);
             }
         }
+    }
+    if (tid == 0) {
         tc_commit(&done);
-        if (!ok) {
-            s_fail = 1;
-            // copies still owed to a stage: wait for them (bounded) before leaving
-            for (int s = 0; s < kTcStages; ++s)
-                for (int w = waits[s]; w < loads[s]; ++w)
-                    if (!tc_mbar_wait(&full[s], (uint32_t)(w & 1))) break;
-        }
+        // copies still owed to a stage (after a failed wait): wait for them, bounded
+        for (int s = 0; s < kTcStages; ++s)
+            for (int w = landed[s]; w < issued[s]; ++w)
+                if (!tc_mbar_wait(&full[s], (uint32_t)(w & 1))) break;
         if (!tc_mbar_wait(&done, 0)) s_fail = 1;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -222,7 +241,9 @@ __global__ void __launch_bounds__(128, 1) k_ft_tc(const uint8_t *__restrict__ Ah
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
     if (!s_fail) {
-        const int row = mt * kTcM + warp * 32 + lane;
+        // each warp turns its 32 x 32 block around in shared memory (the ring
+        // is free now) so that every store writes 32 consecutive doubles
+        float *tb = (float *)ring + warp * 32 * 33;
 #pragma unroll 1
         for (int c0 = 0; c0 < kTcN; c0 += 32) {
             uint32_t v[32];
@@ -240,13 +261,16 @@ __global__ void __launch_bounds__(128, 1) k_ft_tc(const uint8_t *__restrict__ Ah
                 : "r"(ta)
                 : "memory");
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < rows) {
-                double *o = out + (long)row * ncol + nt * kTcN + c0;
-                const int lim = ncol - (nt * kTcN + c0);
 #pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    if (j < lim) o[j] = (double)__uint_as_float(v[j]);
+            for (int j = 0; j < 32; ++j) tb[lane * 33 + j] = __uint_as_float(v[j]);
+            __syncwarp();
+            const int col = nt * kTcN + c0 + lane;
+#pragma unroll 4
+            for (int r = 0; r < 32; ++r) {
+                const int row = row0 + warp * 32 + r;
+                if (row < rows && col < ncol) out[(long)row * ncol + col] = (double)tb[r * 33 + lane];
             }
+            __syncwarp();
         }
     } else if (tid == 0) {
         atomicOr(err, CHX_DEVERR_INDEX);
@@ -268,9 +292,9 @@ static TcPlan tc_plan(int rows, int nk, int nR) {
     p.Mp = (rows + kTcM - 1) / kTcM * kTcM;
     p.Np = (2 * nR + kTcN - 1) / kTcN * kTcN;
     p.Kp = (nk + kTcK - 1) / kTcK * kTcK;
-    p.a_bytes = (size_t)p.Mp * p.Kp * 2;
-    p.b_bytes = (size_t)p.Np * p.Kp * 2;
-    p.total = 256 + 2 * p.a_bytes + 2 * p.b_bytes;
+    p.a_bytes = 0;                              // chi is split inside the main kernel
+    p.b_bytes = (size_t)p.Np * p.Kp * 2;       // Np is a multiple of the basis tile rows
+    p.total = 256 + 2 * p.b_bytes;
     return p;
 }
 
@@ -284,17 +308,17 @@ int ft_batch_tc(const double *chi, int rows, int nk, const double *basis, int nR
     CHX_REQUIRE(((uintptr_t)scratch & 255) == 0, "ft_batch: scratch must be 256-byte aligned");
     uint8_t *base = (uint8_t *)scratch;
     int *err = (int *)base;
-    uint8_t *ahi = base + 256, *alo = ahi + p.a_bytes, *bhi = alo + p.a_bytes,
-            *bl = bhi + p.b_bytes;
+    uint8_t *bhi = base + 256, *bl = bhi + p.b_bytes;
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch memset");
     const int ncol = 2 * nR;
-    k_tc_split<<<592, 256, 0, st>>>(chi, rows, nk, nk, 1, p.Mp, p.Kp, ahi, alo);
-    k_tc_split<<<592, 256, 0, st>>>(basis, ncol, nk, 1, ncol, p.Np, p.Kp, bhi, bl);
+    const long nb = (long)p.Np * p.Kp;
+    k_tc_split<<<(unsigned)std::min<long>((nb + 255) / 256, 592), 256, 0, st>>>(
+        basis, ncol, nk, 1, ncol, p.Np, p.Kp, bhi, bl);
     e = cudaFuncSetAttribute(k_ft_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc attribute");
     dim3 grid(p.Np / kTcN, p.Mp / kTcM);
-    k_ft_tc<<<grid, 128, kTcSmem, st>>>(ahi, alo, bhi, bl, p.Kp / kTcK, rows, ncol, out, err);
+    k_ft_tc<<<grid, 128, kTcSmem, st>>>(chi, rows, nk, bhi, bl, p.Kp / kTcK, ncol, out, err);
     CHX_CHECK_LAUNCH("ft_batch tc");
     return CHX_OK;
 }
