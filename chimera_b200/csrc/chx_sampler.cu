@@ -59,7 +59,9 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     int maxaff = 4 * L.ncoord;
     int nent = L.ms_nblk ? L.nsp * L.ms_nblk : 0;
     int ndn = L.nshell * L.nsp * L.nsp;
-    s.u = o; o += f64 ? al16<double>((size_t)L.nchan * L.ncoef) : al16<float>((size_t)L.nchan * L.ncoef);
+    // resampled rows, channel stride padded to even (channel pairs of the DFT)
+    const size_t nchp = (size_t)L.nchan + (L.nchan & 1);
+    s.u = o; o += f64 ? al16<double>(nchp * L.ncoef) : al16<float>(nchp * L.ncoef);
     size_t xs = f64 ? al16<double2>((size_t)kMaxSplit * L.nchan * L.nwin)
                     : al16<float2>((size_t)kMaxSplit * L.nchan * L.nwin);
     // the surrogate's scratch (partial sums of every warp + one activation
@@ -74,7 +76,7 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     s.dn = o; o += al16<int>((size_t)std::max(ndn, 1));
     s.list = o; o += al16<int>((size_t)(2 * maxaff + 2 * ndn + 2 * nent + 64));
     s.sp = o; o += al16<uint8_t>((size_t)L.natoms);
-    s.nb = o; o += al16<uint16_t>((size_t)2 * std::max(L.ms_D, 1));
+    s.nb = o; o += al16<uint16_t>((size_t)2 * (std::max(L.ms_D, 1) + 2));
     s.cd = o; o += al16<uint8_t>((size_t)((L.mlp || L.log_cap > 0) ? 2 * L.feat_D + 1 : 1));
     s.chi = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.total = o;
@@ -123,6 +125,18 @@ __device__ __forceinline__ int ms_entry(SpeciesOf sp, int4 rc, int nsp, int nblk
     return e;
 }
 
+// d = a * b + c on both halves of a pair (one packed FP32x2 FMA, round to
+// nearest per half, as two fmaf)
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
 template <int PREC>
 struct Real {
     typedef float T;
@@ -161,12 +175,15 @@ __device__ __noinline__ void ft_window(const chx_ladder_t &L, const double *s_tr
     const int tid = threadIdx.x;
     const int nk = L.nk;
     const int nchan = L.nchan, ncoef = L.ncoef, nwin = L.nwin, nkw = L.nkw;
+    const int nchp = nchan + (nchan & 1);      // row stride; the pad channel is zero
     for (int q = tid; q < nchan * ncoef; q += blockDim.x) {
         int ch = q / ncoef, j = q - ch * ncoef, e = ch / nkw;
         int id = L.ft_idx[q];
         double va = s_tr[e * nk + id], vb = s_tr[e * nk + id + 1];
-        s_u[j * nchan + ch] = (real)((va + (vb - va) * L.ft_frac[q]) * L.ft_w[q]);
+        s_u[j * nchp + ch] = (real)((va + (vb - va) * L.ft_frac[q]) * L.ft_w[q]);
     }
+    if (nchan & 1)
+        for (int j = tid; j < ncoef; j += blockDim.x) s_u[j * nchp + nchan] = (real)0;
     __syncthreads();
     const int fmask = L.nfft - 1;
     const int n0 = L.ft_n0[0];
@@ -177,31 +194,66 @@ __device__ __noinline__ void ft_window(const chx_ladder_t &L, const double *s_tr
         int part = item / nwin, q = item - part * nwin;
         int m = L.win_bin[q] & fmask;
         int j0 = part * jper, j1 = min(ncoef, j0 + jper);
-        real ar[MAXCH], ai[MAXCH];
-#pragma unroll
-        for (int c = 0; c < MAXCH; ++c) ar[c] = ai[c] = 0;
         const real inv_half = (real)2.0 / (real)L.nfft;
         const real2 rot = twiddle(m, inv_half);
-        for (int jb = j0; jb < j1; jb += kReseed) {
-            real2 z = twiddle((int)(((long)(n0 + jb) * m) & fmask), inv_half);
-            int je = min(j1, jb + kReseed);
-            for (int j = jb; j < je; ++j) {
-                const real *uj = s_u + j * nchan;
+        if constexpr (PREC != CHX_FP64) {
+            // FP32: channel pairs (c, c + 1) of the real and of the imaginary
+            // sums, one packed fma.rn.f32x2 each per tap
+            constexpr int MAXP = (MAXCH + 1) / 2;
+            const int npair = nchp / 2;
+            float2 are[MAXP], aim[MAXP];
 #pragma unroll
-                for (int c = 0; c < MAXCH; ++c)
-                    if (c < nchan) {
-                        real u = uj[c];
-                        ar[c] = fma(u, z.x, ar[c]);
-                        ai[c] = fma(u, z.y, ai[c]);
-                    }
-                real zx = z.x * rot.x - z.y * rot.y;
-                z.y = fma(z.x, rot.y, z.y * rot.x);
-                z.x = zx;
+            for (int p = 0; p < MAXP; ++p) are[p] = aim[p] = make_float2(0.f, 0.f);
+            for (int jb = j0; jb < j1; jb += kReseed) {
+                float2 z = twiddle((int)(((long)(n0 + jb) * m) & fmask), inv_half);
+                int je = min(j1, jb + kReseed);
+                for (int j = jb; j < je; ++j) {
+                    const float2 *uj = (const float2 *)(s_u + j * nchp);
+                    const float2 zx = make_float2(z.x, z.x), zy = make_float2(z.y, z.y);
+#pragma unroll
+                    for (int p = 0; p < MAXP; ++p)
+                        if (p < npair) {
+                            const float2 u = uj[p];
+                            are[p] = ffma2(u, zx, are[p]);
+                            aim[p] = ffma2(u, zy, aim[p]);
+                        }
+                    float zr = z.x * rot.x - z.y * rot.y;
+                    z.y = fmaf(z.x, rot.y, z.y * rot.x);
+                    z.x = zr;
+                }
             }
-        }
 #pragma unroll
-        for (int c = 0; c < MAXCH; ++c)
-            if (c < nchan) s_x[part * nx + c * nwin + q] = real2{ar[c], ai[c]};
+            for (int p = 0; p < MAXP; ++p) {
+                if (2 * p < nchan)
+                    s_x[part * nx + (2 * p) * nwin + q] = real2{are[p].x, aim[p].x};
+                if (2 * p + 1 < nchan)
+                    s_x[part * nx + (2 * p + 1) * nwin + q] = real2{are[p].y, aim[p].y};
+            }
+        } else {
+            real ar[MAXCH], ai[MAXCH];
+#pragma unroll
+            for (int c = 0; c < MAXCH; ++c) ar[c] = ai[c] = 0;
+            for (int jb = j0; jb < j1; jb += kReseed) {
+                real2 z = twiddle((int)(((long)(n0 + jb) * m) & fmask), inv_half);
+                int je = min(j1, jb + kReseed);
+                for (int j = jb; j < je; ++j) {
+                    const real *uj = s_u + j * nchp;
+#pragma unroll
+                    for (int c = 0; c < MAXCH; ++c)
+                        if (c < nchan) {
+                            real u = uj[c];
+                            ar[c] = fma(u, z.x, ar[c]);
+                            ai[c] = fma(u, z.y, ai[c]);
+                        }
+                    real zx = z.x * rot.x - z.y * rot.y;
+                    z.y = fma(z.x, rot.y, z.y * rot.x);
+                    z.x = zx;
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < MAXCH; ++c)
+                if (c < nchan) s_x[part * nx + c * nwin + q] = real2{ar[c], ai[c]};
+        }
     }
     __syncthreads();
     for (int o = tid; o < nx; o += blockDim.x) {
@@ -614,7 +666,9 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         }
         // ---- MS entry changes along the paths through a and b: the species of
         // each site's neighbourhood (old | new << 8 | 0x8000 for site a), then
-        // the shared path templates
+        // two extra slots per site, D: the site itself, D + 1: zero (an unused
+        // template position adds nothing), so that the template loop below
+        // reads every position the same way, without branches
         const bool do_ms = nent && swp;
         if (do_ms) {
             const int D = L.ms_D;
@@ -623,7 +677,13 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 int site = __ldg(&L.ms_nbr[(long)(half ? b : a) * D + (d - half * D)]);
                 int so = s_sp[site] & 0x7F;
                 int sn = site == a ? nsa : (site == b ? nsb : so);
-                s_nb[d] = (uint16_t)(so | (sn << 8) | (site == a ? 0x8000 : 0));
+                s_nb[d + 2 * half] = (uint16_t)(so | (sn << 8) | (site == a ? 0x8000 : 0));
+            }
+            if (tid < 4) {
+                const int h = tid >> 1, zero = tid & 1;
+                s_nb[h * (D + 2) + D + zero] =
+                    zero ? (uint16_t)0
+                         : (uint16_t)((h ? sb_old : sa_old) | ((h ? nsb : nsa) << 8));
             }
         }
         __syncthreads();
@@ -634,29 +694,19 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             for (int m = tid; m < 2 * M; m += blockDim.x) {
                 const int half = m >= M;
                 const uint2 t = __ldg(&tpl[m - half * M]);
-                const uint16_t *nb = s_nb + half * D;
-                const int so_self = half ? sb_old : sa_old, sn_self = half ? nsb : nsa;
+                const uint16_t *nb = s_nb + half * (D + 2);
                 int eo = (int)t.x, en = (int)t.x, hasa = 0;
 #pragma unroll
                 for (int pp = 0; pp < 4; ++pp) {
                     const int v = (t.y >> (8 * pp)) & 0xFF;
                     const int mul = pp == 0 ? nblk : (pp == 1 ? 1 : (pp == 2 ? NSP : NSP * NSP));
-                    if (v == 0xFF) continue;
-                    int so_, sn_;
-                    if (v == 0xFE) {
-                        so_ = so_self;
-                        sn_ = sn_self;
-                    } else {
-                        const int w = nb[v];
-                        so_ = w & 0x7F;
-                        sn_ = (w >> 8) & 0x7F;
-                        hasa |= w & 0x8000;
-                    }
-                    eo += so_ * mul;
-                    en += sn_ * mul;
+                    const int w = nb[v < 0xFE ? v : D + (v - 0xFE)];
+                    eo += (w & 0x7F) * mul;
+                    en += ((w >> 8) & 0x7F) * mul;
+                    hasa |= w & 0x8000;
                 }
-                if (half && hasa) continue;     // a path through both sites counts once
-                if (eo != en) {
+                // a path through both sites counts once (in the half of site a)
+                if (!(half && hasa) && eo != en) {
                     atomicAdd(&s_hist[en], 1);
                     atomicSub(&s_hist[eo], 1);
                 }
