@@ -66,7 +66,7 @@ class Ladder(C.Structure):
         ("best_sp", c_p), ("best_pos", c_p), ("ms_C", c_p), ("acc_rung", c_p), ("acc_log", c_p), ("n_acc", c_p),
         ("exch_att", c_p), ("exch_acc", c_p),
         ("mlp", c_p), ("feat_nbr", c_p), ("feat_D", c_i), ("da_on", c_p), ("da_stat", c_p),
-        ("log_codes", c_p), ("log_y", c_p), ("log_cap", c_i64)]
+        ("log_codes", c_p), ("log_y", c_p), ("log_cap", c_i64), ("best_stale", c_p)]
 
 
 class Mlp(C.Structure):

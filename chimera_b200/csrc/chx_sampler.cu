@@ -40,6 +40,7 @@ constexpr int kStepThreads = 256;
 constexpr int kMaxCoord = 256;
 constexpr int kReseed = 32;      // taps between exact twiddles in the transform
 constexpr int kMaxSplit = 2;     // threads sharing one bin's taps
+constexpr int kUndo = 32;        // accepted moves kept after a slot's best point
 
 // Shared-memory carve-up of one step CTA (all offsets 16-byte aligned).
 struct StepSmem {
@@ -509,6 +510,15 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     __shared__ float s_sigma;
     __shared__ int s_daon, s_skip;
     __shared__ long long s_logi;
+    // the slot's best state is written once per launch (or when the undo log
+    // fills): the current state with the moves made after the best undone
+    __shared__ double s_bc2;                 // best chi^2 so far
+    __shared__ int s_bimp, s_nu, s_flush;    // best improved, undo entries, flush now
+    __shared__ int s_gst, s_dsp, s_posd;     // best_pos stale, displaced since, copy pos
+    __shared__ int u_a[kUndo], u_b[kUndo];
+    __shared__ uint8_t u_sa[kUndo], u_sb[kUndo], u_sw[kUndo];
+    __shared__ double u_p[kUndo][3];
+    __shared__ int s_wcnt[NT / 32];          // non-zero MS entries per warp segment
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int slot = blockIdx.x;
@@ -543,6 +553,35 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     float *s_mpart = (float *)(smem + so.x);       // surrogate scratch, shares the
     float *s_mh = s_mpart + (NT / 32) * 256;       // transform's region
     auto spc = [s_sp](int i) { return (int)(s_sp[i] & 0x7F); };
+    // write the best state (every thread calls it, with s_bimp set): species
+    // and, if they changed since best_pos was written, positions; then undo
+    // the moves logged after the best point, newest first
+    auto flush_best = [&]() {
+        int *B = L.best_sp + (long)c * natoms;
+        double *BP = L.best_pos + (long)c * natoms * 3;
+        for (int q = tid; q < natoms; q += blockDim.x) B[q] = s_sp[q] & 0x7F;
+        if (s_posd)
+            for (int q = tid; q < 3 * natoms; q += blockDim.x) BP[q] = P[q];
+        __syncthreads();
+        if (tid == 0) {
+            int disp_after = 0;
+            for (int u = s_nu - 1; u >= 0; --u) {
+                B[u_a[u]] = u_sa[u];
+                B[u_b[u]] = u_sb[u];
+                if (!u_sw[u]) {
+                    disp_after = 1;
+                    if (s_posd)
+                        for (int x = 0; x < 3; ++x) BP[3 * u_a[u] + x] = u_p[u][x];
+                }
+            }
+            L.best_chi2[c] = s_bc2;
+            // best_pos now equals pos unless a displacement came after the best
+            s_gst = s_posd ? disp_after : (s_gst || s_dsp);
+            s_dsp = 0;
+            s_bimp = s_nu = s_flush = 0;
+        }
+        __syncthreads();
+    };
 
     if (tid == 0) {
         s_base = *(volatile uint64_t *)stepc;
@@ -550,6 +589,9 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         s_daon = DA && L.mlp != nullptr && L.da_on != nullptr && *L.da_on != 0;
         if (s_daon) s_mlp = *L.mlp;
         for (int q = 0; q < 4; ++q) s_dast[q] = 0.0;
+        s_bc2 = L.best_chi2[c];
+        s_bimp = s_nu = s_flush = s_dsp = s_posd = 0;
+        s_gst = L.best_stale ? L.best_stale[c] : 1;
     }
     if (tid <= NSP) s_msb[tid] = 0;
     for (int i = tid; i < natoms; i += blockDim.x)
@@ -713,22 +755,48 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             }
         }
         __syncthreads();
-        // compact: warp 0 the direct records, warp 1 the table counts, warp 2 the
-        // MS entries, as (index, count) pairs in ascending index order; the MS
-        // list is split into one run per absorber species (entry / nblk)
+        // compact, as (index, count) pairs in ascending index order: the MS
+        // entries by every warp (each counts the non-zero entries of its
+        // segment, then writes them from its offset), then warp 0 the direct
+        // records and warp 1 the table counts; the MS list is split into one
+        // run per absorber species (entry / nblk)
         int *l_dir = s_list;
         int2 *l_dn = (int2 *)(s_list + 2 * maxaff);
         int2 *l_ms = l_dn + ndn;
+        const int nwarp = blockDim.x >> 5;
+        const int mseg = (nent && swp) ? ((nent + nwarp - 1) / nwarp + 31) / 32 * 32 : 0;
+        const int ms0 = min(nent, warp * mseg), ms1 = min(nent, ms0 + mseg);
+        {
+            int cw = 0;
+            for (int i0 = ms0; i0 < ms1; i0 += 32) {
+                const int i = i0 + lane;
+                cw += __popc(__ballot_sync(0xffffffffu, i < ms1 && s_hist[i] != 0));
+            }
+            if (lane == 0) s_wcnt[warp] = cw;
+        }
+        __syncthreads();
+        {
+            int off = 0;
+            for (int w = 0; w < warp; ++w) off += s_wcnt[w];
+            for (int i0 = ms0; i0 < ms1; i0 += 32) {
+                const int i = i0 + lane;
+                const int v = i < ms1 ? s_hist[i] : 0;
+                const unsigned m = __ballot_sync(0xffffffffu, v != 0);
+                if (v != 0) l_ms[off + __popc(m & ((1u << lane) - 1))] = make_int2(i, v);
+                off += __popc(m);
+            }
+            if (warp == nwarp - 1 && lane == 0) s_nhist = off;
+        }
         if (warp == 0) {
             int n = warp_compact(2 * maxaff, [&](int i) { return s_dirv[i] != 0; }, l_dir);
             if (lane == 0) s_ndir = n;
         } else if (warp == 1) {
             int n = warp_compact_pairs(ndn, s_dn, l_dn);
             if (lane == 0) s_ndn = n;
-        } else if (warp == 2) {
-            int n = (nent && swp) ? warp_compact_pairs(nent, s_hist, l_ms) : 0;
-            if (lane == 0) s_nhist = n;
-            // first list position of each absorber block
+        }
+        __syncthreads();
+        if (warp == 2) {   // first list position of each absorber block
+            const int n = s_nhist;
             for (int a_ = lane; a_ <= NSP; a_ += 32) {
                 int lo = 0, hi = n, key = a_ * L.ms_nblk;
                 while (lo < hi) {
@@ -860,33 +928,50 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 for (int q = tid; q < nms; q += blockDim.x) C[l_ms[q].x] += l_ms[q].y;
             }
             if (tid == 0) {
+                const int n = s_nu;
+                const bool logm = s_bimp && !(s_c2 < s_bc2);   // a move after the best point
+                if (logm) {
+                    u_a[n] = a;
+                    u_b[n] = b;
+                    u_sa[n] = (uint8_t)sa_old;
+                    u_sb[n] = (uint8_t)sb_old;
+                    u_sw[n] = (uint8_t)swp;
+                }
                 s_sp[a] = (uint8_t)((s_sp[a] & 0x80) | nsa);
                 s_sp[b] = (uint8_t)((s_sp[b] & 0x80) | nsb);
                 Sg[a] = nsa;
                 Sg[b] = nsb;
                 if (!swp) {
+                    if (logm)
+                        for (int x = 0; x < 3; ++x) u_p[n][x] = P[3 * a + x];
                     P[3 * a] = prop.np[0];
                     P[3 * a + 1] = prop.np[1];
                     P[3 * a + 2] = prop.np[2];
                     s_sp[a] |= 0x80;
                     MVg[a] = 1;
+                    s_dsp = 1;
                 }
                 L.chi2[c] = s_c2;
                 L.n_acc[c] += 1;
+                if (s_c2 < s_bc2) {          // a new best: the current state
+                    s_bc2 = s_c2;
+                    s_bimp = 1;
+                    s_nu = 0;
+                    s_posd = s_gst || s_dsp;
+                } else if (logm) {
+                    s_nu = n + 1;
+                }
+                s_flush = s_bimp && s_nu == kUndo;
             }
             __syncthreads();
-            if (s_c2 < L.best_chi2[c]) {
-                int *B = L.best_sp + (long)c * natoms;
-                double *BP = L.best_pos + (long)c * natoms * 3;
-                for (int q = tid; q < natoms; q += blockDim.x) B[q] = s_sp[q] & 0x7F;
-                for (int q = tid; q < 3 * natoms; q += blockDim.x) BP[q] = P[q];
-                __syncthreads();
-                if (tid == 0) L.best_chi2[c] = s_c2;
-            }
+            if (s_flush) flush_best();
         }
         __syncthreads();
     }  // steps
     for (int q = tid; q < NSP * nk; q += blockDim.x) CHg[q] = s_chi[q];
+    __syncthreads();
+    if (s_bimp) flush_best();
+    if (tid == 0 && L.best_stale) L.best_stale[c] = (uint8_t)(s_gst || s_dsp);
     if (da_on && tid == 0 && L.da_stat)
         for (int q = 0; q < 4; ++q) L.da_stat[(long)c * 4 + q] += s_dast[q];
     __syncthreads();

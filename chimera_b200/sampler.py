@@ -134,11 +134,14 @@ class Ladders:
         self.keep.append(t)
         return t
 
-    def _build_ladder(self, li, s, slot0):
-        torch = self.torch
-        fm = s.fm
-        L = self.host[li]
-        nsp, nk, nrep = self.nsp, fm.nk, s.nrep
+    def _supercell(self, fm):
+        """Per-supercell device data shared by every ladder on the same
+        ForwardModel: reverse pair index, ideal sites, shifts, sigma^2, the
+        pairs that may use the (shell, type) table and the shell radii."""
+        cache = self.__dict__.setdefault("_cell_cache", {})
+        key = id(fm)
+        if key in cache:
+            return cache[key]
         i_np, j_np = fm.i_idx, fm.j_idx
         natoms = fm.natoms
         z = np.bincount(i_np, minlength=natoms)
@@ -158,8 +161,21 @@ class Ladders:
         pair_tab = ((np.abs(d0 - r_shell[shell]) <= 1e-12 * r_shell[shell])
                     & (sig2 == s2_shell[shell]))
         pair_tab = (pair_tab & pair_tab[rev]).astype(np.uint8)   # a pair and its reverse agree
-        b = dict(rev=self._t(rev), ideal=self._t(ideal), shift=self._t(shift),
-                 sig2=self._t(sig2), pair_tab=self._t(pair_tab))
+        c = dict(ncoord=ncoord, r_shell=r_shell, s2_shell=s2_shell, fm=fm,
+                 dev=dict(rev=self._t(rev), ideal=self._t(ideal), shift=self._t(shift),
+                          sig2=self._t(sig2), pair_tab=self._t(pair_tab)))
+        cache[key] = c
+        return c
+
+    def _build_ladder(self, li, s, slot0):
+        torch = self.torch
+        fm = s.fm
+        L = self.host[li]
+        nsp, nk, nrep = self.nsp, fm.nk, s.nrep
+        natoms = fm.natoms
+        cell = self._supercell(fm)
+        ncoord, r_shell, s2_shell = cell["ncoord"], cell["r_shell"], cell["s2_shell"]
+        b = dict(cell["dev"])
         L.natoms, L.ncoord, L.npairs, L.nshell, L.nsp, L.nk = (natoms, ncoord, fm.npairs,
                                                               fm.nshell, nsp, nk)
         L.iidx, L.jidx, L.rev = N.dptr(fm.d_i), N.dptr(fm.d_j), N.dptr(b["rev"])
@@ -172,16 +188,18 @@ class Ladders:
                       fm.d_dr, fm.d_c3, fm.d_s2tab]
         L.s02 = fm.s02
         if self.use_table:
-            b["sstab"] = torch.empty((fm.nshell * nsp * nsp, nk), dtype=torch.float64,
-                                     device="cuda")
-            self.keep.append(b["sstab"])
-            L.sstab = N.dptr(b["sstab"])
-            rs, ss = self._t(r_shell), self._t(s2_shell)
-            N.call("chx_shell_table", C.byref(L), N.ptr(rs), N.ptr(ss), N.ptr(b["sstab"]),
-                   N.stream())
-            b["sstab32"] = b["sstab"].float().contiguous()
-            self.keep.append(b["sstab32"])
-            L.sstab32 = N.dptr(b["sstab32"])
+            if "sstab" not in cell:      # the (shell, type) table, once per supercell
+                cell["sstab"] = torch.empty((fm.nshell * nsp * nsp, nk), dtype=torch.float64,
+                                            device="cuda")
+                self.keep.append(cell["sstab"])
+                L.sstab = N.dptr(cell["sstab"])
+                rs, ss = self._t(r_shell), self._t(s2_shell)
+                N.call("chx_shell_table", C.byref(L), N.ptr(rs), N.ptr(ss),
+                       N.ptr(cell["sstab"]), N.stream())
+                cell["sstab32"] = cell["sstab"].float().contiguous()
+                self.keep.append(cell["sstab32"])
+            b["sstab"], b["sstab32"] = cell["sstab"], cell["sstab32"]
+            L.sstab, L.sstab32 = N.dptr(b["sstab"]), N.dptr(b["sstab32"])
         else:
             L.sstab, L.sstab32 = 0, 0
         # exact multiple scattering
@@ -192,8 +210,11 @@ class Ladders:
             L.ms_tpl, L.ms_nbr, L.ms_T = N.dptr(d["tpl"]), N.dptr(d["nbr"]), N.dptr(ms.T)
             self.keep += [d["tpl"], d["nbr"], ms.T]
             if self.precision != FP64:
-                b["msT32"] = ms.T.float().contiguous()
-                self.keep.append(b["msT32"])
+                key = ("msT32", id(ms))
+                if key not in cell:
+                    cell[key] = ms.T.float().contiguous()
+                    self.keep.append(cell[key])
+                b["msT32"] = cell[key]
                 L.ms_T32 = N.dptr(b["msT32"])
             else:
                 L.ms_T32 = 0
@@ -257,10 +278,11 @@ class Ladders:
                  acc=torch.zeros(nrep, dtype=torch.uint8, device="cuda"),
                  acc_log=torch.zeros((MAX_BLOCK, nrep), dtype=torch.uint8, device="cuda"),
                  n_acc=z32(nrep),
-                 exch_att=z32(max(nrep, 1)), exch_acc=z32(max(nrep, 1)))
+                 exch_att=z32(max(nrep, 1)), exch_acc=z32(max(nrep, 1)),
+                 best_stale=torch.ones(nrep, dtype=torch.uint8, device="cuda"))
         for key in ("species", "pos", "moved", "chi", "chi2", "count", "rung_of", "slot_of",
                     "best_chi2", "best_sp", "best_pos", "ms_C", "acc", "acc_log", "n_acc",
-                    "exch_att", "exch_acc"):
+                    "exch_att", "exch_acc", "best_stale"):
             self.keep.append(b[key])
         L.species, L.pos, L.moved, L.chi = (N.dptr(b["species"]), N.dptr(b["pos"]),
                                             N.dptr(b["moved"]), N.dptr(b["chi"]))
@@ -271,6 +293,7 @@ class Ladders:
         L.ms_C, L.acc_rung, L.n_acc = N.dptr(b["ms_C"]), N.dptr(b["acc"]), N.dptr(b["n_acc"])
         L.acc_log = N.dptr(b["acc_log"])
         L.exch_att, L.exch_acc = N.dptr(b["exch_att"]), N.dptr(b["exch_acc"])
+        L.best_stale = N.dptr(b["best_stale"])
         b["beta_host"] = beta
         b["cplx"] = cplx
         return b
@@ -304,12 +327,14 @@ class Ladders:
         b["pos"].copy_(torch.from_numpy(pos))
         ideal = _host(fm.cell.ideal)
         b["moved"].copy_(torch.from_numpy(np.any(pos != ideal[None], axis=-1).astype(np.uint8)))
-        chi = fm.chi_full(b["pos"], b["species"], precision=FP64)
+        # every rung starts from the same configuration: evaluate it once
+        chi = fm.chi_full(b["pos"][:1].contiguous(), b["species"][:1].contiguous(),
+                          precision=FP64)
         if s.ms is not None:
-            C_ = s.ms.counts(b["species"])
-            b["ms_C"].copy_(C_)
+            C_ = s.ms.counts(b["species"][:1].contiguous())
+            b["ms_C"].copy_(C_.expand(nrep, -1))
             chi = chi + s.ms.chi_of(C_)
-        b["chi"].copy_(chi)
+        b["chi"].copy_(chi.expand(nrep, -1, -1))
         cnt = np.stack([(sp == q).sum(1) for q in range(self.nsp)], axis=1).astype(np.float64)
         b["count"].copy_(torch.from_numpy(cnt))
         b["rung_of"].copy_(torch.arange(nrep, dtype=torch.int32))
@@ -338,6 +363,7 @@ class Ladders:
                 b["best_chi2"].copy_(b["chi2"])
                 b["best_sp"].copy_(b["species"])
                 b["best_pos"].copy_(b["pos"])
+                b["best_stale"].zero_()
 
     def reanchor(self, mask=None):
         """Replace the running chi of the slots in `mask` (a (nslots,) bool
@@ -393,11 +419,13 @@ class Ladders:
         if "feat_nbr" not in b:
             from .surrogate import feature_neighbours
             fm = self.specs[li].fm
-            nbr = feature_neighbours(_host(fm.cell.ideal), fm.i_idx, fm.j_idx,
-                                     _host(fm.d_shift), L.ncoord)
-            b["feat_nbr"] = self._t(nbr)
-            b["feat_nbr_host"] = nbr
-            L.feat_nbr, L.feat_D = N.dptr(b["feat_nbr"]), int(nbr.shape[1])
+            cell = self._supercell(fm)
+            if "feat" not in cell:       # once per supercell
+                nbr = feature_neighbours(_host(fm.cell.ideal), fm.i_idx, fm.j_idx,
+                                         _host(fm.d_shift), L.ncoord)
+                cell["feat"] = (nbr, self._t(nbr))
+            b["feat_nbr_host"], b["feat_nbr"] = cell["feat"]
+            L.feat_nbr, L.feat_D = N.dptr(b["feat_nbr"]), int(b["feat_nbr_host"].shape[1])
         return b["feat_nbr_host"]
 
     def _da_buffers(self, li):

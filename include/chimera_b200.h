@@ -338,6 +338,9 @@ typedef struct {
     float *log_y;                    /* (log_cap, 4): sigma * d, ln beta, chain
                                         (slot0 + rung), step                     */
     int64_t log_cap;
+    /* (nrep) 1 where pos may differ from best_pos (a displacement since
+       best_pos was written), 0 where they are equal; NULL: always copy */
+    uint8_t *best_stale;
 } chx_ladder_t;
 
 /* Bytes of dynamic shared memory the step kernel needs for these ladders. */

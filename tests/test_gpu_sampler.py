@@ -124,3 +124,32 @@ def test_uneven_batch_equals_separate_runs(cuda):
         alone = run([s])[0]
         for k, v in alone.items():
             assert np.array_equal(together[i][k], v), (i, k)
+
+
+def test_best_state_is_the_state_of_the_best_chi2(cuda):
+    """The best state is written once per launch (or when its log of later
+    moves fills up) as the current state with the moves after the best
+    undone. After single launches of 250 FP64 steps with displacements on,
+    enough for that log to fill, every slot's best species and positions
+    give back its best chi^2 exactly."""
+    import torch
+    d = trace_inputs("rmc_trace.npz")
+    d["swap_frac"] = np.float64(0.5)
+    d["tmin"], d["tmax"] = np.float64(1e2), np.float64(1e4)
+    smp, fm = device_objects(d, precision=0, reproduce=False)
+    smp.init_state(d["species0"], d["ideal"])
+    lad, b = smp.lad, smp.b
+    most = 0
+    for _ in range(3):
+        flags = smp.steps(250)
+        most = max(most, int(flags.sum(0).max()))
+    assert most >= 40          # some rung accepted more moves than the log holds
+    assert int(b["moved"].sum()) > 0
+    bsp, bpos = b["best_sp"], b["best_pos"]
+    chi = fm.chi_full(bpos, bsp)
+    cnt = torch.stack([(bsp == s).sum(1) for s in range(d["nsp"])], 1).double()
+    c2 = lad.eval_chi2(chi.contiguous(), cnt.contiguous()).cpu().numpy()
+    best = b["best_chi2"].cpu().numpy()
+    assert np.allclose(c2, best, rtol=1e-10, atol=0), (c2, best)
+    assert (best <= b["chi2"].cpu().numpy() + 1e-12).all()
+    assert lad.device_error() == 0
