@@ -9,14 +9,15 @@
 // precision 1: FP32 SIMT tiles.
 // precision 2: split-BF16 three-product on the tcgen05 tensor cores with FP32
 //              accumulation in tensor memory (chx_ft_tc.cu).
+// precision 3: TF32, one tcgen05 product, FP32 accumulation (chx_ft_tc.cu).
 #include <algorithm>
 #include "chx_common.cuh"
 
 namespace chx {
 
 int ft_batch_tc(const double *chi, int rows, int nk, const double *basis, int nR, double *out,
-                void *scratch, int64_t scratch_bytes, cudaStream_t st);
-int64_t ft_batch_tc_scratch(int rows, int nk, int nR);
+                void *scratch, int64_t scratch_bytes, cudaStream_t st, bool tf32);
+int64_t ft_batch_tc_scratch(int rows, int nk, int nR, bool tf32);
 
 // 64 x 64 output tile per CTA, 256 threads, 4 x 4 outputs per thread
 template <typename T>
@@ -72,7 +73,7 @@ extern "C" {
 
 int64_t chx_ft_batch_scratch_bytes(int rows, int nk, int nR, int precision) {
     if (rows <= 0 || nk <= 0 || nR <= 0) return -1;
-    if (precision == 2) return ft_batch_tc_scratch(rows, nk, nR);
+    if (precision == 2 || precision == 3) return ft_batch_tc_scratch(rows, nk, nR, precision == 3);
     return 0;
 }
 
@@ -87,8 +88,9 @@ int chx_ft_batch(const double *chi, int rows, int nk, const double *basis, int n
         k_ft_simt<double><<<grid, 256, 0, st>>>(chi, rows, nk, basis, ncol, out);
     } else if (precision == 1) {
         k_ft_simt<float><<<grid, 256, 0, st>>>(chi, rows, nk, basis, ncol, out);
-    } else if (precision == 2) {
-        return ft_batch_tc(chi, rows, nk, basis, nR, out, scratch, scratch_bytes, st);
+    } else if (precision == 2 || precision == 3) {
+        return ft_batch_tc(chi, rows, nk, basis, nR, out, scratch, scratch_bytes, st,
+                           precision == 3);
     } else {
         set_error("ft_batch: bad precision %d", precision);
         return CHX_ERR_ARG;

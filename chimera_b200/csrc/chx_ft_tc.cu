@@ -1,24 +1,28 @@
 // chx_ft_tc.cu -- the windowed FT contraction out = chi . B on the tcgen05
-// tensor cores (A5, precision 2 of chx_ft_batch).
+// tensor cores (A5, precisions 2 and 3 of chx_ft_batch).
 //
-// Each FP64 operand x is split into two BF16 numbers, x_hi = bf16(x) and
-// x_lo = bf16(x - x_hi); a product a.b is taken as a_hi b_hi + a_hi b_lo +
-// a_lo b_hi (the a_lo b_lo term is below 2^-16 of it), three BF16 MMAs with
-// FP32 accumulation in tensor memory, which keeps about 16 significant bits
-// per product where one BF16 product keeps 8.
+// Split-BF16 (precision 2): each FP64 operand x is split into two BF16
+// numbers, x_hi = bf16(x) and x_lo = bf16(x - x_hi); a product a.b is taken
+// as a_hi b_hi + a_hi b_lo + a_lo b_hi (the a_lo b_lo term is below 2^-16 of
+// it), three BF16 MMAs (kind::f16) with FP32 accumulation in tensor memory,
+// which keeps about 16 significant bits per product where one BF16 product
+// keeps 8. TF32 (precision 3): the operands rounded to TF32 (10-bit
+// mantissa), one MMA (kind::tf32) per product, FP32 accumulation.
 //
 // Layout. The basis (2 nR x nk, transposed) is split by a pre-pass
-// (k_tc_split) into hi and lo 128 x 32 tiles in scratch, each 8 KB tile
-// already in the no-swizzle K-major shared-memory layout the MMA reads:
-// 8 x 16-byte core matrices, 128 B apart along K and 512 B apart along rows.
+// (k_tc_split) into 128 x 32 tiles in scratch (hi and lo BF16, or TF32),
+// each already in the no-swizzle K-major shared-memory layout the MMA reads:
+// 8 x 16-byte core matrices, 128 B apart along K and one row group (K bytes
+// / 16 core matrices) apart along rows.
 // The main kernel (k_ft_tc, one 128 x 128 output tile per CTA, three CTAs per
 // SM) runs a two-stage ring over 32-wide K chunks: one thread brings the
 // chunk's basis tiles in with bulk-async copies (cp.async.bulk, no
 // multicast) completing on an mbarrier while all 128 threads read the chunk
 // of chi (FP64, any row alignment) and write its hi and lo parts straight
 // into the same layout (each warp load 256 contiguous bytes of one row);
-// one thread then issues the 2 x 3 MMAs (128 x 128 x 16
-// each) into one 128 x 128 FP32 accumulator in tensor memory and commits them
+// one thread then issues the chunk's MMAs (2 x 3 of 128 x 128 x 16 BF16, or
+// 4 of 128 x 128 x 8 TF32) into one 128 x 128 FP32 accumulator in tensor
+// memory and commits them
 // to the stage's mbarrier, and the threads move on to the next chunk while
 // the tensor core works. Four warps finally read the accumulator (lane =
 // row) with tcgen05.ld, turn each 32 x 32 block around in shared memory and
@@ -32,20 +36,31 @@
 
 namespace chx {
 
-constexpr int kTcM = 128, kTcN = 128, kTcK = 32;        // CTA tile; MMA 128 x 128 x 16
-constexpr uint32_t kTcTileA = kTcM * kTcK * 2;          // chi operand tile, 8 KB
-constexpr uint32_t kTcTileB = kTcN * kTcK * 2;          // basis operand tile, 16 KB
-constexpr uint32_t kTcStage = 2 * kTcTileA + 2 * kTcTileB;   // A_hi, A_lo, B_hi, B_lo
+constexpr int kTcM = 128, kTcN = 128, kTcK = 32;        // CTA tile and K chunk
 constexpr int kTcStages = 2;
-constexpr uint32_t kTcLBO = 128, kTcSBO = (kTcK / 8) * 128;   // core-matrix strides (bytes)
+constexpr uint32_t kTcLBO = 128;                        // core matrices along K (bytes)
 constexpr int kTcSpin = 1 << 24;
 constexpr int kTcTmemCols = kTcN;                       // FP32 accumulator columns
-constexpr size_t kTcSmem = (size_t)kTcStages * kTcStage + 1024;
 
-// byte offset of element (r, k) inside one operand tile of 32 K values
-__host__ __device__ __forceinline__ uint32_t tc_tile_off(int r, int k) {
-    return (uint32_t)((r >> 3) * kTcSBO + (k >> 3) * kTcLBO + (r & 7) * 16 + (k & 7) * 2);
-}
+// Operand modes: split-BF16 (two BF16 parts of 2 bytes, MMA K = 16, kind::f16
+// with A and B BF16) and TF32 (one 4-byte part, MMA K = 8, kind::tf32); both
+// D FP32, A and B K-major, N = M = 128 in the instruction descriptor.
+template <bool TF32>
+struct TcMode {
+    static constexpr int esz = TF32 ? 4 : 2, parts = TF32 ? 1 : 2, kmma = TF32 ? 8 : 16;
+    static constexpr uint32_t sbo = (uint32_t)(kTcK * esz / 16) * 128;   // row group stride
+    static constexpr uint32_t tileA = kTcM * kTcK * esz, tileB = kTcN * kTcK * esz;
+    static constexpr uint32_t stage = parts * (tileA + tileB);
+    static constexpr uint32_t fmt = TF32 ? 2u : 1u;
+    static constexpr uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) |
+                                      ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+    static constexpr size_t smem = (size_t)kTcStages * stage + 1024;
+    // byte offset of element (r, k) inside one operand tile of kTcK values
+    static __host__ __device__ __forceinline__ uint32_t off(int r, int k) {
+        return (uint32_t)((r >> 3) * sbo + (k * esz / 16) * kTcLBO + (r & 7) * 16 +
+                          (k * esz) % 16);
+    }
+};
 
 __device__ __forceinline__ uint32_t tc_smem(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -53,15 +68,10 @@ __device__ __forceinline__ uint32_t tc_smem(const void *p) {
 
 // shared-memory matrix descriptor: start address, leading (K) and stride
 // (row-group) byte offsets, descriptor version 1, no swizzle
-__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t sbo) {
     return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)(kTcLBO >> 4) << 16) |
-           ((uint64_t)(kTcSBO >> 4) << 32) | (1ull << 46);
+           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
 }
-
-// instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major,
-// N = 128, M = 128
-constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
-                              ((uint32_t)(kTcM >> 4) << 24);
 
 __device__ __forceinline__ void tc_mbar_init(uint64_t *bar) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(bar)) : "memory");
@@ -82,11 +92,12 @@ __device__ __forceinline__ bool tc_mbar_wait(uint64_t *bar, uint32_t parity) {
     return false;
 }
 
-__device__ __forceinline__ void tc_load_tile(void *dst, const void *src, uint64_t *bar) {
+__device__ __forceinline__ void tc_load_tile(void *dst, const void *src, uint32_t bytes,
+                                             uint64_t *bar) {
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
             "r"(tc_smem(dst)),
-        "l"(src), "r"(kTcTileB), "r"(tc_smem(bar))
+        "l"(src), "r"(bytes), "r"(tc_smem(bar))
         : "memory");
 }
 
@@ -96,14 +107,33 @@ __device__ __forceinline__ void tc_expect(uint64_t *bar, uint32_t bytes) {
                  : "memory");
 }
 
+template <bool TF32>
 __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-            tmem),
-        "l"(da), "l"(db), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-        : "memory");
+    if constexpr (TF32)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::
+                "r"(tmem),
+            "l"(da), "l"(db), "r"(TcMode<true>::idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u),
+            "r"(0u)
+            : "memory");
+    else
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::
+                "r"(tmem),
+            "l"(da), "l"(db), "r"(TcMode<false>::idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u),
+            "r"(0u)
+            : "memory");
+}
+
+// x rounded to TF32 (nearest, ties away), kept in an FP32 container
+__device__ __forceinline__ uint32_t tc_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
 }
 
 __device__ __forceinline__ void tc_commit(uint64_t *bar) {
@@ -113,24 +143,32 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
         : "memory");
 }
 
-// hi / lo BF16 parts of X (R x C, element (r, c) at X[r*sr + c*sc]) zero-padded
-// to Rp x Kp, written as 128 x 32 tiles (tile (rt, kt) at (rt * Kp/32 + kt))
+// the operand parts of X (R x C, element (r, c) at X[r*sr + c*sc]) zero-padded
+// to Rp x Kp, written as 128 x 32 tiles (tile (rt, kt) at (rt * Kp/32 + kt)):
+// hi and lo BF16, or TF32 into hi
+template <bool TF32>
 __global__ void k_tc_split(const double *__restrict__ X, int R, int C, long sr, long sc, int Rp,
                            int Kp, uint8_t *__restrict__ hi, uint8_t *__restrict__ lo) {
+    typedef TcMode<TF32> Md;
     const long n = (long)Rp * Kp;
     for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
          q += (long)gridDim.x * blockDim.x) {
         const int r = (int)(q / Kp), k = (int)(q % Kp);
         const double x = (r < R && k < C) ? X[r * sr + k * sc] : 0.0;
-        const __nv_bfloat16 h = __double2bfloat16(x);
-        const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
-        const long off = ((long)(r / kTcN) * (Kp / kTcK) + k / kTcK) * kTcTileB +
-                         tc_tile_off(r % kTcN, k % kTcK);
-        *(__nv_bfloat16 *)(hi + off) = h;
-        *(__nv_bfloat16 *)(lo + off) = l;
+        const long off = ((long)(r / kTcN) * (Kp / kTcK) + k / kTcK) * Md::tileB +
+                         Md::off(r % kTcN, k % kTcK);
+        if constexpr (TF32) {
+            *(uint32_t *)(hi + off) = tc_tf32((float)x);
+        } else {
+            const __nv_bfloat16 h = __double2bfloat16(x);
+            const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+            *(__nv_bfloat16 *)(hi + off) = h;
+            *(__nv_bfloat16 *)(lo + off) = l;
+        }
     }
 }
 
+template <bool TF32>
 __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi, int rows,
                                                   int nk, const uint8_t *__restrict__ Bhi,
                                                   const uint8_t *__restrict__ Blo, int nkt,
@@ -141,6 +179,7 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     uint8_t *ring = (uint8_t *)(((uintptr_t)tc_raw + 1023) & ~(uintptr_t)1023);
+    typedef TcMode<TF32> Md;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nt = blockIdx.x, mt = blockIdx.y;
 
@@ -165,14 +204,14 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
 
-    const long tstride = (long)nkt * kTcTileB;               // one row of basis tiles
+    const long tstride = (long)nkt * Md::tileB;              // one row of basis tiles
     const uint8_t *b_hi = Bhi + nt * tstride, *b_lo = Blo + nt * tstride;
     const int row0 = mt * kTcM;
     int issued[kTcStages] = {0, 0}, landed[kTcStages] = {0, 0};
     for (int kt = 0; kt < nkt; ++kt) {
         const int s = kt & 1;
         const uint32_t par = (uint32_t)((kt >> 1) & 1);
-        uint8_t *st = ring + (size_t)s * kTcStage;
+        uint8_t *st = ring + (size_t)s * Md::stage;
         // the stage's previous MMAs (chunk kt - 2) must be done before it is refilled
         if (kt >= kTcStages && !s_fail) {
             if (tid == 0 && !tc_mbar_wait(&freed[s], par ^ 1)) s_fail = 1;
@@ -180,9 +219,11 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi
         __syncthreads();
         if (s_fail) break;
         if (tid == 0) {
-            tc_expect(&full[s], 2 * kTcTileB);
-            tc_load_tile(st + 2 * kTcTileA, b_hi + (long)kt * kTcTileB, &full[s]);
-            tc_load_tile(st + 2 * kTcTileA + kTcTileB, b_lo + (long)kt * kTcTileB, &full[s]);
+            // stage: A parts (tileA each), then B parts (tileB each)
+            uint8_t *sb = st + Md::parts * Md::tileA;
+            tc_expect(&full[s], Md::parts * Md::tileB);
+            tc_load_tile(sb, b_hi + (long)kt * Md::tileB, Md::tileB, &full[s]);
+            if (!TF32) tc_load_tile(sb + Md::tileB, b_lo + (long)kt * Md::tileB, Md::tileB, &full[s]);
             ++issued[s];
         }
         // chi chunk, 128 rows x 32 k: lane = k, warp w takes rows w, w + 4, ...,
@@ -198,11 +239,15 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi
             }
 #pragma unroll
             for (int i = 0; i < kTcM / 4; ++i) {
-                const __nv_bfloat16 h = __double2bfloat16(v[i]);
-                const __nv_bfloat16 l = __double2bfloat16(v[i] - (double)__bfloat162float(h));
-                const uint32_t off = tc_tile_off(warp + 4 * i, lane);
-                *(__nv_bfloat16 *)(st + off) = h;
-                *(__nv_bfloat16 *)(st + kTcTileA + off) = l;
+                const uint32_t off = Md::off(warp + 4 * i, lane);
+                if constexpr (TF32) {
+                    *(uint32_t *)(st + off) = tc_tf32((float)v[i]);
+                } else {
+                    const __nv_bfloat16 h = __double2bfloat16(v[i]);
+                    const __nv_bfloat16 l = __double2bfloat16(v[i] - (double)__bfloat162float(h));
+                    *(__nv_bfloat16 *)(st + off) = h;
+                    *(__nv_bfloat16 *)(st + Md::tileA + off) = l;
+                }
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -214,15 +259,19 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi
                 ++landed[s];
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t base = tc_smem(st);
+                const uint32_t bbase = base + Md::parts * Md::tileA;
 #pragma unroll
-                for (int kk = 0; kk < kTcK / 16; ++kk) {
-                    const uint32_t ko = kk * 2 * kTcLBO;   // 16 K values = two core matrices
-                    const uint64_t ahi = tc_desc(base + ko), alo = tc_desc(base + kTcTileA + ko);
-                    const uint64_t bhi = tc_desc(base + 2 * kTcTileA + ko),
-                                   blo = tc_desc(base + 2 * kTcTileA + kTcTileB + ko);
-                    tc_mma(tmem, ahi, bhi, (kt | kk) != 0);
-                    tc_mma(tmem, ahi, blo, 1u);
-                    tc_mma(tmem, alo, bhi, 1u);
+                for (int kk = 0; kk < kTcK / Md::kmma; ++kk) {
+                    const uint32_t ko = kk * 2 * kTcLBO;   // one MMA's K = two core matrices
+                    const uint64_t ahi = tc_desc(base + ko, Md::sbo);
+                    const uint64_t bhi = tc_desc(bbase + ko, Md::sbo);
+                    tc_mma<TF32>(tmem, ahi, bhi, (kt | kk) != 0);
+                    if constexpr (!TF32) {
+                        const uint64_t alo = tc_desc(base + Md::tileA + ko, Md::sbo);
+                        const uint64_t blo = tc_desc(bbase + Md::tileB + ko, Md::sbo);
+                        tc_mma<TF32>(tmem, ahi, blo, 1u);
+                        tc_mma<TF32>(tmem, alo, bhi, 1u);
+                    }
                 }
                 tc_commit(&freed[s]);
             }
@@ -285,26 +334,30 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi
 
 struct TcPlan {
     int Mp, Np, Kp;
-    size_t a_bytes, b_bytes, total;
+    size_t b_bytes, total;
 };
-static TcPlan tc_plan(int rows, int nk, int nR) {
+// chi is split inside the main kernel; the basis parts go to scratch
+static TcPlan tc_plan(int rows, int nk, int nR, bool tf32) {
     TcPlan p;
     p.Mp = (rows + kTcM - 1) / kTcM * kTcM;
     p.Np = (2 * nR + kTcN - 1) / kTcN * kTcN;
     p.Kp = (nk + kTcK - 1) / kTcK * kTcK;
-    p.a_bytes = 0;                              // chi is split inside the main kernel
-    p.b_bytes = (size_t)p.Np * p.Kp * 2;       // Np is a multiple of the basis tile rows
-    p.total = 256 + 2 * p.b_bytes;
+    p.b_bytes = (size_t)p.Np * p.Kp * (tf32 ? 4 : 2);
+    p.total = 256 + (tf32 ? 1 : 2) * p.b_bytes;
     return p;
 }
 
-int64_t ft_batch_tc_scratch(int rows, int nk, int nR) { return (int64_t)tc_plan(rows, nk, nR).total; }
+int64_t ft_batch_tc_scratch(int rows, int nk, int nR, bool tf32) {
+    return (int64_t)tc_plan(rows, nk, nR, tf32).total;
+}
 
-int ft_batch_tc(const double *chi, int rows, int nk, const double *basis, int nR, double *out,
-                void *scratch, int64_t scratch_bytes, cudaStream_t st) {
-    const TcPlan p = tc_plan(rows, nk, nR);
+template <bool TF32>
+static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *basis, int nR,
+                            double *out, void *scratch, int64_t scratch_bytes, cudaStream_t st) {
+    typedef TcMode<TF32> Md;
+    const TcPlan p = tc_plan(rows, nk, nR, TF32);
     CHX_REQUIRE(scratch && scratch_bytes >= (int64_t)p.total,
-                "ft_batch: split-BF16 path needs %zu bytes of scratch", p.total);
+                "ft_batch: the tensor-core path needs %zu bytes of scratch", p.total);
     CHX_REQUIRE(((uintptr_t)scratch & 255) == 0, "ft_batch: scratch must be 256-byte aligned");
     uint8_t *base = (uint8_t *)scratch;
     int *err = (int *)base;
@@ -313,14 +366,23 @@ int ft_batch_tc(const double *chi, int rows, int nk, const double *basis, int nR
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch memset");
     const int ncol = 2 * nR;
     const long nb = (long)p.Np * p.Kp;
-    k_tc_split<<<(unsigned)std::min<long>((nb + 255) / 256, 592), 256, 0, st>>>(
+    k_tc_split<TF32><<<(unsigned)std::min<long>((nb + 255) / 256, 592), 256, 0, st>>>(
         basis, ncol, nk, 1, ncol, p.Np, p.Kp, bhi, bl);
-    e = cudaFuncSetAttribute(k_ft_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    e = cudaFuncSetAttribute(k_ft_tc<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)Md::smem);
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc attribute");
     dim3 grid(p.Np / kTcN, p.Mp / kTcM);
-    k_ft_tc<<<grid, 128, kTcSmem, st>>>(chi, rows, nk, bhi, bl, p.Kp / kTcK, ncol, out, err);
+    k_ft_tc<TF32><<<grid, 128, Md::smem, st>>>(chi, rows, nk, bhi, bl, p.Kp / kTcK, ncol, out,
+                                               err);
     CHX_CHECK_LAUNCH("ft_batch tc");
     return CHX_OK;
+}
+
+int ft_batch_tc(const double *chi, int rows, int nk, const double *basis, int nR, double *out,
+                void *scratch, int64_t scratch_bytes, cudaStream_t st, bool tf32) {
+    return tf32 ? ft_batch_tc_mode<true>(chi, rows, nk, basis, nR, out, scratch, scratch_bytes, st)
+                : ft_batch_tc_mode<false>(chi, rows, nk, basis, nR, out, scratch, scratch_bytes,
+                                          st);
 }
 
 }  // namespace chx

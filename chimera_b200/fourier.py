@@ -157,7 +157,7 @@ def apply_basis(chi, B, precision=0):
     scr = torch.empty(max(nsc, 1), dtype=torch.uint8, device="cuda")
     N.call("chx_ft_batch", N.ptr(x), rows, nk, N.ptr(Bd), nb, precision, N.ptr(out), N.ptr(scr),
            nsc, N.stream())
-    if precision == 2 and int(scr[:4].view(torch.int32).item()):
+    if precision in (2, 3) and int(scr[:4].view(torch.int32).item()):
         raise N.ChxError("chx_ft_batch: the tensor-core contraction gave up a bounded wait")
     z = torch.view_as_complex(out.view(rows, nb, 2)).reshape(lead + (nb,))
     return z.cpu().numpy() if host else z

@@ -403,8 +403,10 @@ CHX_API int chx_apply_exchange(const chx_ladder_t *d_ladders, int ladder, const 
  * 5. Windowed FT of a batch of spectra to chi(R) on arbitrary R points (A5,
  *    fourier.py:75-80 generalised to a direct transform). X (rows, nR) complex
  *    interleaved; basis (nk, nR) complex = w(k) k^kw dk/sqrt(pi) e^{-2ikR}.
- *    precision: 0 FP64 (SIMT), 1 TF32-class (FP32 SIMT), 2 split-BF16
- *    three-product on tcgen05 tensor cores with FP32 accumulation.
+ *    precision: 0 FP64 (SIMT), 1 FP32 (SIMT), 2 split-BF16 three-product on
+ *    the tcgen05 tensor cores with FP32 accumulation, 3 TF32 on the tcgen05
+ *    tensor cores (one product, FP32 accumulation). Precisions 2 and 3 write
+ *    a device error word (CHX_DEVERR_*) into the first 4 bytes of scratch.
  * ------------------------------------------------------------------------ */
 CHX_API int chx_ft_batch(const double *chi, int rows, int nk, const double *basis, int nR,
                  int precision, double *out, void *scratch, int64_t scratch_bytes,
