@@ -420,6 +420,15 @@ def main():
     d2h = NPOS * (prob.cell.natoms * 4 + 8)
     e2e_val = smp2.nslots * EXCH * (e2e_blocks + 1) / e2e_dt
     err = smp.lad.device_error()
+    # chi error vs FP64: the running FP32C chi of every replica against an
+    # FP64 recompute of its state (per absorber), after the timed run
+    chi_err = 0.0
+    for li, bb in enumerate(smp.lad.bufs):
+        spec = smp.lad.specs[li]
+        full = spec.fm.chi_full(bb["pos"], bb["species"])
+        if spec.ms is not None:
+            full = full + spec.ms.chi_of(bb["ms_C"])
+        chi_err = max(chi_err, float(((bb["chi"] - full) / bb["count"][:, :, None]).abs().max()))
     best_all = np.array([[b[1]] for b in best])
     if world > 1:
         # the one collective of the sharded run: per-ladder summaries (ladders
@@ -454,6 +463,9 @@ def main():
             "gpu_launches": args.steps * 2,
             "clocks": clocks,
             "device_error": err,
+            "chi_err_vs_fp64": {"value": chi_err, "unit": "max |chi - chi_FP64| per absorber",
+                                "note": "running FP32C chi of all replicas after the timed "
+                                        "run vs an FP64 path sum of their states"},
             "reanchors": smp.reanchors,
             "autotune": tuning,
             "best_chi2_min": float(np.nanmin(best_all)),
