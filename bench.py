@@ -322,6 +322,109 @@ def bench_ft(args):
     return 0
 
 
+def r_factors(bs, prob):
+    """R-factor of each ladder's best state (chimera/model.py:535-540 with the
+    per-edge profiled scales of model.py:495-510): sum |s m - d|^2 / sum |d|^2
+    over the fit window, m the model chi(R) of the state, d the target."""
+    import torch
+    out = []
+    for li, spec in enumerate(bs.lad.specs):
+        sp, _ = bs.best(li)
+        sp_d = torch.from_numpy(sp[None].astype(np.int32)).cuda()
+        chi = spec.fm.chi_full(torch.from_numpy(prob.cell.ideal[None]).cuda(), sp_d)
+        if spec.ms is not None:
+            chi = chi + spec.ms.full(sp_d)
+        cnt = torch.from_numpy(np.bincount(sp, minlength=prob.nsp).astype(np.float64)).cuda()
+        m = prob.ft.to_R(chi[0] / cnt.clamp_min(1)[:, None]).cpu().numpy()
+        d, mask = spec.target, spec.mask
+        edge = prob.ft.chan_edge
+        num = np.real((np.conj(m[:, mask]) * d[:, mask]).sum(1))
+        den = np.real((np.conj(m[:, mask]) * m[:, mask]).sum(1))
+        ne = int(edge.max()) + 1
+        sc = (np.bincount(edge, num, ne) / np.maximum(np.bincount(edge, den, ne), 1e-30))[edge]
+        r = (np.abs(m[:, mask] * sc[:, None] - d[:, mask]) ** 2).sum() / (np.abs(d[:, mask]) ** 2).sum()
+        out.append(float(r))
+    return np.array(out)
+
+
+def bench_da(args):
+    """GPU-s of the learned + batched sampler to the plain GPU sampler's
+    R-factor, on the ternary configuration: fcc Fe-Ni-Cr 40/40/20, 4,000 sites,
+    a0 3.57 A, target order alpha1(Fe-Cr) = -0.12 plus noise 5e-4, three K
+    edges, 16 sample positions x 32 rungs. The plain sampler runs `--steps`
+    exchange periods (default 200); the learned one starts from the same
+    states and seeds, logs ~1e6 swaps of plain steps, trains the surrogate
+    and screens, and runs until the mean best R-factor reaches the plain
+    one (at most 3x the plain periods). GPU time by CUDA events; the R-factor
+    checks between segments are not counted."""
+    import torch
+    from chimera_b200 import _native as N
+    from chimera_b200 import configs
+    from chimera_b200.sampler import BatchedSampler, LadderSpec
+    N.lib()
+    prob = configs.Problem(elements=("Fe", "Ni", "Cr"), composition=(0.4, 0.4, 0.2), a0=3.57,
+                           alpha1=-0.12, alpha_pair=(0, 2))
+    npos = args.positions
+    specs = []
+    for p in range(npos):
+        pos = prob.position(p)
+        specs.append(LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R, nrep=NREP,
+                                tmin=1e-4, tmax=1e-1, seed=p, swap_frac=1.0,
+                                ms_library=prob.ms))
+    starts = [prob.random_config(1000 + p) for p in range(npos)]
+    nb = min(args.steps, 400) if args.steps != 1200 else 200
+    s = torch.cuda.current_stream()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        fn()
+        b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b) * 1e-3
+
+    plain = BatchedSampler(specs, precision=1, exchange_every=EXCH, reanchor_every=1000,
+                           threads=256, min_blocks=4)
+    plain.init_state(starts, prob.cell.ideal)
+    plain.capture()
+    t_plain = timed(lambda: plain.run_blocks(nb))
+    r_plain = float(r_factors(plain, prob).mean())
+
+    learned = BatchedSampler(specs, precision=1, exchange_every=EXCH, reanchor_every=1000,
+                             threads=256, min_blocks=4)
+    learned.init_state(starts, prob.cell.ideal)
+    learned.capture()
+    lblocks = max(1, -(-1_000_000 // (learned.nslots * EXCH)))     # ~1e6 logged swaps
+    t_learn = timed(lambda: learned.learn(blocks=lblocks, epochs=4))
+    rep = learned.train_report
+    t_run, done, r_l = 0.0, lblocks, float("inf")
+    chunk = max(10, nb // 10)
+    while done < 3 * nb:
+        t_run += timed(lambda: learned.run_blocks(chunk))
+        done += chunk
+        r_l = float(r_factors(learned, prob).mean())
+        if r_l <= r_plain:
+            break
+    st = learned.lad.da_stats().sum(0)
+    line = {"metric": METRIC, "kernel": "learned vs plain sampler",
+            "config": {"workload": "fcc Fe40Ni40Cr20 4000 atoms (a0 3.57 A), alpha1(Fe-Cr) -0.12, "
+                                   "3 K edges, SS 5.0 A + exact MS 5.5 A, k^1/k^2/k^3 Kaiser "
+                                   "complex chi(R) 1.4-5.0 A",
+                       "positions": npos, "rungs": NREP, "plain_periods": nb},
+            "plain": {"gpu_s": t_plain, "r_factor": r_plain, "periods": nb},
+            "learned": {"gpu_s": t_learn + t_run, "gpu_s_log_and_train": t_learn,
+                        "r_factor": r_l, "periods": done, "reached": bool(r_l <= r_plain),
+                        "surrogate_fit_rmse_over_sd": rep.get("rmse_d", 0) / max(rep.get("std_d", 1), 1e-30),
+                        "logged_swaps": rep.get("n"),
+                        "exact_fraction": float(st[1] / max(st[0], 1)),
+                        "screening_error": float(1 - st[3] / max(st[1], 1)),
+                        "fallbacks": learned.fallbacks},
+            "ratio_learned_over_plain": (t_learn + t_run) / t_plain,
+            "device_error": plain.lad.device_error() | learned.lad.device_error()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global NPOS
     ap = argparse.ArgumentParser()
@@ -334,14 +437,18 @@ def main():
     ap.add_argument("--positions", type=int, default=16,
                     help="ladders per GPU (fewer for a small profiling case)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--kernel", default="sampler", choices=["sampler", "ft"],
-                    help="ft: time the windowed FT contraction (chx_ft_batch) instead")
+    ap.add_argument("--kernel", default="sampler", choices=["sampler", "ft", "da"],
+                    help="ft: time the windowed FT contraction (chx_ft_batch); da: GPU-s of "
+                         "the learned (delayed-acceptance) sampler to the plain sampler's "
+                         "R-factor on the ternary configuration")
     args = ap.parse_args()
     NPOS = args.positions
     if args.impl == "reference":
         return run_reference(args)
     if args.kernel == "ft":
         return bench_ft(args)
+    if args.kernel == "da":
+        return bench_da(args)
 
     import torch
     import torch.distributed as dist
