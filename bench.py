@@ -425,6 +425,78 @@ def bench_da(args):
     return 0
 
 
+# the uneven series: (lattice, elements, a0, cells per edge, alpha1 target)
+UNEVEN = (("fcc", ("Fe", "Ni"), 3.55, 5, -0.05), ("fcc", ("Fe", "Ni"), 3.57, 8, -0.10),
+          ("fcc", ("Fe", "Ni"), 3.60, 10, -0.08), ("fcc", ("Fe", "Ni"), 3.62, 5, -0.15),
+          ("bcc", ("Fe", "Cr"), 2.87, 8, -0.06), ("bcc", ("Fe", "Cr"), 2.87, 10, -0.12),
+          ("fcc", ("Fe", "Ni"), 3.59, 8, -0.03), ("bcc", ("Fe", "Cr"), 2.87, 6, -0.09))
+
+
+def bench_uneven(args):
+    """The uneven serving-style batch: 24 series points (8 supercells of
+    432-4,000 sites, fcc Fe-Ni at a0 3.55-3.62 A and bcc Fe-Cr at 2.87 A,
+    exact MS to 5.5 A, seeded SRO targets alpha1 -0.15..-0.03 plus noise,
+    3 sample positions each), 16 rungs per point, all in one launch per
+    exchange period under a CUDA graph, against the same 24 ladders run one
+    ladder per launch one after the other (the reference's host loop over
+    points). Swap attempts/s of both, device time by CUDA events."""
+    import torch
+    from chimera_b200 import _native as N
+    from chimera_b200 import configs
+    from chimera_b200.sampler import BatchedSampler, LadderSpec
+    N.lib()
+    specs, starts = [], []
+    for q, (lat, els, a0, n, al) in enumerate(UNEVEN):
+        prob = configs.Problem(elements=els, a0=a0, lattice=lat, ncell=(n, n, n), alpha1=al,
+                               order_seed=q)
+        for p in range(3):
+            pos = prob.position(10 * q + p)
+            specs.append(LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R,
+                                    nrep=16, tmin=1e-4, tmax=1e-1, seed=10 * q + p,
+                                    swap_frac=1.0, ms_library=prob.ms))
+            starts.append((prob.random_config(100 + 10 * q + p), prob.cell.ideal))
+    nb = 40 if args.steps == 1200 else max(4, min(args.steps, 200))
+    s = torch.cuda.current_stream()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        fn()
+        b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b) * 1e-3
+
+    bs = BatchedSampler(specs, precision=1, exchange_every=EXCH, reanchor_every=1000)
+    bs.init_state([x[0] for x in starts], [x[1] for x in starts])
+    tuning = bs.autotune()
+    bs.capture()
+    bs.run_blocks(max(3, args.warmup))
+    t_batch = timed(lambda: bs.run_blocks(nb))
+    t_sep = 0.0
+    for sp, (s0, p0) in zip(specs, starts):
+        one = BatchedSampler([sp], precision=1, exchange_every=EXCH, reanchor_every=1000,
+                             threads=bs.lad.threads, min_blocks=bs.lad.min_blocks)
+        one.init_state([s0], [p0])
+        one.capture()
+        one.run_blocks(2)
+        t_sep += timed(lambda: one.run_blocks(nb))
+        del one
+    att = bs.nslots * EXCH * nb
+    line = {"metric": METRIC, "kernel": "uneven batch",
+            "config": {"workload": "24 series points: fcc Fe-Ni a0 3.55-3.62 A and bcc Fe-Cr "
+                                   "a0 2.87 A, 432-4,000 sites, exact MS 5.5 A, 2 K edges "
+                                   "each, 16 rungs",
+                       "sites": sorted({int(sp.fm.natoms) for sp in specs}),
+                       "ladders": len(specs), "replicas": bs.nslots, "periods": nb},
+            "batched": {"attempts_per_s": att / t_batch, "gpu_s": t_batch,
+                        "launch_shape": list(tuning["shape"])},
+            "one_ladder_per_launch": {"attempts_per_s": att / t_sep, "gpu_s": t_sep},
+            "speedup": t_sep / t_batch, "unit": UNIT,
+            "device_error": bs.lad.device_error()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global NPOS
     ap = argparse.ArgumentParser()
@@ -437,7 +509,7 @@ def main():
     ap.add_argument("--positions", type=int, default=16,
                     help="ladders per GPU (fewer for a small profiling case)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--kernel", default="sampler", choices=["sampler", "ft", "da"],
+    ap.add_argument("--kernel", default="sampler", choices=["sampler", "ft", "da", "uneven"],
                     help="ft: time the windowed FT contraction (chx_ft_batch); da: GPU-s of "
                          "the learned (delayed-acceptance) sampler to the plain sampler's "
                          "R-factor on the ternary configuration")
@@ -449,6 +521,8 @@ def main():
         return bench_ft(args)
     if args.kernel == "da":
         return bench_da(args)
+    if args.kernel == "uneven":
+        return bench_uneven(args)
 
     import torch
     import torch.distributed as dist
