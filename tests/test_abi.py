@@ -29,6 +29,8 @@ def test_struct_layout_matches_binding():
     assert lib.chx_struct_size(1) == ctypes.sizeof(N.Ladder)
     assert lib.chx_struct_size(2) == N.Ladder.exch_acc.offset
     assert lib.chx_struct_size(3) == N.Ladder.seed.offset
+    assert lib.chx_struct_size(4) == ctypes.sizeof(N.Mlp)
+    assert lib.chx_struct_size(5) == N.Ladder.log_cap.offset
     assert lib.chx_version() >= 1000
 
 
@@ -40,3 +42,42 @@ def test_errors_are_reported_not_raised_in_c():
     assert "compute_r" in N.last_error()
     rc = lib.chx_chi_full_scratch_bytes(None, 1)
     assert rc == -1
+
+
+def test_surrogate_entries_check_their_arguments():
+    """Shapes and alignment are checked before anything reaches the device."""
+    from chimera_b200 import _native as N
+    from oracle import mlp as OM
+    lib = N.lib()
+    for nsp, D, nchain, H in ((2, 42, 512, 256), (3, 12, 0, 64), (4, 8, 7, 8)):
+        nin = OM.nin_of(nsp, D, nchain)
+        assert lib.chx_mlp_nparam(nsp, D, nchain, H) == (nin + 1) * H + 3 * H + 2 * H * H + H + 1
+    for bad in ((1, 42, 0, 256), (2, 0, 0, 256), (2, 42, 0, 260), (2, 42, 0, 264), (2, 128, 0, 64)):
+        assert lib.chx_mlp_nparam(*bad) == -1
+    P = N.Mlp()
+    rc = lib.chx_mlp_bind(ctypes.byref(P), 2, 42, 0, 256, ctypes.c_void_p(4096),
+                          ctypes.c_void_p(4096 + 8))
+    assert rc == -1 and "16-byte" in N.last_error()
+    rc = lib.chx_mlp_bind(ctypes.byref(P), 2, 42, 0, 256, ctypes.c_void_p(4096),
+                          ctypes.c_void_p(8192))
+    assert rc == 0 and P.nin == OM.nin_of(2, 42) and P.H == 256 and P.nchain == 0
+    assert lib.chx_mlp_predict(None, None, None, None, 1, None, None) == -1
+    assert lib.chx_mlp_adam(None, None, None, None, None, 1, 1e-3, .9, .999, 1e-8, 0, None) == -1
+
+
+def test_tensor_core_transform_sizes_its_scratch():
+    """Precisions 2 (split-BF16) and 3 (TF32) need a scratch of the basis
+    parts plus an error word; a smaller one is refused with a message."""
+    from chimera_b200 import _native as N
+    lib = N.lib()
+    rows, nk, nR = 4096, 241, 200
+    Np, Kp = -(-2 * nR // 128) * 128, -(-nk // 32) * 32
+    assert lib.chx_ft_batch_scratch_bytes(rows, nk, nR, 2) == 256 + 2 * Np * Kp * 2
+    assert lib.chx_ft_batch_scratch_bytes(rows, nk, nR, 3) == 256 + Np * Kp * 4
+    assert lib.chx_ft_batch_scratch_bytes(rows, nk, nR, 0) == 0
+    fake = ctypes.c_void_p(1 << 20)
+    for prec in (2, 3):
+        need = lib.chx_ft_batch_scratch_bytes(rows, nk, nR, prec)
+        rc = lib.chx_ft_batch(fake, rows, nk, fake, nR, prec, fake, fake, need - 1, None)
+        assert rc == -1 and "scratch" in N.last_error()
+    assert lib.chx_ft_batch(fake, rows, nk, fake, nR, 7, fake, fake, 0, None) == -1
