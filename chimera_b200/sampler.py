@@ -232,14 +232,19 @@ class Ladders:
             L.energy_beta = 1.0 / (KB_EV * float(T_ann))
         else:
             L.etab, L.energy_beta = 0, 0.0
-        # transform and target
-        f = _ft_setup(s.ft, nsp)
+        # transform and target (the set-up once per transform object)
+        fcache = self.__dict__.setdefault("_ft_cache", {})
+        if id(s.ft) not in fcache:
+            f = _ft_setup(s.ft, nsp)
+            fcache[id(s.ft)] = (s.ft, f, dict(ft_n0=self._t(f["n0"]), ft_idx=self._t(f["idx"]),
+                                              ft_frac=self._t(f["frac"]), ft_w=self._t(f["w"])))
+        f = fcache[id(s.ft)][1]
+        b.update(fcache[id(s.ft)][2])
         win = np.nonzero(s.mask)[0].astype(np.int32)
         cplx = bool(np.iscomplexobj(s.target))
         tm = np.ascontiguousarray(s.target[:, s.mask])
         sm = np.ascontiguousarray(s.sigma_R[:, s.mask], np.float64)
-        b.update(ft_n0=self._t(f["n0"]), ft_idx=self._t(f["idx"]), ft_frac=self._t(f["frac"]),
-                 ft_w=self._t(f["w"]), win=self._t(win),
+        b.update(win=self._t(win),
                  tm_re=self._t(np.ascontiguousarray(tm.real, np.float64)),
                  tm_im=self._t(np.ascontiguousarray(tm.imag if cplx else np.zeros(tm.shape),
                                                     np.float64)),
