@@ -91,6 +91,46 @@ class CrystalSupercell:
         # which the arange(n) branch already handles without repetition
         return cand
 
+    def _heights(self):
+        """Supercell heights: the distance between opposite faces, per axis."""
+        H = self.H
+        vol = abs(np.linalg.det(H))
+        return np.array([vol / np.linalg.norm(np.cross(H[(a + 1) % 3], H[(a + 2) % 3]))
+                         for a in range(3)])
+
+    def _offset_images(self, rmax):
+        """(natoms, ncand) candidates with the 27-image index of each
+        candidate's unwrapped cell, j ascending per row, or None when the
+        supercell is too small for the shortcut.
+
+        When every supercell height exceeds 2 rmax, a pair within rmax has
+        exactly one image within rmax, and that image is the one its
+        candidate cell offset names (the offset does not wrap twice, since
+        2 reach + 1 < ncell on every axis). The 27-image argmin of the
+        reference then picks the same image for every kept pair, so it can be
+        read off the offset instead of searched."""
+        reach = self._cell_reach(rmax)
+        if np.any(self._heights() <= 2.0 * rmax + 1e-9):
+            return None
+        if any(2 * r + 1 >= n for n, r in zip(self.ncell, reach)):
+            return None
+        nx, ny, nz = self.ncell
+        nb = self.basis.shape[0]
+        off = np.array(np.meshgrid(*[np.arange(-r, r + 1) for r in reach],
+                                   indexing="ij")).reshape(3, -1).T
+        cell = np.arange(self.natoms) // nb
+        ci = np.stack([cell // (ny * nz), (cell // nz) % ny, cell % nz], axis=1)
+        raw = ci[:, None, :] + off[None, :, :]                   # unwrapped cell
+        n = np.array(self.ncell)
+        wrap = np.floor_divide(raw, n)                           # -1, 0 or 1 per axis
+        cc = raw - wrap * n
+        flat = (cc[..., 0] * ny + cc[..., 1]) * nz + cc[..., 2]
+        cand = (flat[:, :, None] * nb + np.arange(nb)[None, None, :]).reshape(self.natoms, -1)
+        img = ((wrap[..., 0] + 1) * 9 + (wrap[..., 1] + 1) * 3 + (wrap[..., 2] + 1))
+        img = np.repeat(img, nb, axis=1)
+        order = np.argsort(cand, axis=1, kind="stable")
+        return (np.take_along_axis(cand, order, 1), np.take_along_axis(img, order, 1))
+
     def min_image(self, d):
         """Exact minimum image by explicit search over the 27 nearest images."""
         d = np.atleast_2d(d)
@@ -102,9 +142,12 @@ class CrystalSupercell:
         """(i_idx, j_idx, shift, off): i-major, j ascending, as the reference."""
         pos = self.ideal
         n = self.natoms
+        imgs = self._images
+        fast = self._offset_images(rmax)
+        if fast is not None:
+            return self._neighbour_list_offsets(rmax, *fast)
         cand = self._candidates(rmax)
         I, J, SH = [], [], []
-        imgs = self._images
         for s0 in range(0, n, batch):
             rows = np.arange(s0, min(n, s0 + batch))
             cj = cand[rows]                                        # (b, m)
@@ -120,6 +163,31 @@ class CrystalSupercell:
                 I.append(np.full(sel.size, rows[q]))
                 J.append(cj[q, sel])
                 SH.append(imgs[best[q, sel]])
+        i_idx = np.concatenate(I).astype(np.int32)
+        j_idx = np.concatenate(J).astype(np.int32)
+        shift = np.ascontiguousarray(np.concatenate(SH), np.float64)
+        counts = np.bincount(i_idx, minlength=n)
+        off = np.zeros(n + 1, np.int32)
+        off[1:] = np.cumsum(counts)
+        return i_idx, j_idx, shift, off
+
+    def _neighbour_list_offsets(self, rmax, cand, img, batch=2048):
+        """neighbour_list when the image of each candidate is known: the same
+        expressions (d0 + image, its norm, the rmax test) on one image per
+        candidate instead of 27."""
+        pos, n, imgs = self.ideal, self.natoms, self._images
+        I, J, SH = [], [], []
+        for s0 in range(0, n, batch):
+            rows = np.arange(s0, min(n, s0 + batch))
+            cj, ik = cand[rows], img[rows]
+            d0 = pos[cj] - pos[rows][:, None, :]
+            d = d0 + imgs[ik]
+            r = np.linalg.norm(d.reshape(-1, 3), axis=1).reshape(d.shape[:2])
+            keep = (r <= rmax) & (r > 1e-6)
+            q, c = np.nonzero(keep)                               # row-major: j ascending
+            I.append(rows[q])
+            J.append(cj[q, c])
+            SH.append(imgs[ik[q, c]])
         i_idx = np.concatenate(I).astype(np.int32)
         j_idx = np.concatenate(J).astype(np.int32)
         shift = np.ascontiguousarray(np.concatenate(SH), np.float64)

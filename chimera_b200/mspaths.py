@@ -233,25 +233,45 @@ class SupercellPaths:
         self.p_cls = np.concatenate(P_cls).astype(np.int32)
         self.p_slot = np.concatenate(P_slot).astype(np.int32)
         self.npath = int(self.p_abs.size)
-        site = np.concatenate([self.p_abs] + [self.p_slot[:, q] for q in range(3)])
-        pid = np.tile(np.arange(self.npath), 4)
-        keep = site >= 0
-        site, pid = site[keep], pid[keep]
-        order = np.argsort(site, kind="stable")
-        site, pid = site[order], pid[order]
-        cnt = np.bincount(site, minlength=n)
+        cnt = np.bincount(self.p_abs, minlength=n)
+        for q in range(3):
+            s = self.p_slot[:, q]
+            cnt += np.bincount(s[s >= 0], minlength=n)
         self.M = int(cnt.max())
-        inc = np.full((n, self.M), self.npath, np.int64)
-        start = np.r_[0, np.cumsum(cnt)[:-1]]
-        inc[site, np.arange(site.size) - start[site]] = pid
-        self.inc = inc.astype(np.int32)
         self.records = np.empty((self.npath, 4), np.int32)
         self.records[:, 0] = self.p_abs | (self.cls_off[self.p_cls] << 20)
         self.records[:, 1:] = self.p_slot
-        pad = np.full((1, 4), -1, np.int32)
-        self.inc_rec = np.concatenate([self.records, pad])[self.inc]
+        self._inc = self._inc_rec = None
 
         self._templates(Xi, box, look)
+
+    @property
+    def inc(self):
+        """(natoms, M) ids of the paths through each site, ascending, padded
+        with npath (mslibrary.py:399-404); built on first use."""
+        if self._inc is None:
+            n = self.natoms
+            site = np.concatenate([self.p_abs] + [self.p_slot[:, q] for q in range(3)])
+            pid = np.tile(np.arange(self.npath), 4)
+            keep = site >= 0
+            site, pid = site[keep], pid[keep]
+            order = np.argsort(site, kind="stable")
+            site, pid = site[order], pid[order]
+            cnt = np.bincount(site, minlength=n)
+            inc = np.full((n, self.M), self.npath, np.int64)
+            start = np.r_[0, np.cumsum(cnt)[:-1]]
+            inc[site, np.arange(site.size) - start[site]] = pid
+            self._inc = inc.astype(np.int32)
+        return self._inc
+
+    @property
+    def inc_rec(self):
+        """(natoms, M, 4) records of the paths through each site (-1 rows as
+        padding), for the reference-interface delta; built on first use."""
+        if self._inc_rec is None:
+            pad = np.full((1, 4), -1, np.int32)
+            self._inc_rec = np.concatenate([self.records, pad])[self.inc]
+        return self._inc_rec
 
     # Every site of a cubic Bravais supercell sees the same paths up to a
     # translation, so the paths through a site are one shared list of

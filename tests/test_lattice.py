@@ -40,6 +40,21 @@ def test_neighbour_list_shells_and_wc(n):
     assert np.array_equal(wc, g[f"c{n}_wc"])
 
 
+@pytest.mark.parametrize("lat,nc,a0,rmax", [("fcc", (8, 9, 10), 3.59, 5.0),
+                                             ("bcc", (10, 8, 9), 2.87, 5.0),
+                                             ("hcp", (10, 11, 8), 2.5, 5.0),
+                                             ("sc", (10, 11, 12), 2.9, 6.2)])
+def test_offset_image_shortcut_equals_27_image_search(lat, nc, a0, rmax):
+    """Large cells read each candidate's image off its cell offset; the
+    result is bit-identical to the reference's 27-image argmin."""
+    cell = L.CrystalSupercell(lat, nc, a0)
+    assert cell._offset_images(rmax) is not None
+    fast = cell.neighbour_list(rmax)
+    cell._offset_images = lambda r: None
+    exact = cell.neighbour_list(rmax)
+    assert digest(*fast) == digest(*exact)
+
+
 def test_topology_uniform_and_tabulable():
     cell = L.CrystalSupercell("fcc", (4, 4, 4), 3.59)
     t = L.Topology(cell, 6.2, sigma2=0.006)
