@@ -425,31 +425,43 @@ def bench_da(args):
     return 0
 
 
-# the uneven series: (lattice, elements, a0, cells per edge, alpha1 target)
-UNEVEN = (("fcc", ("Fe", "Ni"), 3.55, 5, -0.05), ("fcc", ("Fe", "Ni"), 3.57, 8, -0.10),
-          ("fcc", ("Fe", "Ni"), 3.60, 10, -0.08), ("fcc", ("Fe", "Ni"), 3.62, 5, -0.15),
-          ("bcc", ("Fe", "Cr"), 2.87, 8, -0.06), ("bcc", ("Fe", "Cr"), 2.87, 10, -0.12),
-          ("fcc", ("Fe", "Ni"), 3.59, 8, -0.03), ("bcc", ("Fe", "Cr"), 2.87, 6, -0.09))
+# the uneven series: (lattice, elements, composition, a0, cells, alpha1 target);
+# exact MS on fcc and bcc, single scattering only on hcp (no hcp MS classes)
+UNEVEN = (("fcc", ("Fe", "Ni"), (0.5, 0.5), 3.55, (5, 5, 5), -0.05),
+          ("fcc", ("Fe", "Ni"), (0.5, 0.5), 3.57, (8, 8, 8), -0.10),
+          ("fcc", ("Fe", "Ni"), (0.5, 0.5), 3.59, (10, 10, 10), -0.08),
+          ("fcc", ("Fe", "Ni"), (0.5, 0.5), 3.60, (20, 20, 10), -0.06),
+          ("fcc", ("Fe", "Ni"), (0.5, 0.5), 3.62, (20, 20, 20), -0.04),
+          ("bcc", ("Fe", "Cr"), (0.5, 0.5), 2.87, (5, 5, 10), -0.06),
+          ("bcc", ("Fe", "Cr"), (0.5, 0.5), 2.87, (10, 10, 10), -0.12),
+          ("hcp", ("Co", "Ni"), (0.5, 0.5), 2.507, (8, 8, 6), -0.05),
+          ("hcp", ("Co", "Ni"), (0.5, 0.5), 2.507, (12, 12, 10), -0.08),
+          ("fcc", ("Fe", "Ni", "Cr"), (0.4, 0.4, 0.2), 3.59, (8, 8, 8), -0.08),
+          ("fcc", ("Fe", "Ni", "Cr"), (0.4, 0.4, 0.2), 3.59, (10, 10, 10), -0.12),
+          ("bcc", ("Fe", "Cr", "Ni"), (0.4, 0.4, 0.2), 2.87, (8, 8, 8), -0.06))
+UNEVEN_POS = 2
 
 
 def bench_uneven(args):
-    """The uneven serving-style batch: 24 series points (8 supercells of
-    432-4,000 sites, fcc Fe-Ni at a0 3.55-3.62 A and bcc Fe-Cr at 2.87 A,
-    exact MS to 5.5 A, seeded SRO targets alpha1 -0.15..-0.03 plus noise,
-    3 sample positions each), 16 rungs per point, all in one launch per
-    exchange period under a CUDA graph, against the same 24 ladders run one
-    ladder per launch one after the other (the reference's host loop over
-    points). Swap attempts/s of both, device time by CUDA events."""
+    """The uneven serving-style batch: 24 series points (12 supercells of
+    500-32,000 sites: fcc Fe-Ni a0 3.55-3.62 A, bcc Fe-Cr 2.87 A, hcp Co-Ni
+    2.507 A, and fcc / bcc Fe-Ni-Cr ternaries; exact MS to 5.5 A on fcc and
+    bcc; seeded SRO targets alpha1 -0.12..-0.04 plus noise, 2 sample
+    positions each), 16 rungs per point. All 24 ladders run in one graph
+    replay per exchange period (one step launch per species count, the two on
+    parallel streams), against the same ladders run one ladder per launch one
+    after the other (the reference's host loop over points). Swap
+    attempts/s of both, device time by CUDA events."""
     import torch
     from chimera_b200 import _native as N
     from chimera_b200 import configs
     from chimera_b200.sampler import BatchedSampler, LadderSpec
     N.lib()
     specs, starts = [], []
-    for q, (lat, els, a0, n, al) in enumerate(UNEVEN):
-        prob = configs.Problem(elements=els, a0=a0, lattice=lat, ncell=(n, n, n), alpha1=al,
-                               order_seed=q)
-        for p in range(3):
+    for q, (lat, els, comp, a0, nc, al) in enumerate(UNEVEN):
+        prob = configs.Problem(elements=els, composition=comp, a0=a0, lattice=lat, ncell=nc,
+                               alpha1=al, order_seed=q, ms=lat != "hcp")
+        for p in range(UNEVEN_POS):
             pos = prob.position(10 * q + p)
             specs.append(LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R,
                                     nrep=16, tmin=1e-4, tmax=1e-1, seed=10 * q + p,
@@ -468,14 +480,15 @@ def bench_uneven(args):
 
     bs = BatchedSampler(specs, precision=1, exchange_every=EXCH, reanchor_every=1000)
     bs.init_state([x[0] for x in starts], [x[1] for x in starts])
-    tuning = bs.autotune()
+    bs.autotune()
     bs.capture()
     bs.run_blocks(max(3, args.warmup))
     t_batch = timed(lambda: bs.run_blocks(nb))
     t_sep = 0.0
-    for sp, (s0, p0) in zip(specs, starts):
+    for li, (sp, (s0, p0)) in enumerate(zip(specs, starts)):
+        lad, _ = bs.ladder(li)
         one = BatchedSampler([sp], precision=1, exchange_every=EXCH, reanchor_every=1000,
-                             threads=bs.lad.threads, min_blocks=bs.lad.min_blocks)
+                             threads=lad.threads, min_blocks=lad.min_blocks)
         one.init_state([s0], [p0])
         one.capture()
         one.run_blocks(2)
@@ -483,16 +496,19 @@ def bench_uneven(args):
         del one
     att = bs.nslots * EXCH * nb
     line = {"metric": METRIC, "kernel": "uneven batch",
-            "config": {"workload": "24 series points: fcc Fe-Ni a0 3.55-3.62 A and bcc Fe-Cr "
-                                   "a0 2.87 A, 432-4,000 sites, exact MS 5.5 A, 2 K edges "
-                                   "each, 16 rungs",
+            "config": {"workload": "24 series points: fcc Fe-Ni a0 3.55-3.62 A (500-32,000 "
+                                   "sites), bcc Fe-Cr 2.87 A, hcp Co-Ni 2.507 A (single "
+                                   "scattering), fcc/bcc Fe-Ni-Cr ternaries; exact MS 5.5 A "
+                                   "on fcc/bcc; one K edge per species, 16 rungs",
                        "sites": sorted({int(sp.fm.natoms) for sp in specs}),
+                       "lattices": sorted({u[0] for u in UNEVEN}),
+                       "species_counts": [g.nsp for g in bs.groups],
                        "ladders": len(specs), "replicas": bs.nslots, "periods": nb},
             "batched": {"attempts_per_s": att / t_batch, "gpu_s": t_batch,
-                        "launch_shape": list(tuning["shape"])},
+                        "launch_shapes": [list(t["shape"]) for t in bs.tuning]},
             "one_ladder_per_launch": {"attempts_per_s": att / t_sep, "gpu_s": t_sep},
             "speedup": t_sep / t_batch, "unit": UNIT,
-            "device_error": bs.lad.device_error()}
+            "device_error": bs.device_error()}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -782,14 +782,34 @@ class BatchedSampler:
     """Many independent ladders in one launch per step, replayed as CUDA
     graphs (one graph = `exchange_every` steps + a device replica exchange),
     with FP64 re-anchoring of the running chi every `reanchor_every`
-    accepted moves (checked every `check_every` blocks)."""
+    accepted moves (checked every `check_every` blocks).
+
+    The step kernel is compiled per species count, so a batch that mixes
+    binaries and ternaries is held as one group of ladders per count (in order
+    of first appearance). Each exchange period launches every group's step
+    and exchange on a stream of its own, forked from and joined back to the
+    caller's stream, so the groups run side by side on the GPU and the whole
+    period is still one graph replay. Ladder indices are global (the order of
+    `specs`)."""
 
     def __init__(self, specs, precision=FP32C, exchange_every=25, use_table=True,
                  reanchor_every=1000, check_every=40, threads=256, min_blocks=3):
         import torch
         self.torch = torch
-        self.lad = Ladders(specs, precision=precision, use_table=use_table, threads=threads,
-                           min_blocks=min_blocks)
+        specs = list(specs)
+        counts = []
+        for s in specs:
+            if int(s.fm.nsp) not in counts:
+                counts.append(int(s.fm.nsp))
+        self.groups, self.where = [], [None] * len(specs)
+        for g, nsp in enumerate(counts):
+            idx = [i for i, s in enumerate(specs) if int(s.fm.nsp) == nsp]
+            self.groups.append(Ladders([specs[i] for i in idx], precision=precision,
+                                       use_table=use_table, threads=threads,
+                                       min_blocks=min_blocks))
+            for q, i in enumerate(idx):
+                self.where[i] = (g, q)
+        self._streams = None
         self.tuning = None
         self.exchange_every = int(exchange_every)
         self.reanchor_every = int(reanchor_every)
@@ -800,30 +820,71 @@ class BatchedSampler:
         self.steps = 0
 
     @property
+    def lad(self):
+        """The Ladders of a batch with one species count."""
+        if len(self.groups) != 1:
+            raise ValueError("a batch of mixed species counts has one Ladders per count: "
+                             "use .groups or .ladder(li)")
+        return self.groups[0]
+
+    def ladder(self, li):
+        """(Ladders, index within it) of global ladder li."""
+        g, q = self.where[li]
+        return self.groups[g], q
+
+    @property
+    def nladders(self):
+        return len(self.where)
+
+    @property
     def nslots(self):
-        return self.lad.nslots
+        return sum(g.nslots for g in self.groups)
 
     def init_state(self, species0, pos0):
         """species0 / pos0: one array per ladder (or one shared by all)."""
-        for li in range(self.lad.nladders):
+        for li in range(self.nladders):
             sp = species0[li] if isinstance(species0, (list, tuple)) else species0
             ps = pos0[li] if isinstance(pos0, (list, tuple)) else pos0
-            self.lad.init_state(li, sp, ps)
-        self.lad.refresh_chi2(reset_best=True)
+            lad, q = self.ladder(li)
+            lad.init_state(q, sp, ps)
+        for lad in self.groups:
+            lad.refresh_chi2(reset_best=True)
 
     def autotune(self, reps=3, path=None):
         """Measure the step kernel's launch shapes on this problem (real
-        steps of the chains) and keep the fastest (chimera_b200.autotune)."""
+        steps of the chains) and keep the fastest (chimera_b200.autotune),
+        per group; the result of a one-group batch, else the list."""
         from .autotune import tune
-        self.tuning = tune(self.lad, nsteps=self.exchange_every, reps=reps, path=path)
+        self.tuning = [tune(lad, nsteps=self.exchange_every, reps=reps, path=path)
+                       for lad in self.groups]
         self.steps += self.exchange_every * (reps + 1) * 3
-        return self.tuning
+        return self.tuning[0] if len(self.groups) == 1 else self.tuning
+
+    def device_error(self):
+        """Error words of the groups OR-ed together (0 = none)."""
+        e = 0
+        for lad in self.groups:
+            e |= lad.device_error()
+        return e
 
     def block(self):
         """One exchange period: exchange_every steps in one launch, then the
-        device exchange."""
-        self.lad.step(self.exchange_every)
-        self.lad.exchange_device()
+        device exchange (per group, the groups on parallel streams)."""
+        if len(self.groups) == 1:
+            self.groups[0].step(self.exchange_every)
+            self.groups[0].exchange_device()
+            return
+        torch = self.torch
+        if self._streams is None:
+            self._streams = [torch.cuda.Stream() for _ in self.groups]
+        cur = torch.cuda.current_stream()
+        for lad, st in zip(self.groups, self._streams):
+            st.wait_stream(cur)
+            with torch.cuda.stream(st):
+                lad.step(self.exchange_every)
+                lad.exchange_device()
+        for st in self._streams:
+            cur.wait_stream(st)
 
     def capture(self):
         torch = self.torch
@@ -849,10 +910,11 @@ class BatchedSampler:
             self.steps += self.exchange_every
             if self.blocks % self.check_every == 0:
                 if self.reanchor_every:
-                    due = self.lad.accepted_since_anchor() >= self.reanchor_every
-                    if bool(due.any()):
-                        self.lad.reanchor(due)
-                        self.reanchors += 1
+                    for lad in self.groups:
+                        due = lad.accepted_since_anchor() >= self.reanchor_every
+                        if bool(due.any()):
+                            lad.reanchor(due)
+                            self.reanchors += 1
                 if self.surrogate is not None:
                     self._check_screen()
 
@@ -903,11 +965,11 @@ class BatchedSampler:
         self.last_screen = st
 
     def best(self, li):
-        b = self.lad.bufs[li]
+        lad, q = self.ladder(li)
+        b = lad.bufs[q]
         bc = _host(b["best_chi2"])
         s = int(bc.argmin())
         return _host(b["best_sp"][s]).astype(np.int32), float(bc[s])
 
     def accept_rate(self):
-        tot = sum(int(b["n_acc"].sum()) for b in self.lad.bufs)
-        return tot
+        return sum(int(b["n_acc"].sum()) for lad in self.groups for b in lad.bufs)
