@@ -426,7 +426,7 @@ def bench_da(args):
 
 
 # the uneven series: (lattice, elements, composition, a0, cells, alpha1 target);
-# exact MS on fcc and bcc, single scattering only on hcp (no hcp MS classes)
+# exact 3-/4-leg MS to 5.5 A on every point
 UNEVEN = (("fcc", ("Fe", "Ni"), (0.5, 0.5), 3.55, (5, 5, 5), -0.05),
           ("fcc", ("Fe", "Ni"), (0.5, 0.5), 3.57, (8, 8, 8), -0.10),
           ("fcc", ("Fe", "Ni"), (0.5, 0.5), 3.59, (10, 10, 10), -0.08),
@@ -445,8 +445,7 @@ UNEVEN_POS = 2
 def bench_uneven(args):
     """The uneven serving-style batch: 24 series points (12 supercells of
     500-32,000 sites: fcc Fe-Ni a0 3.55-3.62 A, bcc Fe-Cr 2.87 A, hcp Co-Ni
-    2.507 A, and fcc / bcc Fe-Ni-Cr ternaries; exact MS to 5.5 A on fcc and
-    bcc; seeded SRO targets alpha1 -0.12..-0.04 plus noise, 2 sample
+    2.507 A, and fcc / bcc Fe-Ni-Cr ternaries; exact MS to 5.5 A; seeded SRO targets alpha1 -0.12..-0.04 plus noise, 2 sample
     positions each), 16 rungs per point. All 24 ladders run in one graph
     replay per exchange period (one step launch per species count, the two on
     parallel streams), against the same ladders run one ladder per launch one
@@ -460,7 +459,7 @@ def bench_uneven(args):
     specs, starts = [], []
     for q, (lat, els, comp, a0, nc, al) in enumerate(UNEVEN):
         prob = configs.Problem(elements=els, composition=comp, a0=a0, lattice=lat, ncell=nc,
-                               alpha1=al, order_seed=q, ms=lat != "hcp")
+                               alpha1=al, order_seed=q)
         for p in range(UNEVEN_POS):
             pos = prob.position(10 * q + p)
             specs.append(LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R,
@@ -497,9 +496,9 @@ def bench_uneven(args):
     att = bs.nslots * EXCH * nb
     line = {"metric": METRIC, "kernel": "uneven batch",
             "config": {"workload": "24 series points: fcc Fe-Ni a0 3.55-3.62 A (500-32,000 "
-                                   "sites), bcc Fe-Cr 2.87 A, hcp Co-Ni 2.507 A (single "
-                                   "scattering), fcc/bcc Fe-Ni-Cr ternaries; exact MS 5.5 A "
-                                   "on fcc/bcc; one K edge per species, 16 rungs",
+                                   "sites), bcc Fe-Cr 2.87 A, hcp Co-Ni 2.507 A, fcc/bcc "
+                                   "Fe-Ni-Cr ternaries; exact 3-/4-leg MS 5.5 A on all; one K "
+                                   "edge per species, 16 rungs",
                        "sites": sorted({int(sp.fm.natoms) for sp in specs}),
                        "lattices": sorted({u[0] for u in UNEVEN}),
                        "species_counts": [g.nsp for g in bs.groups],

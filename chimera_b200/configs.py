@@ -102,10 +102,12 @@ class Problem:
         self.paths = self.ms_table = None
         if ms:
             cls = MP.enumerate_classes(a0, ms_half, lattice)
-            self.paths = MP.SupercellPaths(cls, self.cell.ideal, self.cell.H, a0, self.nsp)
+            self.paths = MP.SupercellPaths(cls, self.cell.ideal, self.cell.H, a0, self.nsp,
+                                           conv=self.cell.cell_matrix)
             self.ms_table = MP.synthetic_table(cls, self.nsp, self.k, self.tables.f,
                                                self.tables.delta, self.tables.lam, sigma2,
-                                               float(self.top.r_shell[0]), a0 / 2.0, s02=s02)
+                                               float(self.top.r_shell[0]),
+                                               MP.length_unit(lattice, a0), s02=s02)
         fts = [FourierTransform(self.k, kmin, kmax, w, window=window)
                for e in range(self.nsp) for w in kweights]
         self.ft = MultiEdgeFT(fts, chan_edge=np.repeat(np.arange(self.nsp), len(kweights)))

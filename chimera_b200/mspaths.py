@@ -24,6 +24,12 @@ reference uses, from its own enumeration:
     paths through it {absorber | class entry offset << 20, slot0, slot1,
     slot2} that the device kernels stream.
 
+The reference builds classes for fcc only. The same construction runs here
+on bcc and sc (integer coordinates in units of a0/2, O_h) and on hcp, in the
+hexagonal integer coordinates (u, v, w) = (3 f1, 3 f2, 2 f3) under the 12
+operations of the hcp site group, with A-site classes placed inverted at B
+sites.
+
 The per-entry spectra come from a path library on the model's k grid; with
 no FEFF library available, `synthetic_table` defines a smooth seeded one.
 """
@@ -51,13 +57,76 @@ def cubic_ops():
 OPS = cubic_ops()
 
 
-def canonical(seq):
-    """Smallest image of a path (points after the absorber) under O_h and
-    reversal, as a tuple of tuples."""
+# hcp: integer coordinates (u, v, w) = (3 f1, 3 f2, 2 f3) of the conventional
+# hexagonal cell (a1, a2 at 120 degrees, c), so A sites have u, v = 0 mod 3
+# and w even, B sites (basis 1/3, 2/3, 1/2) u, v = 1, 2 mod 3 and w odd.
+HCP_SCALE = np.array([3.0, 3.0, 2.0])
+
+
+def hcp_gram(a0, c_over_a=None):
+    """Gram matrix (A^2) of the hcp integer coordinates: |x|^2 = x G x."""
+    ca = np.sqrt(8.0 / 3.0) if c_over_a is None else float(c_over_a)
+    c = ca * a0
+    return np.array([[a0 * a0 / 9.0, -a0 * a0 / 18.0, 0.0],
+                     [-a0 * a0 / 18.0, a0 * a0 / 9.0, 0.0],
+                     [0.0, 0.0, c * c / 4.0]])
+
+
+def _hcp_site_type(x):
+    """0 for a displacement from an A site to an A site, 1 to a B site,
+    -1 for no site (x integer (..., 3))."""
+    x = np.asarray(x)
+    a = (x[..., 0] % 3 == 0) & (x[..., 1] % 3 == 0) & (x[..., 2] % 2 == 0)
+    b = (x[..., 0] % 3 == 1) & (x[..., 1] % 3 == 2) & (x[..., 2] % 2 == 1)
+    return np.where(a, 0, np.where(b, 1, -1))
+
+
+def hcp_ops():
+    """The 12 operations of the hcp site symmetry (D3h) in (u, v, w): the
+    elements of the hexagonal holohedry D6h, generated by the 60 degree
+    rotation (u, v) -> (u - v, u), the mirror (u, v) -> (v, u) and w -> -w,
+    that map the environment of an A site onto itself."""
+    R = np.array([[1, -1, 0], [1, 0, 0], [0, 0, 1]])
+    Mx = np.array([[0, 1, 0], [1, 0, 0], [0, 0, 1]])
+    Mz = np.diag([1, 1, -1])
+    group = {tuple(np.eye(3, dtype=int).ravel())}
+    frontier = list(group)
+    while frontier:
+        nxt = []
+        for g in frontier:
+            G = np.array(g).reshape(3, 3)
+            for h in (R, Mx, Mz):
+                k = tuple((h @ G).ravel())
+                if k not in group:
+                    group.add(k)
+                    nxt.append(k)
+        frontier = nxt
+    g = np.array(list(itertools.product(range(-6, 7), repeat=3)))
+    env = g[_hcp_site_type(g) >= 0]
+    key = {tuple(x) for x in env}
+    ops = []
+    for k in sorted(group):
+        A = np.array(k).reshape(3, 3)
+        img = env @ A.T
+        inside = np.all(np.abs(img) <= 6, axis=1)
+        if all(tuple(x) in key for x in img[inside]) and \
+                np.array_equal(_hcp_site_type(img[inside]), _hcp_site_type(env[inside])):
+            ops.append(A)
+    assert len(group) == 24 and len(ops) == 12, (len(group), len(ops))
+    return ops
+
+
+HCP_OPS = hcp_ops()
+
+
+def canonical(seq, ops=None):
+    """Smallest image of a path (points after the absorber) under the point
+    group (O_h by default) and reversal, as a tuple of tuples."""
+    ops = OPS if ops is None else ops
     s0 = np.asarray(seq, int)
     best = None
     for s in (s0, s0[::-1]):
-        for A in OPS:
+        for A in ops:
             t = tuple(map(tuple, s @ A.T))
             if best is None or t < best:
                 best = t
@@ -65,9 +134,14 @@ def canonical(seq):
 
 
 class PathClass:
-    """One geometric class: representative, slots and directed images."""
+    """One geometric class: representative, slots and directed images.
 
-    def __init__(self, rep):
+    `ops` is the point group (O_h by default) and `gram` the metric of the
+    integer coordinates (None: Euclidean, lengths in units of a0/2)."""
+
+    def __init__(self, rep, ops=None, gram=None):
+        ops = OPS if ops is None else ops
+        self.gram = gram
         self.rep = np.asarray(rep, int)
         self.nleg = self.rep.shape[0] + 1
         slot_of, seen = [], {}
@@ -84,7 +158,7 @@ class PathClass:
         for rev in (False, True):
             s = self.rep[::-1] if rev else self.rep
             so = self.slot_of[::-1] if rev else self.slot_of
-            for A in OPS:
+            for A in ops:
                 t = tuple(map(tuple, s @ A.T))
                 if t not in imgs:
                     imgs[t] = so.copy()
@@ -92,8 +166,12 @@ class PathClass:
         self.deg = len(self.images)
 
     def reff_units(self):
+        """Half path length, in units of a0/2 (cubic) or A (with a gram)."""
         pts = np.vstack([np.zeros((1, 3)), self.rep, np.zeros((1, 3))])
-        return 0.5 * float(np.linalg.norm(np.diff(pts, axis=0), axis=1).sum())
+        d = np.diff(pts, axis=0)
+        if self.gram is None:
+            return 0.5 * float(np.linalg.norm(d, axis=1).sum())
+        return 0.5 * float(np.sqrt(np.einsum("ni,ij,nj->n", d, self.gram, d)).sum())
 
 
 def lattice_points(lattice, radius):
@@ -112,42 +190,90 @@ def lattice_points(lattice, radius):
     return g[np.linalg.norm(g, axis=1) <= radius + 1e-9]
 
 
-def enumerate_classes(a0, rmax_half, lattice="fcc", nleg_max=4):
-    """The 3- and 4-leg path classes of a cubic lattice to half length rmax."""
-    unit = a0 / 2.0
-    Lmax = 2.0 * rmax_half / unit + 1e-9
-    pts = lattice_points(lattice, rmax_half / unit)
+def hcp_points(a0, radius, c_over_a=None):
+    """Integer (u, v, w) points of the sites around an hcp A site within
+    radius (A)."""
+    G = hcp_gram(a0, c_over_a)
+    R = int(np.ceil(2.0 * np.sqrt(3.0) * radius / a0)) + 1    # u^2 - uv + v^2 >= 3u^2/4
+    W = int(np.ceil(2.0 * radius / np.sqrt(G[2, 2] * 4.0))) + 2
+    g = np.array(list(itertools.product(range(-R, R + 1), range(-R, R + 1),
+                                        range(-W, W + 1))))
+    g = g[_hcp_site_type(g) >= 0]
+    return g[np.sqrt(np.einsum("ni,ij,nj->n", g, G, g)) <= radius + 1e-9]
+
+
+def length_unit(lattice, a0):
+    """Length of one unit of a class's reff_units(): a0/2 on the cubic
+    lattices, 1 A on hcp."""
+    return 1.0 if lattice == "hcp" else a0 / 2.0
+
+
+def enumerate_classes(a0, rmax_half, lattice="fcc", nleg_max=4, c_over_a=None):
+    """The 3- and 4-leg path classes of a lattice to half length rmax: the
+    cubic lattices in units of a0/2 under O_h; hcp (A absorbers; B absorbers
+    see the inverted paths) in (u, v, w) under its 12 site operations."""
+    if lattice == "hcp":
+        ops, gram = HCP_OPS, hcp_gram(a0, c_over_a)
+        Lmax = 2.0 * rmax_half + 1e-9
+        pts = hcp_points(a0, rmax_half, c_over_a)
+
+        def norm_of(x):
+            x = np.atleast_2d(x)
+            return np.sqrt(np.einsum("ni,ij,nj->n", x, gram, x))
+    else:
+        ops, gram = OPS, None
+        unit = a0 / 2.0
+        Lmax = 2.0 * rmax_half / unit + 1e-9
+        pts = lattice_points(lattice, rmax_half / unit)
+
+        def norm_of(x):
+            return np.linalg.norm(np.atleast_2d(x), axis=1)
     nz = pts[np.any(pts != 0, axis=1)]
-    norm = np.linalg.norm(pts, axis=1)
+    norm = norm_of(pts)
+    nzn = norm_of(nz)
     keys = set()
-    zero = np.zeros(3, int)
-    for q1 in nz:
-        l1 = np.linalg.norm(q1)
-        # 3 legs: 0 -> q1 -> q2 -> 0
-        for q2 in nz:
-            if np.array_equal(q2, q1):
-                continue
-            L = l1 + np.linalg.norm(q2 - q1) + np.linalg.norm(q2)
-            if L <= Lmax:
-                keys.add(canonical([q1, q2]))
-        if nleg_max < 4:
-            continue
-        # 4 legs: 0 -> q1 -> q2 -> q3 -> 0 (q2 may be the absorber)
-        for i2, q2 in enumerate(pts):
-            if np.array_equal(q2, q1):
-                continue
-            l12 = l1 + np.linalg.norm(q2 - q1)
-            if l12 + norm[i2] > Lmax:
-                continue
-            for q3 in nz:
-                if np.array_equal(q3, q2):
+    if gram is None:
+        for q1 in nz:
+            l1 = np.linalg.norm(q1)
+            # 3 legs: 0 -> q1 -> q2 -> 0
+            for q2 in nz:
+                if np.array_equal(q2, q1):
                     continue
-                L = l12 + np.linalg.norm(q3 - q2) + np.linalg.norm(q3)
+                L = l1 + np.linalg.norm(q2 - q1) + np.linalg.norm(q2)
                 if L <= Lmax:
-                    keys.add(canonical([q1, q2, q3]))
-    del zero
-    ks = sorted(keys, key=lambda k: (len(k), PathClass(k).reff_units(), k))
-    return [PathClass(k) for k in ks]
+                    keys.add(canonical([q1, q2]))
+            if nleg_max < 4:
+                continue
+            # 4 legs: 0 -> q1 -> q2 -> q3 -> 0 (q2 may be the absorber)
+            for i2, q2 in enumerate(pts):
+                if np.array_equal(q2, q1):
+                    continue
+                l12 = l1 + np.linalg.norm(q2 - q1)
+                if l12 + norm[i2] > Lmax:
+                    continue
+                for q3 in nz:
+                    if np.array_equal(q3, q2):
+                        continue
+                    L = l12 + np.linalg.norm(q3 - q2) + np.linalg.norm(q3)
+                    if L <= Lmax:
+                        keys.add(canonical([q1, q2, q3]))
+    else:
+        # the same walks, leg lengths through the metric, vectorised over
+        # the last point
+        for q1, l1 in zip(nz, nzn):
+            L3 = l1 + norm_of(nz - q1) + nzn
+            for q2 in nz[(L3 <= Lmax) & np.any(nz != q1, axis=1)]:
+                keys.add(canonical([q1, q2], ops))
+            if nleg_max < 4:
+                continue
+            l12 = l1 + norm_of(pts - q1)
+            for i2 in np.nonzero((l12 + norm <= Lmax) & np.any(pts != q1, axis=1))[0]:
+                q2 = pts[i2]
+                L4 = l12[i2] + norm_of(nz - q2) + nzn
+                for q3 in nz[(L4 <= Lmax) & np.any(nz != q2, axis=1)]:
+                    keys.add(canonical([q1, q2, q3], ops))
+    ks = sorted(keys, key=lambda k: (len(k), PathClass(k, ops, gram).reff_units(), k))
+    return [PathClass(k, ops, gram) for k in ks]
 
 
 def entry_list(classes, nsp):
@@ -187,39 +313,68 @@ def synthetic_table(classes, nsp, k, f, delta, lam, sigma2_nn, r_nn, unit, c_ms=
 
 
 class SupercellPaths:
-    """Every image of every class at every site of a periodic cubic supercell.
+    """Every image of every class at every site of a periodic supercell.
 
     ideal (natoms, 3) and H (3, 3) of the supercell; a0 its lattice constant.
     Arrays (as mslibrary.py:357-404): p_abs, p_cls (npath), p_slot (npath, 3);
     inc (natoms, M) incident path ids padded with npath; records (npath, 4)
     and inc_rec (natoms, M, 4) for the device.
+
+    Cubic lattices (fcc, bcc, sc) need an orthogonal box and use integer
+    coordinates in units of a0/2. hcp is selected by passing its hexagonal
+    conventional cell `conv` (lattice.CrystalSupercell.cell_matrix): sites
+    then have integer coordinates (u, v, w), the box is periodic in them, and
+    the classes (enumerated for an A absorber) are placed at A sites as they
+    are and at B sites inverted, since inversion through the midpoint of an
+    A-B bond maps the hcp structure onto itself with A and B exchanged.
     """
 
-    def __init__(self, classes, ideal, H, a0, nsp):
+    def __init__(self, classes, ideal, H, a0, nsp, conv=None):
         self.classes = classes
         self.nsp = nsp
         self.nblk = int(sum(nsp ** c.nslot for c in classes))
         self.nent = nsp * self.nblk
         self.cls_off = class_offsets(classes, nsp)
-        unit = a0 / 2.0
-        X = np.asarray(ideal, float) / unit
-        Xi = np.rint(X).astype(int)
-        if not np.allclose(X, Xi, atol=1e-6):
-            raise ValueError("supercell sites are not lattice points in units of a0/2")
-        Hu = np.asarray(H, float) / unit
-        if not np.allclose(Hu, np.diag(np.diag(Hu))):
-            raise ValueError("exact multiple scattering needs an orthogonal box")
-        box = np.rint(np.diag(Hu)).astype(int)
-        Xi %= box
+        self.hex = conv is not None and abs(float(np.asarray(conv)[1, 0])) > 1e-12
+        if self.hex:
+            Ainv = np.linalg.inv(np.asarray(conv, float))
+            X = (np.asarray(ideal, float) @ Ainv) * HCP_SCALE
+            Xi = np.rint(X).astype(int)
+            if not np.allclose(X, Xi, atol=1e-6):
+                raise ValueError("supercell sites are not hcp lattice points")
+            Hu = (np.asarray(H, float) @ Ainv) * HCP_SCALE
+            if not np.allclose(Hu, np.diag(np.diag(Hu))):
+                raise ValueError("exact multiple scattering needs a box of whole hexagonal cells")
+            box = np.rint(np.diag(Hu)).astype(int)
+            Xi %= box
+            kind = _hcp_site_type(Xi)
+            if (kind < 0).any():
+                raise ValueError("supercell sites are not hcp lattice points")
+            self.sign = (1 - 2 * kind).astype(int)           # +1 on A sites, -1 on B
+        else:
+            unit = a0 / 2.0
+            X = np.asarray(ideal, float) / unit
+            Xi = np.rint(X).astype(int)
+            if not np.allclose(X, Xi, atol=1e-6):
+                raise ValueError("supercell sites are not lattice points in units of a0/2")
+            Hu = np.asarray(H, float) / unit
+            if not np.allclose(Hu, np.diag(np.diag(Hu))):
+                raise ValueError("exact multiple scattering needs an orthogonal box")
+            box = np.rint(np.diag(Hu)).astype(int)
+            Xi %= box
+            self.sign = np.ones(len(Xi), int)
         look = -np.ones(tuple(box), int)
         look[Xi[:, 0], Xi[:, 1], Xi[:, 2]] = np.arange(len(Xi))
         n = self.natoms = len(Xi)
+        sgn = self.sign[:, None, None]
         P_abs, P_cls, P_slot = [], [], []
         for g, cl in enumerate(classes):
-            if 2 * np.abs(cl.rep).max() >= box.min():
+            small = (np.any(2 * np.abs(cl.rep).max(0) >= box) if self.hex
+                     else 2 * np.abs(cl.rep).max() >= box.min())
+            if small:
                 raise ValueError("supercell too small for the paths")
             for img, so in cl.images:
-                p = (Xi[:, None, :] + img[None]) % box
+                p = (Xi[:, None, :] + sgn * img[None]) % box
                 sites = look[p[..., 0], p[..., 1], p[..., 2]]
                 if (sites < 0).any():
                     raise ValueError("an image lands off the lattice")
@@ -291,6 +446,12 @@ class SupercellPaths:
                                      for q in range(cl.nslot)]
                 pos += [None] * (4 - len(pos))
                 for r in range(1 + cl.nslot):              # the site at position r
+                    # hcp: a site at an A->B position of an A-absorber image
+                    # is a B site, and the same paths seen from a B site are
+                    # the inverted ones; B sites read their neighbourhood
+                    # table at the inverted offsets, so the row stores the
+                    # offsets inverted and serves both sublattices.
+                    flip = -1 if (self.hex and _hcp_site_type(np.array(pos[r])) == 1) else 1
                     code = 0
                     for p in range(4):
                         if p == r:
@@ -298,7 +459,7 @@ class SupercellPaths:
                         elif pos[p] is None:
                             v = self.NONE
                         else:
-                            d = tuple(int(x) for x in np.subtract(pos[p], pos[r]))
+                            d = tuple(flip * int(x) for x in np.subtract(pos[p], pos[r]))
                             v = offs.setdefault(d, len(offs))
                         code |= v << (8 * p)
                     rows.append((int(self.cls_off[g]), code))
@@ -312,7 +473,7 @@ class SupercellPaths:
         self.tpl = np.empty((len(rows), 2), np.int32)
         self.tpl[:, 0] = t[:, 0]
         self.tpl[:, 1] = (t[:, 1] & 0xFFFFFFFF).astype(np.uint32).view(np.int32)
-        q = (Xi[:, None, :] + D[None, :, :]) % box
+        q = (Xi[:, None, :] + self.sign[:, None, None] * D[None, :, :]) % box
         self.nbr = look[q[..., 0], q[..., 1], q[..., 2]].astype(np.int32)
         if (self.nbr < 0).any():
             raise ValueError("a neighbourhood offset lands off the lattice")

@@ -167,6 +167,31 @@ def test_mixed_species_counts_equal_separate_runs(cuda):
             assert np.array_equal(together[i][k], v), (i, k)
 
 
+def test_hcp_exact_ms_tracks_recount(cuda):
+    """hcp with exact MS (classes in hexagonal coordinates, B sites reading
+    the inverted template offsets): after FP32C batched steps each slot's
+    running MS entry counts equal a recount of its state, and its running
+    chi equals the FP64 recompute to 1e-6 per absorber."""
+    from chimera_b200 import configs
+    from chimera_b200.sampler import BatchedSampler, LadderSpec
+    prob = configs.Problem(elements=("Co", "Ni"), a0=2.507, lattice="hcp", ncell=(8, 8, 6),
+                           alpha1=-0.05)
+    assert prob.paths is not None and prob.paths.hex
+    pos = prob.position(0)
+    spec = LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R, nrep=16, tmin=1e-3,
+                      tmax=1e-1, seed=1, swap_frac=1.0, ms_library=prob.ms)
+    bs = BatchedSampler([spec], precision=1, exchange_every=25, reanchor_every=0)
+    bs.init_state([prob.random_config(1)], [prob.cell.ideal])
+    bs.run_blocks(8)
+    assert bs.device_error() == 0
+    b = bs.lad.bufs[0]
+    assert int(b["n_acc"].sum()) > 50
+    assert np.array_equal(b["ms_C"].cpu().numpy(), prob.ms.counts(b["species"]).cpu().numpy())
+    full = (prob.fm.chi_full(b["pos"], b["species"]) + prob.ms.chi_of(b["ms_C"])).cpu().numpy()
+    cnt = b["count"].cpu().numpy()[:, :, None]
+    assert np.abs(b["chi"].cpu().numpy() / cnt - full / cnt).max() <= 1e-6
+
+
 def test_best_state_is_the_state_of_the_best_chi2(cuda):
     """The best state is written once per launch (or when its log of later
     moves fills up) as the current state with the moves after the best

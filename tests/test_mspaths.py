@@ -124,3 +124,118 @@ def test_templates_give_the_incident_paths_entries(classes, nsp):
                      sp.cls_off, nsp, sp.nblk, np.array([a], np.int32), np.array([b], np.int32),
                      np.array([nsa], np.int32), np.array([nsb], np.int32))[0]
     assert np.array_equal(dC, ref)
+
+
+def _closed_walks(pts, norm_of, Lmax, nleg_max=4):
+    """Every closed walk 0 -> q1 -> q2 (-> q3) -> 0 by brute force: q1 and
+    the last point off the absorber, consecutive points distinct, total
+    length <= Lmax (the 4-leg middle point may be the absorber)."""
+    nz = [tuple(q) for q in pts if any(q)]
+    walks = set()
+    for q1 in nz:
+        for q2 in nz:
+            if q2 != q1 and (norm_of(q1) + norm_of(np.subtract(q2, q1)) + norm_of(q2)) <= Lmax:
+                walks.add((q1, q2))
+        if nleg_max < 4:
+            continue
+        for q2 in map(tuple, pts):
+            if q2 == q1:
+                continue
+            l12 = norm_of(q1) + norm_of(np.subtract(q2, q1))
+            for q3 in nz:
+                if q3 != q2 and l12 + norm_of(np.subtract(q3, q2)) + norm_of(q3) <= Lmax:
+                    walks.add((q1, q2, q3))
+    return walks
+
+
+@pytest.mark.parametrize("lattice", ["fcc", "hcp"])
+def test_class_images_are_every_closed_walk(lattice):
+    """The directed images of all classes are exactly the closed walks of
+    the lattice (each once), fcc in units of a0/2 under O_h and hcp in
+    hexagonal integer coordinates under its 12 site operations, to a half
+    length of 4.6 A (3- and 4-leg)."""
+    if lattice == "fcc":
+        a0, rh = 3.59, 4.6
+        cls = MP.enumerate_classes(a0, rh, "fcc")
+        pts = MP.lattice_points("fcc", rh / (a0 / 2))
+        Lmax = 2 * rh / (a0 / 2) + 1e-9
+
+        def norm_of(x):
+            return float(np.linalg.norm(x))
+    else:
+        a0, rh = 2.507, 4.6
+        cls = MP.enumerate_classes(a0, rh, "hcp")
+        pts = MP.hcp_points(a0, rh)
+        G = MP.hcp_gram(a0)
+        Lmax = 2 * rh + 1e-9
+
+        def norm_of(x):
+            x = np.asarray(x, float)
+            return float(np.sqrt(x @ G @ x))
+    imgs = [tuple(map(tuple, img)) for c in cls for img, _ in c.images]
+    assert len(imgs) == len(set(imgs))
+    assert set(imgs) == _closed_walks(pts, norm_of, Lmax)
+    assert all(c.nleg in (3, 4) for c in cls)
+
+
+def test_hcp_operations_are_the_site_group():
+    """The 12 hcp operations form a group, preserve the metric and map A->A
+    and A->B displacements onto themselves; the 60-degree rotation (a screw
+    axis in hcp) is not among them."""
+    ops = MP.HCP_OPS
+    G = MP.hcp_gram(2.507)
+    keys = {tuple(A.ravel()) for A in ops}
+    assert len(keys) == 12
+    for A in ops:
+        assert np.allclose(A.T @ G @ A, G)
+        for B in ops:
+            assert tuple((A @ B).ravel()) in keys
+    assert (1, -1, 0, 1, 0, 0, 0, 0, 1) not in keys
+    pts = MP.hcp_points(2.507, 6.0)
+    kind = MP._hcp_site_type(pts)
+    for A in ops:
+        assert np.array_equal(MP._hcp_site_type(pts @ A.T), kind)
+
+
+@pytest.mark.parametrize("lattice,a0,nc", [("bcc", 2.87, (6, 6, 6)), ("hcp", 2.507, (8, 8, 6))])
+def test_templates_cover_incident_paths_on_bcc_and_hcp(lattice, a0, nc):
+    """On bcc and on hcp (both sublattices, B sites reading the inverted
+    offsets), each site's template paths carry the entries of its incidence
+    records, every site has the same number of incident paths, and a swap's
+    count change from templates equals the oracle's recount difference."""
+    cell = L.CrystalSupercell(lattice, nc, a0)
+    cls = MP.enumerate_classes(a0, 5.5, lattice)
+    nsp = 2
+    sp = MP.SupercellPaths(cls, cell.ideal, cell.H, a0, nsp, conv=cell.cell_matrix)
+    cnt = np.bincount(sp.p_abs, minlength=sp.natoms)
+    for q in range(3):
+        s = sp.p_slot[:, q]
+        cnt += np.bincount(s[s >= 0], minlength=sp.natoms)
+    assert cnt.min() == cnt.max() == sp.M
+    rng = np.random.default_rng(7)
+    species = rng.integers(0, nsp, sp.natoms).astype(np.int32)
+    sites = list(rng.integers(0, sp.natoms, 3)) + [1, 2]      # hcp: sites 0/1 are A/B
+    for site in sites:
+        pids = sp.inc[site]
+        pids = pids[pids < sp.npath]
+        rec = []
+        for pid in pids:
+            e = species[sp.p_abs[pid]] * sp.nblk + sp.cls_off[sp.p_cls[pid]]
+            for q in range(3):
+                if sp.p_slot[pid, q] >= 0:
+                    e += species[sp.p_slot[pid, q]] * nsp ** q
+            rec.append(e)
+        assert np.array_equal(np.sort(sp.template_entries(species, site)), np.sort(rec))
+    if lattice == "hcp":
+        assert set(sp.sign[:2]) == {1, -1}
+    a, b = 3, int(sp.nbr[3, 5])
+    while species[a] == species[b]:
+        species[b] = 1 - species[b]
+    C0 = K.ms_counts(species[None], sp.p_abs, sp.p_cls, sp.p_slot, sp.cls_off, nsp, sp.nblk)[0]
+    sw = species.copy()
+    sw[a], sw[b] = species[b], species[a]
+    C1 = K.ms_counts(sw[None], sp.p_abs, sp.p_cls, sp.p_slot, sp.cls_off, nsp, sp.nblk)[0]
+    dC = K.ms_delta(species[None], sp.inc, sp.p_abs, sp.p_cls, sp.p_slot, sp.npath,
+                    sp.cls_off, nsp, sp.nblk, np.array([a], np.int32), np.array([b], np.int32),
+                    np.array([species[b]], np.int32), np.array([species[a]], np.int32))[0]
+    assert np.array_equal(C1 - C0, dC)
