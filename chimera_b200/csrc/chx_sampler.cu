@@ -809,10 +809,78 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         }
         __syncthreads();
 
-        // ---- 3. delta chi(k): thread per k
+        // ---- 3. delta chi(k)
         const int ndir = s_ndir, ndnz = s_ndn, nms = s_nhist;
         const double *CH = s_chi;
         const double *CNT = L.count + (long)c * NSP;
+        if (PREC != CHX_FP64 && (nent == 0 || msT32 != nullptr)) {
+            // FP32 tables: one item per (absorber species, pair of k points),
+            // each summing only its absorber's direct records, table rows and
+            // MS rows (two float2 loads' worth of k per row), in the same
+            // order as a sum per k over all rows, so the result is the same
+            // to the bit; the FP32 tables' row stride is nk rounded up to even.
+            // The k pairs of one absorber fill whole warps (npw, a multiple
+            // of 32), so no warp runs two absorbers' row loops in turn.
+            const int nk2 = (nk + 1) & ~1, npk = nk2 >> 1, npw = (npk + 31) & ~31;
+            for (int it = tid; it < NSP * npw; it += blockDim.x) {
+                const int sa_ = it / npw, k0 = 2 * (it - sa_ * npw);
+                if (k0 >= nk) continue;
+                const bool k1ok = k0 + 1 < nk;
+                double acc0 = 0.0, acc1 = 0.0;
+                if (ndir) {
+                    KConst<NSP> kc0, kc1;
+                    load_kconst<NSP>(kc0, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, k0);
+                    load_kconst<NSP>(kc1, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk,
+                                     k1ok ? k0 + 1 : k0);
+                    for (int q = 0; q < ndir; ++q) {
+                        PairRec d = s_dir[l_dir[q]];
+                        const int neg = d.t >> 16;
+                        d.t &= 0xFFFF;
+                        if (d.t / NSP != sa_) continue;
+                        const double v0 = rec_term<NSP, PREC>(d, kc0);
+                        acc0 += neg ? -v0 : v0;
+                        if (k1ok) {
+                            const double v1 = rec_term<NSP, PREC>(d, kc1);
+                            acc1 += neg ? -v1 : v1;
+                        }
+                    }
+                }
+                if (use_tab) {
+                    for (int q = 0; q < ndnz; ++q) {
+                        const int2 jc = l_dn[q];
+                        if ((jc.x % nn) / NSP != sa_) continue;
+                        const float2 t = __ldg((const float2 *)&L.sstab32[(long)jc.x * nk2 + k0]);
+                        acc0 += (double)((float)jc.y * t.x);
+                        acc1 += (double)((float)jc.y * t.y);
+                    }
+                }
+                {
+                    const int q0 = s_msb[sa_], q1 = s_msb[sa_ + 1];
+                    float2 sm = make_float2(0.f, 0.f);
+#pragma unroll 16
+                    for (int q = q0; q < q1; ++q) {
+                        const int2 ec = l_ms[q];
+                        const float w = (float)ec.y;
+                        sm = ffma2(make_float2(w, w),
+                                   __ldg((const float2 *)&msT32[(long)ec.x * nk2 + k0]), sm);
+                    }
+                    acc0 += (double)sm.x;
+                    acc1 += (double)sm.y;
+                }
+                const double inv = fmax(CNT[sa_], 1.0);
+                const int o = sa_ * nk + k0;
+                s_dchi[o] = acc0;
+                double v = (CH[o] + acc0) / inv;
+                if (L.chi_extra) v += L.chi_extra[o];
+                s_tr[o] = v;
+                if (k1ok) {
+                    s_dchi[o + 1] = acc1;
+                    v = (CH[o + 1] + acc1) / inv;
+                    if (L.chi_extra) v += L.chi_extra[o + 1];
+                    s_tr[o + 1] = v;
+                }
+            }
+        } else
         for (int ik = tid; ik < nk; ik += blockDim.x) {
             double acc[NSP];
 #pragma unroll

@@ -45,6 +45,17 @@ def _host(x):
     return np.asarray(x)
 
 
+def _fp32_rows(t):
+    """FP32 copy of a (rows, nk) FP64 table with the row stride rounded up to
+    an even count (a zero column when nk is odd), the layout of the step
+    kernel's FP32 tables: it reads k points in pairs."""
+    import torch
+    rows, nk = t.shape
+    out = torch.zeros((rows, nk + (nk & 1)), dtype=torch.float32, device=t.device)
+    out[:, :nk] = t
+    return out
+
+
 def _ft_setup(ft, nsp):
     """Per-channel window coefficients of a MultiEdgeFT-like object (or one
     FourierTransform): n0, idx, frac, w padded to a common length."""
@@ -196,7 +207,7 @@ class Ladders:
                 rs, ss = self._t(r_shell), self._t(s2_shell)
                 N.call("chx_shell_table", C.byref(L), N.ptr(rs), N.ptr(ss),
                        N.ptr(cell["sstab"]), N.stream())
-                cell["sstab32"] = cell["sstab"].float().contiguous()
+                cell["sstab32"] = _fp32_rows(cell["sstab"])
                 self.keep.append(cell["sstab32"])
             b["sstab"], b["sstab32"] = cell["sstab"], cell["sstab32"]
             L.sstab, L.sstab32 = N.dptr(b["sstab"]), N.dptr(b["sstab32"])
@@ -212,7 +223,7 @@ class Ladders:
             if self.precision != FP64:
                 key = ("msT32", id(ms))
                 if key not in cell:
-                    cell[key] = ms.T.float().contiguous()
+                    cell[key] = _fp32_rows(ms.T)
                     self.keep.append(cell[key])
                 b["msT32"] = cell[key]
                 L.ms_T32 = N.dptr(b["msT32"])

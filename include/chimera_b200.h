@@ -263,7 +263,9 @@ typedef struct {
     const double *ftab, *dtab, *lamtab, *ktab, *drtab, *c3tab, *s2tab;
     double s02;
     const double *sstab;             /* (nshell*nsp*nsp, nk) ideal-shell terms, or NULL */
-    const float *sstab32;            /* the same table in FP32 (CHX_FP32C), or NULL    */
+    const float *sstab32;            /* the same table in FP32 (CHX_FP32C), or NULL;
+                                        row stride nk rounded up to even, the pad
+                                        column zero (k points are read in pairs)   */
     /* exact multiple scattering, ms_nblk == 0 when off. The paths through a
        site are ms_M shared templates {class entry offset, 4 position bytes:
        neighbourhood index of the absorber and slots 0-2, 0xFE the site itself,
@@ -272,7 +274,8 @@ typedef struct {
     const int *ms_tpl;               /* (ms_M, 2) path templates                  */
     const int *ms_nbr;               /* (natoms, ms_D) neighbourhood site indices */
     const double *ms_T;              /* (nsp*ms_nblk, nk)                         */
-    const float *ms_T32;             /* the same table in FP32 (CHX_FP32C), or NULL */
+    const float *ms_T32;             /* the same table in FP32 (CHX_FP32C), or NULL;
+                                        row stride nk rounded up to even, as sstab32 */
     /* pair-interaction prior, etab NULL when off (method_a_rmc.py:147-157,310-320) */
     const double *etab;              /* (nshell*nsp*nsp) eV per directed pair     */
     double energy_beta;
