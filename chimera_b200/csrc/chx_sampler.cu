@@ -732,25 +732,36 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         if (do_ms) {
             const int M = L.ms_M, D = L.ms_D, nblk = L.ms_nblk;
             const uint2 *tpl = (const uint2 *)L.ms_tpl;
-#pragma unroll 4
-            for (int m = tid; m < 2 * M; m += blockDim.x) {
-                const int half = m >= M;
-                const uint2 t = __ldg(&tpl[m - half * M]);
-                const uint16_t *nb = s_nb + half * (D + 2);
-                int eo = (int)t.x, en = (int)t.x, hasa = 0;
+            // each template once, resolved at site a (half 0) and site b
+            // (half 1): one load feeds two independent lookup chains
+#pragma unroll 2
+            for (int m = tid; m < M; m += blockDim.x) {
+                const uint2 t = __ldg(&tpl[m]);
+                int eo[2], en[2], hasa[2];
 #pragma unroll
-                for (int pp = 0; pp < 4; ++pp) {
-                    const int v = (t.y >> (8 * pp)) & 0xFF;
-                    const int mul = pp == 0 ? nblk : (pp == 1 ? 1 : (pp == 2 ? NSP : NSP * NSP));
-                    const int w = nb[v < 0xFE ? v : D + (v - 0xFE)];
-                    eo += (w & 0x7F) * mul;
-                    en += ((w >> 8) & 0x7F) * mul;
-                    hasa |= w & 0x8000;
+                for (int half = 0; half < 2; ++half) {
+                    const uint16_t *nb = s_nb + half * (D + 2);
+                    eo[half] = en[half] = (int)t.x;
+                    hasa[half] = 0;
+#pragma unroll
+                    for (int pp = 0; pp < 4; ++pp) {
+                        const int v = (t.y >> (8 * pp)) & 0xFF;
+                        const int mul =
+                            pp == 0 ? nblk : (pp == 1 ? 1 : (pp == 2 ? NSP : NSP * NSP));
+                        const int w = nb[v < 0xFE ? v : D + (v - 0xFE)];
+                        eo[half] += (w & 0x7F) * mul;
+                        en[half] += ((w >> 8) & 0x7F) * mul;
+                        hasa[half] |= w & 0x8000;
+                    }
                 }
                 // a path through both sites counts once (in the half of site a)
-                if (!(half && hasa) && eo != en) {
-                    atomicAdd(&s_hist[en], 1);
-                    atomicSub(&s_hist[eo], 1);
+                if (eo[0] != en[0]) {
+                    atomicAdd(&s_hist[en[0]], 1);
+                    atomicSub(&s_hist[eo[0]], 1);
+                }
+                if (!hasa[1] && eo[1] != en[1]) {
+                    atomicAdd(&s_hist[en[1]], 1);
+                    atomicSub(&s_hist[eo[1]], 1);
                 }
             }
         }
