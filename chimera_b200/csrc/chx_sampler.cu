@@ -188,6 +188,96 @@ __device__ __noinline__ void ft_window(const chx_ladder_t &L, const double *s_tr
     __syncthreads();
     const int fmask = L.nfft - 1;
     const int n0 = L.ft_n0[0];
+    if constexpr (PREC != CHX_FP64 && (MAXCH + 1) / 2 <= 3) {
+        // FP32, up to 3 channel pairs: two window bins per thread (qa and
+        // qb = qa + nbp), so one shared-memory load of a tap's channel pair
+        // feeds both; the taps split into ns runs held by ns adjacent lanes,
+        // whose partial sums meet by shuffles, the first lane writing the
+        // scaled result. Every lane takes the same number of passes, so the
+        // shuffles always see the whole warp.
+        constexpr int MAXP = (MAXCH + 1) / 2;
+        const int npair = nchp / 2;
+        const int nbp = (nwin + 1) >> 1;
+        const int ns = nbp * 4 <= (int)blockDim.x ? 4 : (nbp * 2 <= (int)blockDim.x ? 2 : 1);
+        const int total = nbp * ns;
+        const int jper = (ncoef + ns - 1) / ns;
+        const float inv_half = 2.0f / (float)L.nfft;
+        const int passes = (total + blockDim.x - 1) / blockDim.x;
+        for (int pass = 0; pass < passes; ++pass) {
+            const int item = pass * blockDim.x + tid;
+            const bool valid = item < total;
+            const int bp = valid ? item / ns : 0, part = item - (item / ns) * ns;
+            const int qa = bp, qb = bp + nbp;
+            const bool hasb = valid && qb < nwin;
+            const int ma = L.win_bin[qa] & fmask, mb = L.win_bin[hasb ? qb : qa] & fmask;
+            const int j0 = valid ? part * jper : 0, j1 = valid ? min(ncoef, j0 + jper) : 0;
+            const float2 ra = twiddle(ma, inv_half), rb = twiddle(mb, inv_half);
+            float2 are[MAXP], aim[MAXP], bre[MAXP], bim[MAXP];
+#pragma unroll
+            for (int p = 0; p < MAXP; ++p)
+                are[p] = aim[p] = bre[p] = bim[p] = make_float2(0.f, 0.f);
+            for (int jb = j0; jb < j1; jb += kReseed) {
+                float2 za = twiddle((int)(((long)(n0 + jb) * ma) & fmask), inv_half);
+                float2 zb = twiddle((int)(((long)(n0 + jb) * mb) & fmask), inv_half);
+                const int je = min(j1, jb + kReseed);
+                for (int j = jb; j < je; ++j) {
+                    const float2 *uj = (const float2 *)(s_u + j * nchp);
+                    const float2 zax = make_float2(za.x, za.x), zay = make_float2(za.y, za.y);
+                    const float2 zbx = make_float2(zb.x, zb.x), zby = make_float2(zb.y, zb.y);
+#pragma unroll
+                    for (int p = 0; p < MAXP; ++p)
+                        if (p < npair) {
+                            const float2 u = uj[p];
+                            are[p] = ffma2(u, zax, are[p]);
+                            aim[p] = ffma2(u, zay, aim[p]);
+                            bre[p] = ffma2(u, zbx, bre[p]);
+                            bim[p] = ffma2(u, zby, bim[p]);
+                        }
+                    float t = za.x * ra.x - za.y * ra.y;
+                    za.y = fmaf(za.x, ra.y, za.y * ra.x);
+                    za.x = t;
+                    t = zb.x * rb.x - zb.y * rb.y;
+                    zb.y = fmaf(zb.x, rb.y, zb.y * rb.x);
+                    zb.x = t;
+                }
+            }
+            for (int o = 1; o < ns; o <<= 1) {
+#pragma unroll
+                for (int p = 0; p < MAXP; ++p) {
+                    are[p].x += __shfl_xor_sync(0xffffffffu, are[p].x, o);
+                    are[p].y += __shfl_xor_sync(0xffffffffu, are[p].y, o);
+                    aim[p].x += __shfl_xor_sync(0xffffffffu, aim[p].x, o);
+                    aim[p].y += __shfl_xor_sync(0xffffffffu, aim[p].y, o);
+                    bre[p].x += __shfl_xor_sync(0xffffffffu, bre[p].x, o);
+                    bre[p].y += __shfl_xor_sync(0xffffffffu, bre[p].y, o);
+                    bim[p].x += __shfl_xor_sync(0xffffffffu, bim[p].x, o);
+                    bim[p].y += __shfl_xor_sync(0xffffffffu, bim[p].y, o);
+                }
+            }
+            if (valid && part == 0) {
+                const double nrm = L.ft_norm;
+#pragma unroll
+                for (int p = 0; p < MAXP; ++p) {
+                    if (2 * p < nchan) {
+                        s_x[(2 * p) * nwin + qa] =
+                            real2{(real)(are[p].x * nrm), (real)(aim[p].x * nrm)};
+                        if (hasb)
+                            s_x[(2 * p) * nwin + qb] =
+                                real2{(real)(bre[p].x * nrm), (real)(bim[p].x * nrm)};
+                    }
+                    if (2 * p + 1 < nchan) {
+                        s_x[(2 * p + 1) * nwin + qa] =
+                            real2{(real)(are[p].y * nrm), (real)(aim[p].y * nrm)};
+                        if (hasb)
+                            s_x[(2 * p + 1) * nwin + qb] =
+                                real2{(real)(bre[p].y * nrm), (real)(bim[p].y * nrm)};
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        return;
+    }
     const int nsplit = max(1, min(kMaxSplit, (int)blockDim.x / max(nwin, 1)));
     const int jper = (ncoef + nsplit - 1) / nsplit;
     const int nx = nchan * nwin;
