@@ -922,6 +922,29 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             // to the bit; the FP32 tables' row stride is nk rounded up to even.
             // The k pairs of one absorber fill whole warps (npw, a multiple
             // of 32), so no warp runs two absorbers' row loops in turn.
+            // Direct records (pairs with a displaced atom) first, one thread
+            // per k over all of them as the per-k sum does, so that their
+            // cost spreads evenly whatever absorbers they belong to; their
+            // sums seed the per-absorber items below.
+            if (ndir) {
+                for (int ik = tid; ik < nk; ik += blockDim.x) {
+                    double acc[NSP];
+#pragma unroll
+                    for (int s = 0; s < NSP; ++s) acc[s] = 0.0;
+                    KConst<NSP> kc;
+                    load_kconst<NSP>(kc, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, ik);
+                    for (int q = 0; q < ndir; ++q) {
+                        PairRec d = s_dir[l_dir[q]];
+                        const int neg = d.t >> 16;
+                        d.t &= 0xFFFF;
+                        const double v = rec_term<NSP, PREC>(d, kc);
+                        add_by_species<NSP>(acc, d.t / NSP, neg ? -v : v);
+                    }
+#pragma unroll
+                    for (int s = 0; s < NSP; ++s) s_dchi[s * nk + ik] = acc[s];
+                }
+                __syncthreads();
+            }
             const int nk2 = (nk + 1) & ~1, npk = nk2 >> 1, npw = (npk + 31) & ~31;
             for (int it = tid; it < NSP * npw; it += blockDim.x) {
                 const int sa_ = it / npw, k0 = 2 * (it - sa_ * npw);
@@ -929,22 +952,8 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 const bool k1ok = k0 + 1 < nk;
                 double acc0 = 0.0, acc1 = 0.0;
                 if (ndir) {
-                    KConst<NSP> kc0, kc1;
-                    load_kconst<NSP>(kc0, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, k0);
-                    load_kconst<NSP>(kc1, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk,
-                                     k1ok ? k0 + 1 : k0);
-                    for (int q = 0; q < ndir; ++q) {
-                        PairRec d = s_dir[l_dir[q]];
-                        const int neg = d.t >> 16;
-                        d.t &= 0xFFFF;
-                        if (d.t / NSP != sa_) continue;
-                        const double v0 = rec_term<NSP, PREC>(d, kc0);
-                        acc0 += neg ? -v0 : v0;
-                        if (k1ok) {
-                            const double v1 = rec_term<NSP, PREC>(d, kc1);
-                            acc1 += neg ? -v1 : v1;
-                        }
-                    }
+                    acc0 = s_dchi[sa_ * nk + k0];
+                    if (k1ok) acc1 = s_dchi[sa_ * nk + k0 + 1];
                 }
                 if (use_tab) {
                     for (int q = 0; q < ndnz; ++q) {
