@@ -494,6 +494,13 @@ def bench_uneven(args):
         t_sep += timed(lambda: one.run_blocks(nb))
         del one
     att = bs.nslots * EXCH * nb
+    # the same batch with delayed acceptance: one surrogate per (species
+    # count, feature width) class, learned from 40 periods of its own swaps
+    rep = bs.learn(blocks=40, epochs=4, H=256)
+    bs.capture()
+    bs.run_blocks(2)
+    t_learned = timed(lambda: bs.run_blocks(nb))
+    st = bs.last_screen.sum(0) if hasattr(bs, "last_screen") else np.zeros(4)
     line = {"metric": METRIC, "kernel": "uneven batch",
             "config": {"workload": "24 series points: fcc Fe-Ni a0 3.55-3.62 A (500-32,000 "
                                    "sites), bcc Fe-Cr 2.87 A, hcp Co-Ni 2.507 A, fcc/bcc "
@@ -506,6 +513,12 @@ def bench_uneven(args):
             "batched": {"attempts_per_s": att / t_batch, "gpu_s": t_batch,
                         "launch_shapes": [list(t["shape"]) for t in bs.tuning]},
             "one_ladder_per_launch": {"attempts_per_s": att / t_sep, "gpu_s": t_sep},
+            "learned": {"attempts_per_s": att / t_learned, "gpu_s": t_learned,
+                        "surrogates": len(bs.surrogates),
+                        "fit_rmse_over_sd": [round(r["rmse_d"] / r["std_d"], 3)
+                                             for r in (rep if isinstance(rep, list) else [rep])],
+                        "passed_to_exact": float(st[1] / max(st[0], 1)),
+                        "fallbacks": bs.fallbacks},
             "speedup": t_sep / t_batch, "unit": UNIT,
             "device_error": bs.device_error()}
     print(json.dumps(line), flush=True)

@@ -935,28 +935,43 @@ class BatchedSampler:
     fallbacks = 0
 
     def learn(self, blocks=40, epochs=4, H=256, lr=1e-3, seed=0, batch=4096, cap=None):
-        """Log the swaps of `blocks` exchange periods of plain steps, train a
-        surrogate on them (chimera_b200.surrogate) with one input row per
+        """Log the swaps of `blocks` exchange periods of plain steps, train
+        surrogates on them (chimera_b200.surrogate) with one input row per
         chain (ladder and rung), and switch every ladder to delayed
-        acceptance. Returns the training report."""
+        acceptance. A surrogate's input is the species around the swapped
+        pair, so ladders share one when they have the same species count and
+        feature width (lattices with the same first-shell coordination); a
+        batch of several lattices or species counts trains one per class.
+        Returns the training report (a list, one per class, when there are
+        several)."""
         from .surrogate import SwapSurrogate
-        lad = self.lad
-        cap = int(cap or self.exchange_every * blocks * max(s.nrep for s in lad.specs))
-        lad.enable_log(cap)
+        for lad in self.groups:
+            lad.enable_log(int(cap or self.exchange_every * blocks *
+                               max(s.nrep for s in lad.specs)))
         self.graph = None
         self.run_blocks(blocks)
-        codes, lnb, y, chain, _ = lad.swap_log(extra=True)
-        lad.disable_log()
-        D = lad.host[0].feat_D
-        if self.surrogate is None or self.surrogate.H != H or self.surrogate.nchain != lad.nslots:
-            self.surrogate = SwapSurrogate(lad.nsp, D, H=H, nchain=lad.nslots, seed=seed)
-        rep = self.surrogate.fit(codes, lnb, y, chain=chain, epochs=epochs, lr=lr, seed=seed,
-                                 batch=batch)
-        lad.attach_surrogate(self.surrogate)
-        lad.da_stats(reset=True)
+        old = getattr(self, "surrogates", None) or {}
+        self.surrogates, reports = {}, []
+        for g, lad in enumerate(self.groups):
+            classes = {}
+            for li in range(lad.nladders):
+                lad.feature_table(li)
+                classes.setdefault(int(lad.host[li].feat_D), []).append(li)
+            for D, lis in classes.items():
+                codes, lnb, y, chain, _ = lad.swap_log(ladders=lis, extra=True)
+                sur = old.get((g, D))
+                if sur is None or sur.H != H or sur.nchain != lad.nslots:
+                    sur = SwapSurrogate(lad.nsp, D, H=H, nchain=lad.nslots, seed=seed)
+                reports.append(sur.fit(codes, lnb, y, chain=chain, epochs=epochs, lr=lr,
+                                       seed=seed, batch=batch))
+                lad.attach_surrogate(sur, ladders=lis)
+                self.surrogates[(g, D)] = sur
+            lad.disable_log()
+            lad.da_stats(reset=True)
+        self.surrogate = next(iter(self.surrogates.values()))
         self.graph = None
-        self.train_report = rep
-        return rep
+        self.train_report = reports[0] if len(reports) == 1 else reports
+        return self.train_report
 
     def _check_screen(self):
         """Ladders whose screening error since the last check exceeds
@@ -964,16 +979,22 @@ class BatchedSampler:
         stage-2 rejection probability of the moves the screen let through,
         1 - mean min(1, exp(-beta nfit (d - d^))): 0 for an exact screen,
         the plain rejection rate for a screen that passes everything, the
-        share of exact evaluations the screen could have saved."""
-        st = self.lad.da_stats(reset=True)
-        on = self.lad.screening_on()
-        for li in range(self.lad.nladders):
-            if on[li] and st[li, 1] > 0:
-                err = 1.0 - st[li, 3] / st[li, 1]
-                if err > self.da_max_err:
-                    self.lad.set_screening(li, False)
-                    self.fallbacks += 1
-        self.last_screen = st
+        share of exact evaluations the screen could have saved.
+        `last_screen` keeps the (nladders, 4) statistics in ladder order."""
+        out = np.zeros((self.nladders, 4))
+        for lad in self.groups:
+            st = lad.da_stats(reset=True)
+            on = lad.screening_on()
+            for li in range(lad.nladders):
+                if on[li] and st[li, 1] > 0:
+                    err = 1.0 - st[li, 3] / st[li, 1]
+                    if err > self.da_max_err:
+                        lad.set_screening(li, False)
+                        self.fallbacks += 1
+            for gi, (g, q) in enumerate(self.where):
+                if self.groups[g] is lad:
+                    out[gi] = st[q]
+        self.last_screen = out
 
     def best(self, li):
         lad, q = self.ladder(li)

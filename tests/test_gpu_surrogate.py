@@ -272,3 +272,43 @@ def test_learned_screen_saves_exact_evaluations(cuda):
     assert passed < 0.75 and err < bs.da_max_err
     assert all(bs.lad.screening_on()) and bs.fallbacks == 0
     assert bs.lad.device_error() == 0
+
+
+def test_learn_on_mixed_lattices_and_species_counts(cuda):
+    """A batch of fcc and bcc binaries and an fcc ternary learns one
+    surrogate per (species count, feature width) class, each fitted on its
+    own ladders' logged swaps, and every ladder then screens with the
+    surrogate of its class: screened moves are counted on every ladder and
+    the chains stay error-free."""
+    from chimera_b200 import configs
+    from chimera_b200.sampler import BatchedSampler, LadderSpec
+    probs = [configs.Problem(ncell=(5, 5, 5)),
+             configs.Problem(elements=("Fe", "Cr"), a0=2.87, lattice="bcc", ncell=(6, 6, 6)),
+             configs.Problem(elements=("Fe", "Ni", "Cr"), composition=(0.4, 0.4, 0.2),
+                             ncell=(5, 5, 5))]
+    specs, starts = [], []
+    for q, prob in enumerate(probs):
+        for p in range(2):
+            pos = prob.position(10 * q + p)
+            specs.append(LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R,
+                                    nrep=16, tmin=0.05, tmax=0.5, seed=10 * q + p,
+                                    swap_frac=1.0, ms_library=prob.ms))
+            starts.append((prob.random_config(q + p), prob.cell.ideal))
+    bs = BatchedSampler(specs, precision=1, exchange_every=25, reanchor_every=0,
+                        check_every=10 ** 6)
+    bs.init_state([s for s, _ in starts], [x for _, x in starts])
+    bs.run_blocks(4)
+    reps = bs.learn(blocks=8, epochs=2, H=64)
+    assert isinstance(reps, list) and len(reps) == 3
+    keys = sorted(bs.surrogates)
+    assert [k[0] for k in keys] == [0, 0, 1]          # binaries: fcc and bcc widths; ternary
+    widths = {bs.ladder(li)[0].host[bs.ladder(li)[1]].feat_D for li in range(6)}
+    assert len(widths) == 2
+    for (g, D), sur in bs.surrogates.items():
+        assert sur.nsp == bs.groups[g].nsp and sur.D == D
+    bs.run_blocks(10)
+    bs._check_screen()                 # the first screening window after learning
+    st = bs.last_screen
+    assert (st[:, 0] > 0).all(), st
+    assert (st[:, 1] <= st[:, 0]).all() and (st[:, 2] <= st[:, 1]).all()
+    assert bs.device_error() == 0
