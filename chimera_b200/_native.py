@@ -78,6 +78,18 @@ class Mlp(C.Structure):
                 ("nchain", c_i)]
 
 
+class Shell(C.Structure):
+    """chx_shell_t"""
+    _fields_ = [("nsp", c_i), ("nshell", c_i), ("nk", c_i), ("nkw", c_i), ("nbin", c_i),
+                ("nfft", c_i), ("magnitude", c_i),
+                ("a0_ref", c_d), ("s02", c_d), ("dk_win", c_d), ("dk", c_d), ("etok", c_d),
+                ("k", c_p), ("f", c_p), ("delta", c_p), ("lam", c_p), ("shells_ref", c_p),
+                ("sigma2_ref", c_p), ("shell_mult", c_p), ("N", c_p), ("kweight", c_p),
+                ("bins", c_p), ("data", c_p),
+                ("npath", c_i), ("ms_dnn", c_d), ("ms_abs", c_p), ("ms_reff", c_p),
+                ("ms_deg", c_p), ("ms_F", c_p), ("ms_D", c_p), ("ms_L", c_p)]
+
+
 # argument types of every entry point, in header order
 _SIGS = {
     "chx_version": ([], c_i),
@@ -114,6 +126,8 @@ _SIGS = {
     "chx_mlp_grad": ([c_p] * 5 + [c_i] + [c_p] * 5, c_i),
     "chx_mlp_adam": ([c_p] * 5 + [c_i64, C.c_float, C.c_float, C.c_float, C.c_float, c_i, c_p],
                      c_i),
+    "chx_shell_nparam": ([c_i, c_i], c_i),
+    "chx_shell_rfactor": ([c_p, c_p, c_i, c_p, c_p, c_p], c_i),
 }
 
 # entry points declared in include/chimera_b200.h (checked by the tests)
@@ -142,9 +156,9 @@ def lib():
 
 
 def _check_abi(L):
-    got = tuple(L.chx_struct_size(q) for q in range(6))
+    got = tuple(L.chx_struct_size(q) for q in range(7))
     want = (C.sizeof(Pairs), C.sizeof(Ladder), Ladder.exch_acc.offset, Ladder.seed.offset,
-            C.sizeof(Mlp), Ladder.log_cap.offset)
+            C.sizeof(Mlp), Ladder.log_cap.offset, C.sizeof(Shell))
     if got != want:
         raise ChxError(f"ABI mismatch between chimera_b200.h and the binding: {got} != {want}")
 

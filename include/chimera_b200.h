@@ -416,6 +416,53 @@ CHX_API int chx_ft_batch(const double *chi, int rows, int nk, const double *basi
                  void *stream);
 CHX_API int64_t chx_ft_batch_scratch_bytes(int rows, int nk, int nR, int precision);
 
+/* ------------------------------------------------------------------------
+ * Pair-count (shell) calibration objective, for a population of parameter sets
+ *
+ * Replaces the host loop over a differential-evolution population of the
+ * reference's ShellModel.r_factor (chimera/shellmodel.py:427-440; basis
+ * :290-336, chi_k :411-413, chi_ms :338-356 with multiscat.py:133-145,
+ * transforms :358-372; called by chimera/calibrate.py:364-371, 473-478).
+ * One row of `params` per member, FP64, laid out as
+ *   [a0, sigma_scale, ms_amp, ms_c, kmin, kmax, dE0[nsp],
+ *    sigma_shell_scale[nshell], dr[nsp*nsp], c3[nshell], c4[nshell],
+ *    sigma_pair[nsp*nsp], ms_amp_edge[nsp]]
+ * (chx_shell_nparam values). Per member: the basis B[a,b,s](k) at its
+ * parameters contracted with the pair counts N, plus the averaged MS term;
+ * each channel (edge e, k weight w; edge-major) resampled from the member's
+ * k axis sqrt(k^2 - etok dE0[e]) onto n dk, times the Hanning window of its
+ * kmin, kmax (taper dk_win) and k^w, and transformed (e^{-2ikR}, dk/sqrt(pi))
+ * on the fitted FFT bins; one amplitude per edge profiled out and the
+ * R-factor over all channels (model.py:497-545).
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    int nsp, nshell, nk, nkw, nbin, nfft;
+    int magnitude;                   /* 1: fit |chi(R)| to real data          */
+    double a0_ref, s02, dk_win, dk, etok;
+    const double *k;                 /* (nk) model k grid (k_phys)            */
+    const double *f, *delta, *lam;   /* (nsp, nk), (nsp*nsp, nk), (nk)        */
+    const double *shells_ref;        /* (nshell) shell radii at a0_ref        */
+    const double *sigma2_ref;        /* (nshell) reference sigma^2 per shell  */
+    const double *shell_mult;        /* (nshell) coordination per shell       */
+    const double *N;                 /* (nsp, nsp, nshell) ordered pair counts */
+    const int *kweight;              /* (nkw)                                  */
+    const int *bins;                 /* (nbin) FFT bins of the fitted points   */
+    const double *data;              /* (nsp*nkw, nbin, 2) re, im (im unused
+                                        for magnitude data)                   */
+    /* averaged multiple scattering, npath == 0 when off */
+    int npath;
+    double ms_dnn;                   /* nearest-neighbour distance of the paths */
+    const int *ms_abs;               /* (npath) absorber species of each path  */
+    const double *ms_reff, *ms_deg;  /* (npath)                               */
+    const double *ms_F, *ms_D, *ms_L; /* (npath, nk)                          */
+} chx_shell_t;
+
+CHX_API int chx_shell_nparam(int nsp, int nshell);
+/* rf (P), scales (P, nsp) per-edge amplitudes; a member whose k axis or
+ * window leaves the built tap range gets rf = NaN. */
+CHX_API int chx_shell_rfactor(const chx_shell_t *S, const double *params, int P, double *rf,
+                              double *scales, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
