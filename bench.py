@@ -525,6 +525,100 @@ def bench_uneven(args):
     return 0
 
 
+def bench_calib(args):
+    """The calibration objective (chimera/calibrate.py's differential
+    evolution over the pair-count model): an fcc Fe-Ni 4x4x4 model to
+    6.2 A (5 shells), 241 k points, k^1/k^2/k^3 complex chi(R) data of an
+    ordered configuration (its path sum through the Hanning-window transform,
+    fitted over 1.4-5.0 A). Times (1) the population objective, members per
+    second, for the reference's stage-1 population (popsize 12 x 12
+    parameters = 144 members) and for 4,096 members, CUDA events; (2) the
+    reference's whole global stage (maxiter 120, popsize 12, tol 1e-8,
+    polished) with one launch per generation, wall clock; beside the CPU
+    restatement of the objective per member on one core."""
+    import time
+    import torch
+    from chimera_b200 import _native as N
+    from chimera_b200 import configs
+    from chimera_b200.calibrate import Stage1, de_stage1
+    from chimera_b200.fourier import FourierTransform
+    from chimera_b200.shellmodel import ShellModel
+    N.lib()
+    prob = configs.Problem(ncell=(4, 4, 4), rmax=6.2, ms=False, alpha1=-0.08)
+    top = prob.top
+    z = np.bincount(top.shell, minlength=top.nshell) / top.natoms
+    sm = ShellModel(prob.k, prob.tables, top.r_shell, z, top.s2_shell, top.natoms, 3.59,
+                    s02=0.85, pairs=(top.i, top.j, top.shell), composition=(0.5, 0.5),
+                    elements=("Fe", "Ni"))
+    kw = (1, 2, 3)
+    sm.set_params(kweight=kw)
+    chi = prob.target_chi()
+    fts = [FourierTransform(prob.k, 3.0, 13.0, w) for e in range(2) for w in kw]
+    bins = np.arange(200)
+    data = np.array([f.to_R(chi[e], bins=bins) for f, e in zip(fts, (0, 0, 0, 1, 1, 1))])
+    R = fts[0].R[:200]
+    mask = (R > 1.4) & (R < 5.0)
+    Nc = sm.counts_of(prob.target_species)
+    st = Stage1(sm, (0.5, 0.5), ms=False, elements=("Fe", "Ni"))
+    rng = np.random.default_rng(0)
+    lo, hi = np.array(st.bounds).T
+
+    def pop(n):
+        return st.rows(lo + (hi - lo) * rng.uniform(size=(n, lo.size)), a0=3.59)
+
+    s = torch.cuda.current_stream()
+    out = {}
+    for P in (12 * len(st.names), 4096):
+        X = pop(P)
+        for _ in range(3):
+            sm.r_factor_batch(Nc, data, mask, bins, X)
+        reps = 10
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record(s)
+        for _ in range(reps):
+            sm.r_factor_batch(Nc, data, mask, bins, X)
+        b.record(s)
+        b.synchronize()
+        wall = (time.perf_counter() - t0) / reps
+        out[P] = dict(members_per_s_device_span=P * reps / (a.elapsed_time(b) * 1e-3),
+                      members_per_s_with_host=P / wall)
+    # the whole global stage, wall clock
+    t0 = time.perf_counter()
+    gens = 120 if args.steps == 1200 else max(1, min(args.steps, 120))   # small profiling case
+    res, nev = de_stage1(sm, Nc, data, mask, bins, st, a0=3.59, maxiter=gens, popsize=12,
+                         seed=0, tol=1e-8, polish=gens == 120)
+    t_de = time.perf_counter() - t0
+    # CPU: the restatement of the objective, one member at a time
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import shellmodel as OS
+        m = dict(k=sm.k, f=sm.f, delta=sm.delta, lam=sm.lam, shells_ref=sm.shells_ref,
+                 shell_mult=sm.z, sigma2_ref=sm.sigma2_shell_ref, a0_ref=sm.a0_ref,
+                 s02=sm.s02, dk_win=sm.dk_win, etok=sm.etok)
+        X = pop(40)
+        t0 = time.perf_counter()
+        for x in X:
+            OS.r_factor(x, Nc, m, data[:, mask], bins[mask], kw)
+        cpu = 40 / (time.perf_counter() - t0)
+    line = {"metric": "calibration objective: pair-count R-factor per parameter set",
+            "kernel": "calibration population (chx_shell_rfactor)", "unit": "members/s",
+            "config": {"workload": "fcc Fe50Ni50 pair-count model, 4x4x4 cells, SS to 6.2 A "
+                                   "(5 shells), 241 k, k^1/k^2/k^3 complex chi(R), Hanning "
+                                   "window 3-13 A^-1, fitted 1.4-5.0 A",
+                       "parameters": len(st.names), "fitted_bins": int(mask.sum())},
+            "population": {str(k): v for k, v in out.items()},
+            "de_stage1": {"wall_s": t_de, "members_evaluated": nev, "generations": int(res.nit),
+                          "r_factor": float(res.fun),
+                          "cpu_estimate_s": (nev / cpu) if cpu else None},
+            "cpu_baseline": None if cpu is None else {
+                "value": cpu, "unit": "members/s", "cores": 1, "kind": "port",
+                "sample": "CPU restatement of the objective, 40 members one at a time"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global NPOS
     ap = argparse.ArgumentParser()
@@ -537,7 +631,8 @@ def main():
     ap.add_argument("--positions", type=int, default=16,
                     help="ladders per GPU (fewer for a small profiling case)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--kernel", default="sampler", choices=["sampler", "ft", "da", "uneven"],
+    ap.add_argument("--kernel", default="sampler",
+                    choices=["sampler", "ft", "da", "uneven", "calib"],
                     help="ft: time the windowed FT contraction (chx_ft_batch); da: GPU-s of "
                          "the learned (delayed-acceptance) sampler to the plain sampler's "
                          "R-factor on the ternary configuration")
@@ -551,6 +646,8 @@ def main():
         return bench_da(args)
     if args.kernel == "uneven":
         return bench_uneven(args)
+    if args.kernel == "calib":
+        return bench_calib(args)
 
     import torch
     import torch.distributed as dist
