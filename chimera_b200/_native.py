@@ -87,7 +87,8 @@ class Shell(C.Structure):
                 ("sigma2_ref", c_p), ("shell_mult", c_p), ("N", c_p), ("kweight", c_p),
                 ("bins", c_p), ("data", c_p),
                 ("npath", c_i), ("ms_dnn", c_d), ("ms_abs", c_p), ("ms_reff", c_p),
-                ("ms_deg", c_p), ("ms_F", c_p), ("ms_D", c_p), ("ms_L", c_p)]
+                ("ms_deg", c_p), ("ms_F", c_p), ("ms_D", c_p), ("ms_L", c_p),
+                ("N_member", c_p), ("resid", c_p), ("sigma", c_p), ("profile", c_i)]
 
 
 # argument types of every entry point, in header order

@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(kShellThreads) k_shell_rfactor(chx_shell_t S, 
     const double *dE0 = par + 6, *sss = dE0 + nsp, *dr = sss + nshell, *c3 = dr + nn,
                  *c4 = c3 + nshell, *spair = c4 + nshell, *ms_edge = spair + nn;
     const double rscale = a0 / S.a0_ref;
+    const double *Nm = S.N_member ? S.N_member + (long)m * nsp * nsp * nshell : S.N;
     if (tid == 0) {
         double zsum = 0.0;
         for (int s = 0; s < nshell; ++s) zsum += S.shell_mult[s];
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(kShellThreads) k_shell_rfactor(chx_shell_t S, 
             const double amp4 = (2.0 / 3.0) * k4 * c4[s];
             const double ph3 = (4.0 / 3.0) * k3 * c3[s];
             for (int b = 0; b < nsp; ++b) {
-                const double Nab = S.N[(a * nsp + b) * nshell + s];
+                const double Nab = Nm[(a * nsp + b) * nshell + s];
                 cnt += Nab;
                 if (Nab == 0.0) continue;
                 const double r = rs + (s == 0 ? dr[a * nsp + b] : 0.0);
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(kShellThreads) k_shell_rfactor(chx_shell_t S, 
                 nu += num[e * S.nkw + q];
                 de += den[e * S.nkw + q];
             }
-            s_scale[e] = nu / fmax(de, 1e-30);
+            s_scale[e] = S.profile ? nu / fmax(de, 1e-30) : 1.0;
         }
     }
     __syncthreads();
@@ -253,6 +254,12 @@ __global__ void __launch_bounds__(kShellThreads) k_shell_rfactor(chx_shell_t S, 
             const double di_ = S.magnitude ? 0.0 : S.data[((long)c * S.nbin + q) * 2 + 1];
             const double er = sc * x.x - dr_, ei = sc * x.y - di_;
             r_ += er * er + ei * ei;
+            if (S.resid) {
+                const double sg = S.sigma ? S.sigma[(long)c * S.nbin + q] : 1.0;
+                double *o = S.resid + (((long)m * pl.nchan + c) * S.nbin + q) * 2;
+                o[0] = er / sg;
+                o[1] = ei / sg;
+            }
         }
         r_ = warp_sum(r_);
         if (lane == 0) res[c] = r_;
@@ -289,7 +296,7 @@ int chx_shell_rfactor(const chx_shell_t *S, const double *params, int P, double 
                 "shell_rfactor: sizes outside the built limits (nsp %d, nkw %d, nbin %d, nfft %d)",
                 S->nsp, S->nkw, S->nbin, S->nfft);
     CHX_REQUIRE(S->k && S->f && S->delta && S->lam && S->shells_ref && S->sigma2_ref &&
-                    S->shell_mult && S->N && S->kweight && S->bins && S->data,
+                    S->shell_mult && (S->N || S->N_member) && S->kweight && S->bins && S->data,
                 "shell_rfactor: a model array is NULL");
     CHX_REQUIRE(S->npath == 0 || (S->ms_abs && S->ms_reff && S->ms_deg && S->ms_F && S->ms_D &&
                                   S->ms_L && S->ms_dnn > 0.0),

@@ -212,6 +212,23 @@ class ShellModel:
         Nc for every row of X (P, nparam) against `data` (nchan, nR) on the
         model R grid points idx, fitted over mask. magnitude: fit |chi(R)|
         (default: when data is real)."""
+        rf, sc, _ = self._launch(Nc, data, mask, idx, X, kweight, magnitude)
+        return rf, sc
+
+    def residual_batch(self, Nc, data, mask, idx, X, sigma=None, profile=True, kweight=None,
+                       magnitude=None):
+        """Residuals (scale m - data) / sigma on the fitted points of every
+        member, ordered as chimera/shellmodel.py:504-508 orders them (channel-
+        major; the real parts, then the imaginary parts for complex data).
+        Nc is one (nsp, nsp, nshell) array or one per member (P, ...)."""
+        rf, sc, r = self._launch(Nc, data, mask, idx, X, kweight, magnitude, resid=True,
+                                 sigma=sigma, profile=profile)
+        cplx = np.iscomplexobj(data) if magnitude is None else not magnitude
+        re, im = r[..., 0].reshape(len(r), -1), r[..., 1].reshape(len(r), -1)
+        return np.concatenate([re, im], axis=1) if cplx else re
+
+    def _launch(self, Nc, data, mask, idx, X, kweight=None, magnitude=None, resid=False,
+                sigma=None, profile=True):
         import torch
         d = self._fixed()
         kw = as_kweights(self.p["kweight"] if kweight is None else kweight)
@@ -222,19 +239,22 @@ class ShellModel:
         dm = data[:, mask]
         dd = np.stack([dm.real, dm.imag if np.iscomplexobj(dm) else np.zeros_like(dm.real)],
                       axis=-1).astype(np.float64)
-        assert dd.shape[0] == self.nsp * len(kw), "data must have one row per (edge, k weight)"
+        nchan = self.nsp * len(kw)
+        assert dd.shape[0] == nchan, "data must have one row per (edge, k weight)"
         X = np.ascontiguousarray(np.atleast_2d(X), np.float64)
         assert X.shape[1] == self.nparam, f"need {self.nparam} parameters per row"
         P = X.shape[0]
-        t = dict(N=N.to_dev(np.ascontiguousarray(Nc, np.float64)),
-                 kw=N.to_dev(np.array(kw, np.int32)), bins=N.to_dev(bins),
+        Nc = np.ascontiguousarray(Nc, np.float64)
+        per_member = Nc.ndim == 4
+        assert not per_member or Nc.shape[0] == P, "one pair-count array per member"
+        t = dict(N=N.to_dev(Nc), kw=N.to_dev(np.array(kw, np.int32)), bins=N.to_dev(bins),
                  data=N.to_dev(np.ascontiguousarray(dd)), X=N.to_dev(X))
         rf = torch.empty(P, dtype=torch.float64, device="cuda")
         sc = torch.empty((P, self.nsp), dtype=torch.float64, device="cuda")
         S = N.Shell()
         S.nsp, S.nshell, S.nk, S.nkw, S.nbin, S.nfft = (self.nsp, self.nshell, self.k.size,
                                                         len(kw), bins.size, self.nfft)
-        S.magnitude = int(mag)
+        S.magnitude, S.profile = int(mag), int(bool(profile))
         S.a0_ref, S.s02, S.dk_win, S.dk, S.etok = (self.a0_ref, self.s02, self.dk_win, self.dk,
                                                    self.etok)
         S.k, S.f, S.delta, S.lam = (N.dptr(d["k"]), N.dptr(d["f"]), N.dptr(d["delta"]),
@@ -242,8 +262,24 @@ class ShellModel:
         S.shells_ref, S.sigma2_ref, S.shell_mult = (N.dptr(d["shells_ref"]),
                                                     N.dptr(d["sigma2_ref"]),
                                                     N.dptr(d["shell_mult"]))
-        S.N, S.kweight, S.bins, S.data = (N.dptr(t["N"]), N.dptr(t["kw"]), N.dptr(t["bins"]),
-                                          N.dptr(t["data"]))
+        if per_member:
+            S.N_member = N.dptr(t["N"])
+        else:
+            S.N = N.dptr(t["N"])
+        S.kweight, S.bins, S.data = N.dptr(t["kw"]), N.dptr(t["bins"]), N.dptr(t["data"])
+        r = None
+        if resid:
+            r = torch.empty((P, nchan, bins.size, 2), dtype=torch.float64, device="cuda")
+            S.resid = N.dptr(r)
+            if sigma is not None:
+                sg = np.asarray(sigma, float)
+                if sg.ndim == 0:
+                    sg = np.full((nchan, data.shape[1]), float(sg))
+                elif sg.ndim == 1:                      # per channel (shellmodel.py:496-498)
+                    sg = np.repeat(sg[:, None], data.shape[1], axis=1)
+                sg = sg[:, mask]
+                t["sigma"] = N.to_dev(np.ascontiguousarray(sg))
+                S.sigma = N.dptr(t["sigma"])
         if self.ms is not None:
             S.npath, S.ms_dnn = int(self.ms["reff"].size), float(self.ms["dnn"])
             S.ms_abs, S.ms_reff, S.ms_deg = (N.dptr(d["ms_abs"]), N.dptr(d["ms_reff"]),
@@ -251,10 +287,145 @@ class ShellModel:
             S.ms_F, S.ms_D, S.ms_L = N.dptr(d["ms_F"]), N.dptr(d["ms_D"]), N.dptr(d["ms_L"])
         N.call("chx_shell_rfactor", C.byref(S), N.ptr(t["X"]), P, N.ptr(rf), N.ptr(sc),
                N.stream())
-        return rf.cpu().numpy(), sc.cpu().numpy()
+        return rf.cpu().numpy(), sc.cpu().numpy(), (None if r is None else r.cpu().numpy())
 
     def r_factor(self, Nc, data, mask, idx, return_scales=False):
         """The reference's r_factor (shellmodel.py:427-440) at the current
         parameters, on the device."""
         rf, sc = self.r_factor_batch(Nc, data, mask, idx, self.flat()[None])
         return (float(rf[0]), sc[0]) if return_scales else float(rf[0])
+
+
+# ================================================================ Fisher bounds
+# Prior widths, nuisance list and finite-difference steps of the reference's
+# bound (chimera/shellmodel.py:444-446, 491-493), kept identical so that the
+# bounds are the same numbers.
+PRIOR_SD = dict(alpha=1.0, a0=0.02, sigma_scale=0.5, ms_amp=0.5, ms_c=0.5, c3=2e-4,
+                dE0=5.0, dr=0.05)
+NUISANCE_DEFAULT = ("a0", "sigma_scale", "ms_amp", "dE0", "dr", "c3")
+STEPS = dict(a0=0.002, sigma_scale=0.05, ms_amp=0.05, ms_c=0.05, c3=2e-5, dE0=0.5, dr=0.005)
+
+
+def sro_directions(nsp):
+    """Independent short-range-order directions per shell: (a, b), a < b."""
+    return [(a, b) for a in range(nsp) for b in range(a + 1, nsp)]
+
+
+def dN_direction(nsp, nshell, s, a, b):
+    """+1 on (a,b) and (b,a), -1 on (a,a) and (b,b) in shell s: a change of
+    the pair counts that keeps every absorber's coordination."""
+    d = np.zeros((nsp, nsp, nshell))
+    d[a, b, s] += 1.0
+    d[b, a, s] += 1.0
+    d[a, a, s] -= 1.0
+    d[b, b, s] -= 1.0
+    return d
+
+
+def crlb(model: ShellModel, Nc, data, sigma, mask, idx, shells=None, alpha_shell=0,
+         nuisance=NUISANCE_DEFAULT, profile_scale=True, threshold=0.3, steps=None,
+         prior_sd=None, whiten=None):
+    """Cramer-Rao bounds on the shell-`alpha_shell` Warren-Cowley parameters
+    (chimera/shellmodel.py:449-593): the Jacobian of the sigma-scaled
+    residual along the SRO directions of every shell in `shells` and the
+    nuisance parameters by central differences, all 2 x ncolumn perturbed
+    models in one chx_shell_rfactor launch, then the FP64 Fisher matrix with
+    a weak Gaussian prior, its inverse and the marginal widths on the host.
+    Returns the reference's dictionary."""
+    from .calibrate import dr_from_free
+    nsp, nshell = model.nsp, model.nshell
+    shells = list(range(nshell)) if shells is None else list(shells)
+    Nc = np.asarray(Nc, float)
+    cnt = model.absorber_counts(Nc)
+    c = cnt / cnt.sum()
+    iu = np.triu_indices(nsp)
+    st = dict(STEPS)
+    if steps:
+        st.update(steps)
+    pr = dict(PRIOR_SD)
+    if prior_sd:
+        pr.update(prior_sd)
+    Ns, dicts, step_of, A, names, prec = [], [], [], [], [], []
+    for s in shells:
+        h = 0.02 * cnt.min() * model.z[s] * c.min()
+        for a, b in sro_directions(nsp):
+            d = dN_direction(nsp, nshell, s, a, b)
+            Ns += [Nc + h * d, Nc - h * d]
+            dicts += [{}, {}]
+            step_of.append(h)
+            names.append(f"sro_s{s + 1}_{a}{b}")
+            dalpha = (model.alpha(Nc + h * d, s) - model.alpha(Nc, s)) / h
+            A.append(dalpha[iu] if s == alpha_shell else np.zeros(len(iu[0])))
+            prec.append((np.abs(dalpha).max() / pr["alpha"]) ** 2)
+    nsro = len(names)
+    saved = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in model.p.items()}
+
+    def column(name, hi_, lo_, step):
+        Ns.extend([Nc, Nc])
+        dicts.extend([{name: hi_}, {name: lo_}])
+        step_of.append(step)
+        prec.append(1.0 / pr[name] ** 2)
+
+    ndr_free = nsp * (nsp + 1) // 2 - 1
+    for name in nuisance or ():
+        v0 = saved[name]
+        if name == "a0":
+            column(name, v0 + st[name], v0 - st[name], st[name])
+            names.append(name)
+        elif name == "c3":
+            hi_ = v0.copy()
+            hi_[0] += st[name]
+            lo_ = v0.copy()
+            lo_[0] -= st[name]
+            column(name, hi_, lo_, st[name])
+            names.append(name)
+        elif name == "dE0":
+            for e in range(nsp):
+                hi_ = v0.copy()
+                hi_[e] += st[name]
+                lo_ = v0.copy()
+                lo_[e] -= st[name]
+                column(name, hi_, lo_, st[name])
+                names.append(f"dE0_{e}")
+        elif name == "dr":
+            for q in range(ndr_free):
+                e_ = np.zeros(ndr_free)
+                e_[q] = st[name]
+                d = dr_from_free(e_, c)
+                column(name, v0 + d, v0 - d, st[name])
+                names.append(f"dr_{q}")
+        else:
+            column(name, v0 * np.exp(st[name]), v0 * np.exp(-st[name]), st[name])
+            names.append(name)
+    X = model.flat_rows(dicts)
+    R = model.residual_batch(np.array(Ns), data, mask, idx, X, sigma=sigma,
+                             profile=profile_scale)
+    if whiten is not None:
+        R = np.array([whiten(r) for r in R])
+    J = ((R[0::2] - R[1::2]) / (2.0 * np.asarray(step_of))[:, None]).T
+    F = J.T @ J
+    cov = np.linalg.inv(F + np.diag(prec))
+    A = np.array(A)
+    cov_alpha = A.T @ cov[:nsro, :nsro] @ A
+    sd = np.sqrt(np.maximum(np.diag(cov_alpha), 0.0))
+    ev = np.linalg.eigvalsh(F[:nsro, :nsro])[::-1]
+    with np.errstate(divide="ignore"):
+        eig_sd = 1.0 / np.sqrt(np.maximum(ev, 1e-300))
+    csd = np.sqrt(np.maximum(np.diag(cov), 0.0))
+    nuis_sd = {}
+    for j, name in enumerate(names[nsro:], start=nsro):
+        key = name.split("_")[0] if name.startswith(("dE0_", "dr_")) else name
+        nuis_sd.setdefault(key, []).append(float(csd[j]))
+    dr_entry_sd = None
+    if "dr" in nuis_sd:
+        q = [j for j, n in enumerate(names) if n.startswith("dr_")]
+        D = np.array([dr_from_free(np.eye(ndr_free)[i], c)[iu] for i in range(ndr_free)])
+        dr_entry_sd = np.sqrt(np.maximum(np.einsum("ie,ij,je->e", D, cov[np.ix_(q, q)], D),
+                                         0.0)).tolist()
+    return dict(alpha_sd=sd.tolist(), determined=(sd < threshold).tolist(),
+                threshold=threshold, prior_alpha_sd=pr["alpha"],
+                shells=[int(s) + 1 for s in shells], nuisance=list(nuisance or ()),
+                n_sro_directions=int(nsro), eig_sd=eig_sd.tolist(), columns=names,
+                alpha_cov=cov_alpha.tolist(),
+                nuisance_sd={k: (v[0] if len(v) == 1 else v) for k, v in nuis_sd.items()},
+                dr_entry_sd=dr_entry_sd, n_models=len(Ns))

@@ -455,6 +455,15 @@ typedef struct {
     const int *ms_abs;               /* (npath) absorber species of each path  */
     const double *ms_reff, *ms_deg;  /* (npath)                               */
     const double *ms_F, *ms_D, *ms_L; /* (npath, nk)                          */
+    /* Fisher-bound extensions (chimera/shellmodel.py:449-593): per-member
+       pair counts (P, nsp, nsp, nshell) in place of N, or NULL; the residual
+       (scale m - data) / sigma of every member (P, nchan, nbin, 2: re, im)
+       written to resid when not NULL, sigma (nchan, nbin) or NULL for 1;
+       profile 0 holds the amplitudes at 1 */
+    const double *N_member;
+    double *resid;
+    const double *sigma;
+    int profile;
 } chx_shell_t;
 
 CHX_API int chx_shell_nparam(int nsp, int nshell);

@@ -13,8 +13,10 @@ parameter sets spanning the calibration's search ranges
 (chimera/calibrate.py:129-193), against complex chi(R) data and against
 |chi(R)| data made by the same model at a reference parameter set plus
 seeded noise. It saves the model inputs, the data, every parameter set in
-the flat layout of chimera_b200.shellmodel, and the reference's R-factors and
-per-edge amplitudes (shellmodel.npz).
+the flat layout of chimera_b200.shellmodel, the reference's R-factors and
+per-edge amplitudes, its global-stage search vector (calibrate.Stage1) and
+its Cramer-Rao bounds (shellmodel.crlb, :449-593) at the data's parameters
+(shellmodel.npz).
 """
 from __future__ import annotations
 
@@ -105,6 +107,21 @@ def main():
         sm.set_params(kweight=kw, **q)
         stage_rows.append(flat(sm.p, nsp, nshell))
     sm.p = base
+    # Cramer-Rao bounds (shellmodel.py:449-593) at the data's parameters
+    sm.set_params(**true)
+    crlb_base = flat(sm.p, nsp, nshell)
+    sig = np.full(nsp * len(kw), 2e-4)
+    cr = {}
+    for tag, dat in (("c", data_c), ("m", data_m)):
+        r = SM.crlb(sm, N1, dat, sig, mask, idx)
+        ns = r["nuisance_sd"]
+        cr[f"crlb_{tag}_alpha_sd"] = np.array(r["alpha_sd"])
+        cr[f"crlb_{tag}_eig_sd"] = np.array(r["eig_sd"])
+        cr[f"crlb_{tag}_alpha_cov"] = np.array(r["alpha_cov"])
+        cr[f"crlb_{tag}_nuis"] = np.concatenate([np.atleast_1d(ns[k]) for k in
+                                                 ("a0", "sigma_scale", "ms_amp", "dE0", "dr",
+                                                  "c3")])
+        cr[f"crlb_{tag}_dr_entry_sd"] = np.array(r["dr_entry_sd"])
     _, f, delta, lam = S.tables.as_float64()
     out = dict(k=np.asarray(sm.k, float), f=f, delta=delta.reshape(nsp * nsp, -1), lam=lam,
                shells_ref=sm.shells_ref, shell_mult=sm.z, sigma2_shell_ref=sm.sigma2_shell_ref,
@@ -117,7 +134,7 @@ def main():
                stage_names=np.array(stage.names), stage_bounds=np.array(stage.bounds),
                stage_x0=stage.x0(), stage_dE0_start=np.float64(stage.dE0_start),
                stage_X=X, stage_rows=np.array(stage_rows),
-               stage_base=flat(base, nsp, nshell))
+               stage_base=flat(base, nsp, nshell), crlb_base=crlb_base, crlb_sigma=sig, **cr)
     np.savez_compressed(os.path.join(HERE, "shellmodel.npz"), **out)
     print("wrote shellmodel.npz:", {k: np.shape(v) for k, v in out.items()})
     print("R-factors (complex):", np.round(out["rf_c"], 4))

@@ -124,3 +124,29 @@ def test_differential_evolution_stage1(cuda):
     r, _ = OS.r_factor(row, g["N1"], oracle_model(g), g["data_c"][:, mask], g["idx"][mask],
                        g["kweight"])
     assert abs(res.fun - r) <= 1e-9 * r
+
+
+@pytest.mark.parametrize("tag", ["c", "m"])
+def test_crlb_matches_reference(cuda, tag):
+    """Cramer-Rao bounds with the default nuisances (a0, sigma^2 scale, MS
+    amplitude, dE0 per edge, the free bond offsets, C3): every perturbed
+    model of the finite-difference Jacobian (26 here) in one launch, then the
+    FP64 Fisher matrix with the prior on the host. alpha widths, the SRO
+    eigen-widths, the alpha covariance and the nuisance widths equal the
+    reference's crlb to 1e-6 relative, complex and |chi(R)| data."""
+    from chimera_b200.shellmodel import crlb
+    g = golden("shellmodel.npz")
+    sm = device_model(g)
+    sm.set_flat(g["crlb_base"])
+    data = g["data_c"] if tag == "c" else g["data_m"]
+    r = crlb(sm, g["N1"], data, g["crlb_sigma"], g["mask"], g["idx"])
+    assert r["n_models"] == 2 * (5 + 8)
+    ns = r["nuisance_sd"]
+    nuis = np.concatenate([np.atleast_1d(ns[k]) for k in
+                           ("a0", "sigma_scale", "ms_amp", "dE0", "dr", "c3")])
+    for got, key in ((r["alpha_sd"], "alpha_sd"), (r["eig_sd"], "eig_sd"),
+                     (r["alpha_cov"], "alpha_cov"), (nuis, "nuis"),
+                     (r["dr_entry_sd"], "dr_entry_sd")):
+        ref = g[f"crlb_{tag}_{key}"]
+        assert np.allclose(np.asarray(got), ref, rtol=1e-6, atol=0), (key, got, ref)
+    assert np.array_equal(sm.flat(), g["crlb_base"])       # the model is left as it was
