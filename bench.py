@@ -619,6 +619,70 @@ def bench_calib(args):
     return 0
 
 
+def bench_band(args):
+    """The systematic band (chimera/fitrun.py:652-718): the reference's 18
+    calibration variants of the 4,000-site fcc Fe-Ni workload (exact MS,
+    k^1/k^2/k^3 Kaiser complex chi(R)), 48 rungs each (its nrep), 6,000 steps
+    (240 exchange periods, its nsteps) of every variant as ONE batched sampler,
+    against the same variants run one after the other (the reference's loop).
+    Device time by CUDA events; swap attempts/s of both; the band of the
+    batched run."""
+    import torch
+    from chimera_b200 import _native as N
+    from chimera_b200 import band as B
+    from chimera_b200.sampler import BatchedSampler
+    N.lib()
+    nb = 240 if args.steps == 1200 else max(4, min(args.steps, 240))
+    base, vs = B.build_variants(dict(ncell=(10, 10, 10)))
+    specs, meta = B.variant_specs(base, vs, positions=(0,), nrep=48)
+    starts = [v.prob.random_config(100 + i) for i, (v, _) in enumerate(meta)]
+    ideal = [v.prob.cell.ideal for v, _ in meta]
+    s = torch.cuda.current_stream()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        fn()
+        b.record(s)
+        b.synchronize()
+        return a.elapsed_time(b) * 1e-3
+
+    bs = BatchedSampler(specs, precision=1, exchange_every=EXCH, reanchor_every=1000,
+                        threads=256, min_blocks=4)
+    bs.init_state(starts, ideal)
+    bs.capture()
+    t_batch = timed(lambda: bs.run_blocks(nb))
+    common = vs[0].ft_data.window_mask(*vs[0].rwin)
+    rows = [B.variant_result(bs, li, v, specs[li], common) for li, (v, _) in enumerate(meta)]
+    band = B.band_from_variants(rows)
+    t_seq = 0.0
+    for li in range(len(specs)):
+        one = BatchedSampler([specs[li]], precision=1, exchange_every=EXCH,
+                             reanchor_every=1000, threads=256, min_blocks=4)
+        one.init_state([starts[li]], [ideal[li]])
+        one.capture()
+        t_seq += timed(lambda: one.run_blocks(nb))
+        del one
+    att = bs.nslots * EXCH * nb
+    line = {"metric": METRIC, "kernel": "systematic band (18 calibration variants)",
+            "unit": UNIT,
+            "config": {"workload": "fcc Fe50Ni50 4000 atoms, SS 5.0 A + exact MS 5.5 A, "
+                                   "k^1/k^2/k^3 Kaiser complex chi(R) 1.4-5.0 A; the 18 "
+                                   "calibration variants (a0, dE0, sigma^2, k weight, k and R "
+                                   "window, MS amplitude, dr, C3)",
+                       "variants": len(vs), "rungs": 48, "replicas": bs.nslots,
+                       "steps": nb * EXCH},
+            "batched": {"attempts_per_s": att / t_batch, "gpu_s": t_batch},
+            "one_variant_per_launch": {"attempts_per_s": att / t_seq, "gpu_s": t_seq},
+            "speedup": t_seq / t_batch,
+            "band": {k: band[k] for k in ("wc_min", "wc_max", "n_admissible", "n_comparable",
+                                          "excluded_incomparable", "r_factor_baseline",
+                                          "r_factor_range")},
+            "device_error": bs.device_error()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global NPOS
     ap = argparse.ArgumentParser()
@@ -632,7 +696,7 @@ def main():
                     help="ladders per GPU (fewer for a small profiling case)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--kernel", default="sampler",
-                    choices=["sampler", "ft", "da", "uneven", "calib"],
+                    choices=["sampler", "ft", "da", "uneven", "calib", "band"],
                     help="ft: time the windowed FT contraction (chx_ft_batch); da: GPU-s of "
                          "the learned (delayed-acceptance) sampler to the plain sampler's "
                          "R-factor on the ternary configuration")
@@ -648,6 +712,8 @@ def main():
         return bench_uneven(args)
     if args.kernel == "calib":
         return bench_calib(args)
+    if args.kernel == "band":
+        return bench_band(args)
 
     import torch
     import torch.distributed as dist
