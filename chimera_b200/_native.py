@@ -91,6 +91,14 @@ class Shell(C.Structure):
                 ("N_member", c_p), ("resid", c_p), ("sigma", c_p), ("profile", c_i)]
 
 
+class PathSet(C.Structure):
+    """chx_path_t"""
+    _fields_ = [("npath", c_i), ("maxs", c_i), ("ne", c_i), ("ntype", c_i), ("nlt", c_i),
+                ("glmax", c_i), ("nsc", c_p), ("typ", c_p), ("leg", c_p), ("eul", c_p),
+                ("p", c_p), ("t", c_p), ("lmax", c_p), ("goff", c_p), ("gcnt", c_p),
+                ("glpp", c_p), ("gA", c_p), ("doff", c_p), ("dflat", c_p)]
+
+
 # argument types of every entry point, in header order
 _SIGS = {
     "chx_version": ([], c_i),
@@ -129,6 +137,7 @@ _SIGS = {
                      c_i),
     "chx_shell_nparam": ([c_i, c_i], c_i),
     "chx_shell_rfactor": ([c_p, c_p, c_i, c_p, c_p, c_p], c_i),
+    "chx_path_trace": ([c_p, c_p, c_p], c_i),
 }
 
 # entry points declared in include/chimera_b200.h (checked by the tests)
@@ -157,9 +166,9 @@ def lib():
 
 
 def _check_abi(L):
-    got = tuple(L.chx_struct_size(q) for q in range(7))
+    got = tuple(L.chx_struct_size(q) for q in range(8))
     want = (C.sizeof(Pairs), C.sizeof(Ladder), Ladder.exch_acc.offset, Ladder.seed.offset,
-            C.sizeof(Mlp), Ladder.log_cap.offset, C.sizeof(Shell))
+            C.sizeof(Mlp), Ladder.log_cap.offset, C.sizeof(Shell), C.sizeof(PathSet))
     if got != want:
         raise ChxError(f"ABI mismatch between chimera_b200.h and the binding: {got} != {want}")
 

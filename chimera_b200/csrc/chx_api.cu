@@ -270,6 +270,7 @@ int64_t chx_struct_size(int which) {
         case 4: return (int64_t)sizeof(chx_mlp_t);
         case 5: return (int64_t)offsetof(chx_ladder_t, log_cap);
         case 6: return (int64_t)sizeof(chx_shell_t);
+        case 7: return (int64_t)sizeof(chx_path_t);
         default: return -1;
     }
 }

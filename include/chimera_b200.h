@@ -472,6 +472,37 @@ CHX_API int chx_shell_nparam(int nsp, int nshell);
 CHX_API int chx_shell_rfactor(const chx_shell_t *S, const double *params, int P, double *rf,
                               double *scales, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Curved-wave multiple-scattering path trace (K edge, orientation averaged)
+ *
+ * Replaces the reference's path_trace kernel and its host driver
+ * (exafs_gpu/abinitio/pathsum.py:158-343, CPU twin trace_numpy :106-126,
+ * called by path_sum / provider.py:173-225): Tr_{l=1} of every path's
+ * product G(a_N) t_N D_N ... t_1 D_1 G(a_0) and the closing rotation, one
+ * CTA per (energy, path), FP64 complex. Complex values are (re, im) pairs.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    int npath, maxs, ne, ntype, nlt, glmax;  /* glmax: the tables' lmax (<= 40)  */
+    const int *nsc;                  /* (npath) scatterers per path              */
+    const int *typ;                  /* (npath, maxs) scatterer types            */
+    const double *leg;               /* (npath, maxs+1) leg lengths (bohr)       */
+    const double *eul;               /* (npath, maxs+1, 3) zyz Euler angles of the
+                                        frame changes, the closing one last      */
+    const double *p;                 /* (ne, 2) complex momentum (bohr^-1)       */
+    const double *t;                 /* (ntype, ne, nlt, 2) t_l = (S_l - 1)/2     */
+    const int *lmax;                 /* (npath, ne) angular momentum cut, <= glmax */
+    const int *goff, *gcnt;          /* ((glmax+1)^3) runs of the propagator
+                                        coefficients A^m_{l'l l''}, [|m|][l'][l] */
+    const int *glpp;                 /* l'' of every run entry                   */
+    const double *gA;                /* (nruns, 2) A of every run entry          */
+    const int64_t *doff;             /* (glmax+2) offsets of Delta^l = d^l(pi/2) */
+    const double *dflat;             /* Delta^l[m''+l][m+l] blocks               */
+} chx_path_t;
+
+/* out (npath, ne, 2): the trace of every path at every energy (NaN for a path
+ * whose sizes or types are out of range). */
+CHX_API int chx_path_trace(const chx_path_t *P, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
