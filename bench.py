@@ -683,6 +683,87 @@ def bench_band(args):
     return 0
 
 
+def bench_pathtrace(args):
+    """The curved-wave path trace (exafs_gpu/abinitio/pathsum.py): every
+    3- and 4-leg path class of fcc to 5.5 A half length (25 classes) and the
+    first three single-scattering shells, Fe-Ni alternating along the path,
+    at 120 energies (k 2-18 A^-1) with smooth synthetic complex phase shifts
+    of two types; lmax per (path, energy) where |t_l| > 1e-6 (at most 40).
+    Traces per second of one chx_path_trace launch (CUDA events) and of the
+    whole call from host arrays; beside the CPU evaluation (oracle, dense
+    matrices) on a bounded sample."""
+    import time
+    import torch
+    from chimera_b200 import _native as N
+    from chimera_b200 import mspaths as MP
+    from chimera_b200 import pathtrace as PT
+    N.lib()
+    bohr = 0.529177210903
+    a0 = 3.59
+    unit = a0 / 2.0 / bohr
+    cls = MP.enumerate_classes(a0, 5.5, "fcc")
+    sites = [np.array([[1, 1, 0]]) * unit, np.array([[2, 0, 0]]) * unit,
+             np.array([[2, 1, 1]]) * unit]
+    for c in cls:
+        rep = np.asarray(c.rep, float) * unit
+        sites.append(rep)
+    # a 4-leg class may pass through the absorber (q2 = 0); the trace needs
+    # scatterers off the origin, so such classes are left out
+    sites = [s_ for s_ in sites if np.all(np.linalg.norm(s_, axis=1) > 1e-9)]
+    types = [tuple(q % 2 for q in range(len(s_))) for s_ in sites]
+    nE, nl = 120, 41
+    k = np.linspace(2.0, 18.0, nE)
+    kb = k * bohr
+    p = kb + 1j * (0.02 + 0.002 * kb)
+    l = np.arange(nl)
+    S = np.empty((2, nE, nl), complex)
+    for ty in range(2):
+        width = 0.75 * kb[:, None] * (2.3 + 0.3 * ty) + 1.0
+        d = (0.9 + 0.25 * ty) * np.exp(-(l[None, :] / width) ** 2)
+        S[ty] = np.exp(2j * (d + 0.02j * np.exp(-(l[None, :] / width) ** 2)))
+    t = 0.5 * (S - 1.0)
+    big = np.abs(t).max(0) > 1e-6
+    lm_e = np.array([max(2, int(np.nonzero(row)[0].max())) for row in big])
+    lmax = np.minimum(np.tile(lm_e, (len(sites), 1)), PT.MAX_L).astype(np.int32)
+    PT.path_trace(sites, types, p, t, lmax)                  # tables, attributes
+    s = torch.cuda.current_stream()
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        tr = PT.path_trace(sites, types, p, t, lmax)
+    wall = (time.perf_counter() - t0) / reps
+    # device time of the launch alone: re-run through the entry with CUDA events
+    a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a_.record(s)
+    PT.path_trace(sites, types, p, t, lmax)
+    b_.record(s)
+    b_.synchronize()
+    span = a_.elapsed_time(b_) * 1e-3
+    ntr = len(sites) * nE
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import pathtrace as OP
+        sample = [(q, e) for q in (0, 5, 12) for e in (10, 60)]
+        t0 = time.perf_counter()
+        for q, e in sample:
+            OP.trace(sites[q], types[q], p[e], t[:, e], int(lmax[q, e]))
+        cpu = len(sample) / (time.perf_counter() - t0)
+    line = {"metric": "curved-wave path trace (ab initio path sum)", "unit": "traces/s",
+            "kernel": "chx_path_trace",
+            "config": {"workload": "fcc Fe-Ni: 3 SS shells + MS classes to 5.5 A, 120 energies "
+                                   "k 2-18 A^-1, synthetic phase shifts of two types",
+                       "paths": len(sites), "energies": nE,
+                       "lmax_range": [int(lmax.min()), int(lmax.max())]},
+            "traces_per_s_with_host": ntr / wall, "traces_per_s_span": ntr / span,
+            "finite": bool(np.isfinite(tr).all()),
+            "cpu_baseline": None if cpu is None else {
+                "value": cpu, "unit": "traces/s", "cores": 1, "kind": "port",
+                "sample": "CPU evaluation with dense Wigner matrices, 6 traces (3 paths x 2 energies)"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global NPOS
     ap = argparse.ArgumentParser()
@@ -696,7 +777,7 @@ def main():
                     help="ladders per GPU (fewer for a small profiling case)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--kernel", default="sampler",
-                    choices=["sampler", "ft", "da", "uneven", "calib", "band"],
+                    choices=["sampler", "ft", "da", "uneven", "calib", "band", "pathtrace"],
                     help="ft: time the windowed FT contraction (chx_ft_batch); da: GPU-s of "
                          "the learned (delayed-acceptance) sampler to the plain sampler's "
                          "R-factor on the ternary configuration")
@@ -714,6 +795,8 @@ def main():
         return bench_calib(args)
     if args.kernel == "band":
         return bench_band(args)
+    if args.kernel == "pathtrace":
+        return bench_pathtrace(args)
 
     import torch
     import torch.distributed as dist
