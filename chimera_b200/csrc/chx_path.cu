@@ -10,6 +10,7 @@
 //   rotation: x = i^{-m} e^{-i m gamma} v; y_m'' = e^{-i m'' beta} sum_m' Delta_{m''m'} x_m';
 //             w_m = i^m e^{-i m alpha} sum_m'' Delta_{m''m} y_m''   (Delta = d^l(pi/2))
 //   leg:      w_l'm = sum_l g^m_{l'l}(p |a|) v_lm,  g = sum_l'' A^m_{l'l l''} h_l''(p |a|),
+//             one |m| block of g built in shared memory and applied to +-m,
 //             h by upward recurrence from h_0 = -i e^{ix}/x, h_1 = -e^{ix}/x (1 + i/x).
 #include "chx_common.cuh"
 
@@ -53,6 +54,7 @@ __global__ void __launch_bounds__(kPathThreads) k_path_trace(chx_path_t P, doubl
     extern __shared__ __align__(16) unsigned char smem[];
     const int G = P.glmax, NLM = (G + 1) * (G + 1);
     double2 *bufA = (double2 *)smem, *bufB = bufA + 3 * NLM, *hk = bufB + 3 * NLM;
+    double2 *gb = hk + 2 * G + 2;                   // (G+1)^2: one |m| block of g
     const int ie = blockIdx.x, ip = blockIdx.y, tid = threadIdx.x, nth = blockDim.x;
     const int ns = P.nsc[ip];
     const int lm = P.lmax[(long)ip * P.ne + ie];
@@ -130,11 +132,13 @@ __global__ void __launch_bounds__(kPathThreads) k_path_trace(chx_path_t P, doubl
                                  cscale(hk[l - 1], -1.0));
         }
         __syncthreads();
-        for (int q = tid; q < 3 * nlm; q += nth) {
-            const int c = q / nlm, L = q - c * nlm;
-            const int lp = l_of(L), m = L - lp * lp - lp, am = m < 0 ? -m : m;
-            double2 acc = make_double2(0, 0);
-            for (int l = am; l <= lm; ++l) {
+        // one |m| block at a time: g^|m|_{l'l} (l', l = |m| .. lm) built once
+        // into shared memory, then applied to m = +|m| and -|m| of all three
+        // columns (g is even in m)
+        for (int am = 0; am <= lm; ++am) {
+            const int n = lm - am + 1;
+            for (int q = tid; q < n * n; q += nth) {
+                const int lp = am + q / n, l = am + (q - (q / n) * n);
                 const long g3 = ((long)am * (G + 1) + lp) * (G + 1) + l;
                 const int off = P.goff[g3], cnt = P.gcnt[g3];
                 double2 g = make_double2(0, 0);
@@ -142,11 +146,21 @@ __global__ void __launch_bounds__(kPathThreads) k_path_trace(chx_path_t P, doubl
                     const double2 A = make_double2(P.gA[2 * (off + u)], P.gA[2 * (off + u) + 1]);
                     g = cadd(g, cmul(A, hk[P.glpp[off + u]]));
                 }
-                acc = cadd(acc, cmul(g, v[c * NLM + l * l + l + m]));
+                gb[q] = g;
             }
-            w[c * NLM + L] = acc;
+            __syncthreads();
+            const int nsg = am ? 2 : 1;
+            for (int q = tid; q < 3 * nsg * n; q += nth) {
+                const int c = q / (nsg * n), r = q - c * (nsg * n);
+                const int m = (r / n) ? -am : am, lp = am + (r - (r / n) * n);
+                const double2 *grow = gb + (lp - am) * n;
+                double2 acc = make_double2(0, 0);
+                for (int l = am; l <= lm; ++l)
+                    acc = cadd(acc, cmul(grow[l - am], v[c * NLM + l * l + l + m]));
+                w[c * NLM + lp * lp + lp + m] = acc;
+            }
+            __syncthreads();
         }
-        __syncthreads();
         { double2 *s = v; v = w; w = s; }
     }
     // ---- closing rotation, l = 1 rows only, and the trace
@@ -189,7 +203,7 @@ int chx_path_trace(const chx_path_t *P, double *out, void *stream) {
                 "path_trace: an array is NULL");
     CHX_REQUIRE(P->npath <= 65535, "path_trace: at most 65535 paths per call");
     const size_t nlm = (size_t)(P->glmax + 1) * (P->glmax + 1);
-    const size_t smem = sizeof(double2) * (6 * nlm + 2 * (size_t)P->glmax + 2);
+    const size_t smem = sizeof(double2) * (7 * nlm + 2 * (size_t)P->glmax + 2);
     CHX_REQUIRE(smem <= 227 * 1024, "path_trace: %zu bytes of shared memory needed", smem);
     cudaError_t e = cudaFuncSetAttribute(k_path_trace, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);

@@ -146,17 +146,37 @@ def path_frames(sites):
     return np.linalg.norm(legs, axis=1), np.array(eul)
 
 
+BUCKETS = (8, 16, 24, 32, MAX_L)     # table sizes energies are grouped by
+_DEV_TABLES = {}
+
+
+def _tables_on_device(cap):
+    """Device copies of the propagator runs and Delta blocks for lmax <= cap."""
+    if cap not in _DEV_TABLES:
+        off, cnt, lpp, A = propagator_runs(cap)
+        doff, dflat = delta_runs(cap)
+        _DEV_TABLES[cap] = dict(
+            goff=N.to_dev(off), gcnt=N.to_dev(cnt), glpp=N.to_dev(lpp),
+            gA=N.to_dev(np.ascontiguousarray(np.stack([A.real, A.imag], -1))),
+            doff=N.to_dev(doff), dflat=N.to_dev(dflat))
+    return _DEV_TABLES[cap]
+
+
 def path_trace(sites_list, types_list, p, t, lmax, stream=None):
     """Tr_{l=1} of every path's product at every energy, complex (npath, nE),
     on the device. sites_list: per path (N, 3) scatterer positions (bohr);
     types_list: per path N type indices into t; p (nE,) complex momenta
-    (bohr^-1); t (ntype, nE, nl) complex amplitudes; lmax (npath, nE)."""
+    (bohr^-1); t (ntype, nE, nl) complex amplitudes; lmax (npath, nE).
+    Energies are grouped by their largest lmax into table sizes of BUCKETS,
+    one launch each, so that low-lmax energies run with small shared-memory
+    footprints (more CTAs per SM)."""
     import torch
     lmax = np.asarray(lmax, np.int32)
     npath, ne = lmax.shape
     Lc = int(lmax.max())
-    if Lc > MAX_L or Lc + 1 > np.asarray(t).shape[2]:
-        raise ValueError(f"lmax {Lc} beyond the built cap {MAX_L} or the phase shifts")
+    t = np.asarray(t, complex)
+    if Lc > MAX_L or Lc + 1 > t.shape[2] or int(lmax.min()) < 1:
+        raise ValueError(f"lmax {Lc} outside 1..{MAX_L} or beyond the phase shifts")
     maxs = max(len(ty) for ty in types_list)
     nsc = np.array([len(ty) for ty in types_list], np.int32)
     typ = np.zeros((npath, maxs), np.int32)
@@ -167,22 +187,31 @@ def path_trace(sites_list, types_list, p, t, lmax, stream=None):
         typ[q, :len(ty)] = ty
         leg[q, :len(ls)] = ls
         eul[q, :len(eu)] = eu
-    off, cnt, lpp, A = propagator_runs(Lc)
-    doff, dflat = delta_runs(Lc)
-    t = np.asarray(t, complex)
-    dev = dict(nsc=N.to_dev(nsc), typ=N.to_dev(typ), leg=N.to_dev(leg), eul=N.to_dev(eul),
-               p=N.to_dev(np.stack([np.real(p), np.imag(p)], -1).astype(np.float64)),
-               t=N.to_dev(np.ascontiguousarray(np.stack([t.real, t.imag], -1))),
-               lmax=N.to_dev(lmax), goff=N.to_dev(off), gcnt=N.to_dev(cnt),
-               glpp=N.to_dev(lpp),
-               gA=N.to_dev(np.ascontiguousarray(np.stack([A.real, A.imag], -1))),
-               doff=N.to_dev(doff), dflat=N.to_dev(dflat))
-    out = torch.empty((npath, ne, 2), dtype=torch.float64, device="cuda")
-    P = N.PathSet()
-    P.npath, P.maxs, P.ne, P.ntype, P.nlt, P.glmax = npath, maxs, ne, t.shape[0], t.shape[2], Lc
-    for k in ("nsc", "typ", "leg", "eul", "p", "t", "lmax", "goff", "gcnt", "glpp", "gA",
-              "doff", "dflat"):
-        setattr(P, k, N.dptr(dev[k]))
-    N.call("chx_path_trace", C.byref(P), N.ptr(out), N.stream() if stream is None else stream)
-    o = out.cpu().numpy()
-    return o[..., 0] + 1j * o[..., 1]
+    paths = dict(nsc=N.to_dev(nsc), typ=N.to_dev(typ), leg=N.to_dev(leg), eul=N.to_dev(eul))
+    p = np.asarray(p, complex)
+    emax = lmax.max(axis=0)
+    # table size per energy: the bucket of its largest lmax, no larger than
+    # the phase shifts cover (lmax + 1 <= nl is checked above)
+    cap_of = np.array([min(next(b for b in BUCKETS if b >= e), t.shape[2] - 1) for e in emax])
+    result = np.empty((npath, ne), complex)
+    outs = []
+    for cap in sorted(set(cap_of.tolist())):
+        sel = np.nonzero(cap_of == cap)[0]
+        tab = _tables_on_device(cap)
+        ts = t[:, sel]
+        dev = dict(p=N.to_dev(np.stack([p[sel].real, p[sel].imag], -1).astype(np.float64)),
+                   t=N.to_dev(np.ascontiguousarray(np.stack([ts.real, ts.imag], -1))),
+                   lmax=N.to_dev(np.ascontiguousarray(lmax[:, sel])))
+        out = torch.empty((npath, sel.size, 2), dtype=torch.float64, device="cuda")
+        P = N.PathSet()
+        P.npath, P.maxs, P.ne, P.ntype, P.nlt, P.glmax = (npath, maxs, int(sel.size),
+                                                          t.shape[0], t.shape[2], cap)
+        for k, v in list(paths.items()) + list(tab.items()) + list(dev.items()):
+            setattr(P, k, N.dptr(v))
+        N.call("chx_path_trace", C.byref(P), N.ptr(out),
+               N.stream() if stream is None else stream)
+        outs.append((sel, out, dev))
+    for sel, out, _ in outs:
+        o = out.cpu().numpy()
+        result[:, sel] = o[..., 0] + 1j * o[..., 1]
+    return result
