@@ -151,9 +151,13 @@ class Problem:
         return np.random.default_rng(p).normal(0, self.noise, (self.nsp, self.k.size))
 
     def sigma_R(self):
-        """Per-component R-space sd of white k-space noise through each channel."""
-        sig = [self.noise * np.sqrt(0.5 * (np.abs(f.basis()) ** 2).sum(0)) for f in self.ft.fts]
-        return np.maximum(np.array(sig), 1e-12)
+        """Per-component R-space sd of white k-space noise through each channel
+        (a constant of the problem, computed once)."""
+        if getattr(self, "_sigma_R", None) is None:
+            sig = [self.noise * np.sqrt(0.5 * (np.abs(f.basis()) ** 2).sum(0))
+                   for f in self.ft.fts]
+            self._sigma_R = np.maximum(np.array(sig), 1e-12)
+        return self._sigma_R
 
     def position(self, p):
         """Target of sample position p: noise seeded by p."""

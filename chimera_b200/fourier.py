@@ -125,8 +125,13 @@ class FourierTransform:
 
     # ---------------------------------------------------------- evaluation
     def to_R(self, chi, bins=None, precision=0):
-        """chi (..., nk) -> complex chi(R) (..., nbins), default all nfft/2."""
-        return apply_basis(chi, self.basis(bins), precision)
+        """chi (..., nk) -> complex chi(R) (..., nbins), default all nfft/2.
+        The basis is uploaded to the device once per set of bins."""
+        key = None if bins is None else tuple(np.asarray(bins).tolist())
+        dev = self.__dict__.setdefault("_basis_dev", {})
+        if key not in dev:
+            dev[key] = basis_to_device(self.basis(bins))
+        return apply_basis(chi, self.basis(bins), precision, Bd=dev[key])
 
     def magnitude(self, chi):
         out = self.to_R(chi)
@@ -140,8 +145,18 @@ class FourierTransform:
         return (a + (b - a) * self._frac) * self._inside
 
 
-def apply_basis(chi, B, precision=0):
-    """Device contraction of chi (..., nk) with a complex basis (nk, nb)."""
+def basis_to_device(B):
+    """The (nk, nb) complex basis as the (nk, 2 nb) FP64 device array the
+    contraction takes (re, im interleaved)."""
+    import torch
+    nk = B.shape[0]
+    return torch.from_numpy(np.ascontiguousarray(
+        np.stack([B.real, B.imag], axis=-1).reshape(nk, -1))).to("cuda")
+
+
+def apply_basis(chi, B, precision=0, Bd=None):
+    """Device contraction of chi (..., nk) with a complex basis (nk, nb);
+    Bd: its device copy from basis_to_device, when already uploaded."""
     import torch
     N.require_cuda()
     host = not (isinstance(chi, torch.Tensor) and chi.is_cuda)
@@ -149,8 +164,8 @@ def apply_basis(chi, B, precision=0):
     lead = tuple(x.shape[:-1])
     nk = x.shape[-1]
     rows = int(np.prod(lead)) if lead else 1
-    Bd = torch.from_numpy(np.ascontiguousarray(
-        np.stack([B.real, B.imag], axis=-1).reshape(nk, -1))).to("cuda")
+    if Bd is None:
+        Bd = basis_to_device(B)
     nb = B.shape[1]
     out = torch.empty((rows, 2 * nb), dtype=torch.float64, device="cuda")
     nsc = int(N.lib().chx_ft_batch_scratch_bytes(rows, nk, nb, precision))

@@ -331,8 +331,11 @@ class Ladders:
         self._upload()
 
     # --------------------------------------------------------------- state
-    def init_state(self, li, species0, pos0, stream_species=None):
-        """Every rung of ladder li starts from (species0, pos0)."""
+    def init_state(self, li, species0, pos0, stream_species=None, defer=False):
+        """Every rung of ladder li starts from (species0, pos0). With `defer`
+        (and the shell table on) the FP64 start chi is left to one
+        chx_reanchor launch over every slot of the batch (`anchor_pending`)
+        instead of a full path sum per ladder; the two agree to rounding."""
         torch = self.torch
         s, b = self.specs[li], self.bufs[li]
         fm = s.fm
@@ -344,13 +347,18 @@ class Ladders:
         ideal = _host(fm.cell.ideal)
         b["moved"].copy_(torch.from_numpy(np.any(pos != ideal[None], axis=-1).astype(np.uint8)))
         # every rung starts from the same configuration: evaluate it once
-        chi = fm.chi_full(b["pos"][:1].contiguous(), b["species"][:1].contiguous(),
-                          precision=FP64)
         if s.ms is not None:
             C_ = s.ms.counts(b["species"][:1].contiguous())
             b["ms_C"].copy_(C_.expand(nrep, -1))
-            chi = chi + s.ms.chi_of(C_)
-        b["chi"].copy_(chi.expand(nrep, -1, -1))
+        if defer and self.use_table:
+            b["chi"].zero_()
+            self.__dict__.setdefault("_pending", set()).add(li)
+        else:
+            chi = fm.chi_full(b["pos"][:1].contiguous(), b["species"][:1].contiguous(),
+                              precision=FP64)
+            if s.ms is not None:
+                chi = chi + s.ms.chi_of(C_)
+            b["chi"].copy_(chi.expand(nrep, -1, -1))
         cnt = np.stack([(sp == q).sum(1) for q in range(self.nsp)], axis=1).astype(np.float64)
         b["count"].copy_(torch.from_numpy(cnt))
         b["rung_of"].copy_(torch.arange(nrep, dtype=torch.int32))
@@ -402,6 +410,18 @@ class Ladders:
                 b["chi"].copy_(chi)
                 b["n_acc"].zero_()
         self.refresh_chi2()
+
+    def anchor_pending(self):
+        """FP64 start chi of the ladders initialised with `defer`: one
+        chx_reanchor launch over their slots (pair-count form)."""
+        pend = self.__dict__.pop("_pending", set())
+        if not pend:
+            return
+        mask = np.zeros(self.nslots, bool)
+        for li in pend:
+            s0 = self.host[li].slot0
+            mask[s0:s0 + self.specs[li].nrep] = True
+        self.reanchor(mask)
 
     def accepted_since_anchor(self):
         """(nslots,) accepted moves since each slot's last re-anchoring."""
@@ -857,8 +877,9 @@ class BatchedSampler:
             sp = species0[li] if isinstance(species0, (list, tuple)) else species0
             ps = pos0[li] if isinstance(pos0, (list, tuple)) else pos0
             lad, q = self.ladder(li)
-            lad.init_state(q, sp, ps)
+            lad.init_state(q, sp, ps, defer=True)
         for lad in self.groups:
+            lad.anchor_pending()
             lad.refresh_chi2(reset_best=True)
 
     def autotune(self, reps=3, path=None):
