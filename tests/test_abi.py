@@ -81,3 +81,31 @@ def test_tensor_core_transform_sizes_its_scratch():
         rc = lib.chx_ft_batch(fake, rows, nk, fake, nR, prec, fake, fake, need - 1, None)
         assert rc == -1 and "scratch" in N.last_error()
     assert lib.chx_ft_batch(fake, rows, nk, fake, nR, 7, fake, fake, 0, None) == -1
+
+
+def test_calibration_and_path_trace_entries_check_their_arguments():
+    """chx_shell_rfactor and chx_path_trace reject bad descriptors with a
+    message before touching the device (no GPU needed); their structs match
+    the binding."""
+    import ctypes as C
+    from chimera_b200 import _native as N
+    lib = N.lib()
+    assert lib.chx_struct_size(6) == C.sizeof(N.Shell)
+    assert lib.chx_struct_size(7) == C.sizeof(N.PathSet)
+    assert lib.chx_shell_nparam(2, 5) == 33 and lib.chx_shell_nparam(3, 3) == 39
+    assert lib.chx_shell_nparam(0, 5) == -1
+    S = N.Shell()
+    S.nsp, S.nshell, S.nk, S.nkw, S.nbin, S.nfft, S.dk, S.dk_win = 2, 5, 241, 3, 100, 2048, 0.05, 1.0
+    dummy = C.c_void_p(16)
+    rc = lib.chx_shell_rfactor(C.byref(S), dummy, 4, dummy, dummy, None)
+    assert rc == -1 and "NULL" in N.last_error()
+    S.nfft = 1000                                    # not a power of two
+    rc = lib.chx_shell_rfactor(C.byref(S), dummy, 4, dummy, dummy, None)
+    assert rc == -1 and "limits" in N.last_error()
+    P = N.PathSet()
+    P.npath, P.maxs, P.ne, P.ntype, P.nlt, P.glmax = 3, 2, 10, 2, 60, 48   # lmax cap is 40
+    rc = lib.chx_path_trace(C.byref(P), dummy, None)
+    assert rc == -1 and "bad sizes" in N.last_error()
+    P.glmax = 20
+    rc = lib.chx_path_trace(C.byref(P), dummy, None)
+    assert rc == -1 and "NULL" in N.last_error()
