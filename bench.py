@@ -764,6 +764,75 @@ def bench_pathtrace(args):
     return 0
 
 
+def bench_pathsum(args):
+    """The full path sum (A1/A2): every single-scattering pair of a 4,000-site
+    fcc Fe-Ni cell to 6.2 A (z = 78, 312,000 pairs) at 241 k points for 256
+    configurations, FP32C and FP64 (chx_chi_full, CUDA events), and the exact
+    MS entry counts of the same configurations (3.94 M paths each,
+    chx_ms_counts + chx_ms_chi_of). Terms/s (one (pair, k) term each) and
+    paths/s; beside the CPU restatement of the reference kernels (oracle, C)
+    on one configuration."""
+    import time
+    import torch
+    from chimera_b200 import _native as N
+    from chimera_b200 import configs
+    from chimera_b200.forward import FP32C, FP64
+    N.lib()
+    prob = configs.Problem(ncell=(10, 10, 10), rmax=6.2, ms=True)
+    fm, ms = prob.fm, prob.ms
+    nconf = 256 if args.steps == 1200 else max(8, min(args.steps, 256))
+    rng = np.random.default_rng(0)
+    sp = torch.from_numpy(np.stack([prob.random_config(int(rng.integers(1 << 30)))
+                                    for _ in range(nconf)])).cuda()
+    pos = torch.from_numpy(np.repeat(prob.cell.ideal[None], nconf, 0)).cuda()
+    s = torch.cuda.current_stream()
+
+    def timed(fn, reps=3):
+        fn()
+        a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a_.record(s)
+        for _ in range(reps):
+            fn()
+        b_.record(s)
+        b_.synchronize()
+        return a_.elapsed_time(b_) * 1e-3 / reps
+
+    terms = nconf * fm.npairs * fm.nk
+    t32 = timed(lambda: fm.chi_full(pos, sp, precision=FP32C))
+    t64 = timed(lambda: fm.chi_full(pos, sp, precision=FP64))
+    tms = timed(lambda: ms.full(sp))
+    c32 = fm.chi_full(pos[:4], sp[:4], precision=FP32C)
+    c64 = fm.chi_full(pos[:4], sp[:4], precision=FP64)
+    err = float((c32 - c64).abs().max() / (c64.abs().max()))
+    cpu = None
+    if not args.no_cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import sampler as OS
+        pr = OS.Problem(prob.cell.ideal, prob.top.i, prob.top.j, prob.top.shift, prob.top.shell,
+                        prob.top.sigma2, prob.k, prob.tables.f, prob.tables.delta,
+                        prob.tables.lam, prob.tables.s02, [], np.zeros((0, 1024), complex),
+                        np.zeros(1024, bool), np.ones((0, 1024)), prob.nsp)
+        sp0 = sp[:1].cpu().numpy()
+        t0 = time.perf_counter()
+        pr.chi_full(prob.cell.ideal[None], sp0)
+        cpu = fm.npairs * fm.nk / (time.perf_counter() - t0)
+    line = {"metric": "full path sum (single + exact multiple scattering)", "unit": "terms/s",
+            "kernel": "chx_chi_full, chx_ms_counts",
+            "config": {"workload": "fcc Fe50Ni50 4000 atoms, SS to 6.2 A (z 78), exact MS 5.5 A, "
+                                   "241 k", "configurations": nconf, "pairs": fm.npairs,
+                       "ms_paths": int(prob.paths.npath)},
+            "fp32c_terms_per_s": terms / t32, "fp64_terms_per_s": terms / t64,
+            "fp32c_ms_per_config": t32 / nconf * 1e3, "fp64_ms_per_config": t64 / nconf * 1e3,
+            "ms_paths_per_s": nconf * prob.paths.npath / tms,
+            "fp32c_vs_fp64_max_rel": err,
+            "cpu_baseline": None if cpu is None else {
+                "value": cpu, "unit": "terms/s", "cores": 1, "kind": "port",
+                "sample": "C restatement of the reference's compute_r / build_ptype / "
+                          "chi_forward, one configuration"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     global NPOS
     ap = argparse.ArgumentParser()
@@ -777,7 +846,8 @@ def main():
                     help="ladders per GPU (fewer for a small profiling case)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--kernel", default="sampler",
-                    choices=["sampler", "ft", "da", "uneven", "calib", "band", "pathtrace"],
+                    choices=["sampler", "ft", "da", "uneven", "calib", "band", "pathtrace",
+                             "pathsum"],
                     help="ft: time the windowed FT contraction (chx_ft_batch); da: GPU-s of "
                          "the learned (delayed-acceptance) sampler to the plain sampler's "
                          "R-factor on the ternary configuration")
@@ -797,6 +867,8 @@ def main():
         return bench_band(args)
     if args.kernel == "pathtrace":
         return bench_pathtrace(args)
+    if args.kernel == "pathsum":
+        return bench_pathsum(args)
 
     import torch
     import torch.distributed as dist
