@@ -160,7 +160,8 @@ class Stage1:
                          for n in self.names])
 
     def rows(self, X, a0=None):
-        """Flat parameter rows of the search vectors X (P, ndim)."""
+        """Flat parameter rows of the search vectors X (P, ndim), one
+        `unpack` and set_params per vector (the reference's path)."""
         dicts = []
         for x in np.atleast_2d(X):
             p = self.unpack(x)
@@ -168,6 +169,68 @@ class Stage1:
                 p.setdefault("a0", a0)
             dicts.append(p)
         return self.sm.flat_rows(dicts)
+
+    def rows_fast(self, X, a0=None):
+        """The rows of `rows`, for a whole population at once: every block of
+        the vector maps to the flat layout linearly (bond offsets and pair-
+        width logs through their free-entry bases) or through exp."""
+        sm, nsp, nsh = self.sm, self.nsp, self.sm.nshell
+        X = np.atleast_2d(np.asarray(X, float))
+        P = X.shape[0]
+        sl = sm._slices()
+        out = np.tile(sm.flat(), (P, 1))
+        if a0 is not None and not self.free_a0:
+            out[:, sl["a0"]] = a0
+        i = 0
+        out[:, sl["dE0"]] = X[:, i:i + nsp]
+        i += nsp
+        if self.with_sigma:
+            out[:, sl["sigma_scale"]] = np.exp(X[:, i:i + 1])
+            i += 1
+        if self.nsss:
+            sss = np.ones((P, nsh))
+            sss[:, 1:] = np.exp(X[:, i:i + self.nsss])
+            out[:, sl["sigma_shell_scale"]] = sss
+            i += self.nsss
+        if self.ndr:
+            basis = np.array([dr_from_free(np.eye(self.ndr)[q], self.comp).ravel()
+                              for q in range(self.ndr)])
+            out[:, sl["dr"]] = X[:, i:i + self.ndr] @ basis
+            i += self.ndr
+        if self.c3:
+            c = np.zeros((P, nsh))
+            c[:, 0] = X[:, i]
+            out[:, sl["c3"]] = c
+            i += 1
+        if self.c4:
+            c = np.zeros((P, nsh))
+            c[:, 0] = X[:, i]
+            out[:, sl["c4"]] = c
+            i += 1
+        if self.nsp_pair:
+            basis = np.array([np.log(pair_log_from_free(np.eye(self.nsp_pair)[q],
+                                                        self.comp)).ravel()
+                              for q in range(self.nsp_pair)])
+            out[:, sl["sigma_pair"]] = np.exp(X[:, i:i + self.nsp_pair] @ basis)
+            i += self.nsp_pair
+        if self.ms:
+            out[:, sl["ms_amp"]] = np.exp(X[:, i:i + 1])
+            out[:, sl["ms_c"]] = np.exp(X[:, i + 1:i + 2])
+            i += 2
+        if self.ms_edge:
+            u = np.zeros((P, nsp))
+            u[:, :nsp - 1] = X[:, i:i + nsp - 1]
+            u[:, -1] = -u[:, :-1].sum(1)
+            out[:, sl["ms_amp_edge"]] = np.exp(u)
+            i += nsp - 1
+        if self.window:
+            out[:, sl["kmin"]] = X[:, i:i + 1]
+            out[:, sl["kmax"]] = X[:, i + 1:i + 2]
+            i += 2
+        if self.free_a0:
+            out[:, sl["a0"]] = X[:, i:i + 1]
+            i += 1
+        return out
 
 
 def de_stage1(sm: ShellModel, Nc, data, mask, idx, stage: Stage1, kweight=None, a0=None,
@@ -183,7 +246,7 @@ def de_stage1(sm: ShellModel, Nc, data, mask, idx, stage: Stage1, kweight=None, 
     def score(xT):
         X = np.asarray(xT, float)
         X = X[:, None] if X.ndim == 1 else X
-        rows = stage.rows(X.T, a0=a0)
+        rows = stage.rows_fast(X.T, a0=a0)
         calls[0] += rows.shape[0]
         rf, _ = sm.r_factor_batch(Nc, data, mask, idx, rows)
         rf = np.where(np.isfinite(rf), rf, np.inf)

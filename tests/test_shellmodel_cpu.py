@@ -78,3 +78,20 @@ def test_stage1_vector_matches_reference():
     rows = st.rows(g["stage_X"], a0=3.59)
     assert np.allclose(rows, g["stage_rows"], rtol=1e-15, atol=0)
     assert np.array_equal(sm.flat(), g["stage_base"])      # the model's own state is untouched
+
+
+@pytest.mark.parametrize("flags", [dict(), dict(free_c4=True, free_sigma_pair=True,
+                                               free_ms_edge=True, free_a0=True),
+                                   dict(ms=False, free_window=False, free_dr=False)])
+def test_stage1_rows_fast_equal_rows(flags):
+    """The population-at-once mapping gives the rows of one unpack +
+    set_params per vector, to rounding (exp of a sum of logs)."""
+    from chimera_b200.calibrate import Stage1
+    g = golden("shellmodel.npz")
+    sm = host_model(g)
+    sm.set_flat(g["stage_base"])
+    st = Stage1(sm, (0.5, 0.5), elements=("Fe", "Ni"), **flags)
+    lo, hi = np.array(st.bounds).T
+    X = lo + (hi - lo) * np.random.default_rng(1).uniform(size=(40, lo.size))
+    a0 = None if flags.get("free_a0") else 3.59
+    assert np.allclose(st.rows_fast(X, a0=a0), st.rows(X, a0=a0), rtol=1e-13, atol=1e-16)
