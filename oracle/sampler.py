@@ -221,7 +221,8 @@ class PlainSampler:
             d = p.etab[sh * nn + ptnew] - p.etab[sh * nn + pold]
             x = x + p.energy_beta * (d * valid).sum(axis=1)
         u = self.urng.random(n)
-        acc = (x <= 0) | (u < np.exp(-np.minimum(x, 60.0)))
+        with np.errstate(over="ignore"):       # exp(-x) for x <= 0 is not used
+            acc = (x <= 0) | (u < np.exp(-np.minimum(x, 60.0)))
         # the step's proposals and exact chi^2 changes, by rung (read by tests)
         self.last = dict(a=a.copy(), b=b.copy(), swap=isswap.copy(), species=self.species.copy(),
                          d=c2 - self.chi2)
