@@ -9,24 +9,22 @@
 // keeps 8. TF32 (precision 3): the operands rounded to TF32 (10-bit
 // mantissa), one MMA (kind::tf32) per product, FP32 accumulation.
 //
-// Layout. The basis (2 nR x nk, transposed) is split by a pre-pass
-// (k_tc_split) into 128 x 32 tiles in scratch (hi and lo BF16, or TF32),
-// each already in the no-swizzle K-major shared-memory layout the MMA reads:
-// 8 x 16-byte core matrices, 128 B apart along K and one row group (K bytes
-// / 16 core matrices) apart along rows.
+// Layout. Both operands are split by a pre-pass (k_tc_split: the basis,
+// 2 nR x nk transposed, and chi, rows x nk) into 128 x 32 tiles in scratch
+// (hi and lo BF16, or TF32), each already in the no-swizzle K-major
+// shared-memory layout the MMA reads: 8 x 16-byte core matrices, 128 B apart
+// along K and one row group (K bytes / 16 core matrices) apart along rows;
+// one thread of the pre-pass writes one 16-byte core-matrix row.
 // The main kernel (k_ft_tc, one 128 x 128 output tile per CTA, three CTAs per
-// SM) runs a two-stage ring over 32-wide K chunks: one thread brings the
-// chunk's basis tiles in with bulk-async copies (cp.async.bulk, no
-// multicast) completing on an mbarrier while all 128 threads read the chunk
-// of chi (FP64, any row alignment) and write its hi and lo parts straight
-// into the same layout (each warp load 256 contiguous bytes of one row);
-// one thread then issues the chunk's MMAs (2 x 3 of 128 x 128 x 16 BF16, or
-// 4 of 128 x 128 x 8 TF32) into one 128 x 128 FP32 accumulator in tensor
-// memory and commits them
-// to the stage's mbarrier, and the threads move on to the next chunk while
-// the tensor core works. Four warps finally read the accumulator (lane =
-// row) with tcgen05.ld, turn each 32 x 32 block around in shared memory and
-// write FP64 rows with coalesced stores.
+// SM) runs a two-stage ring over 32-wide K chunks driven by one thread: the
+// chunk's A and B tiles arrive by bulk-async copies (cp.async.bulk, no
+// multicast) completing on the stage's mbarrier, the chunk's MMAs (6 of
+// 128 x 128 x 16 BF16, or 4 of 128 x 128 x 8 TF32) go into one 128 x 128 FP32
+// accumulator in tensor memory and commit to the stage's second mbarrier,
+// and the stage is refilled with the chunk two ahead once they are done.
+// Four warps finally read the accumulator (lane = row) with tcgen05.ld, turn
+// each 32 x 32 block around in shared memory and write FP64 rows with
+// coalesced stores.
 //
 // Every wait is bounded (kTcSpin polls); a wait that runs out sets the error
 // word in the first 4 bytes of scratch (CHX_DEVERR_INDEX), waits (bounded)
@@ -37,7 +35,7 @@
 namespace chx {
 
 constexpr int kTcM = 128, kTcN = 128, kTcK = 32;        // CTA tile and K chunk
-constexpr int kTcStages = 2;
+constexpr int kTcStages = 2;                           // copy/MMA ring depth
 constexpr uint32_t kTcLBO = 128;                        // core matrices along K (bytes)
 constexpr int kTcSpin = 1 << 24;
 constexpr int kTcTmemCols = kTcN;                       // FP32 accumulator columns
@@ -145,32 +143,50 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
 
 // the operand parts of X (R x C, element (r, c) at X[r*sr + c*sc]) zero-padded
 // to Rp x Kp, written as 128 x 32 tiles (tile (rt, kt) at (rt * Kp/32 + kt)):
-// hi and lo BF16, or TF32 into hi
+// hi and lo BF16, or TF32 into hi. One thread takes 8 consecutive k of one
+// row (a 16-byte row of a core matrix in BF16, two in TF32) and threads run
+// row-fastest, so that rows of chi (k contiguous) and columns of the basis
+// (rows contiguous) are both read coalesced and every store is 16 bytes.
 template <bool TF32>
 __global__ void k_tc_split(const double *__restrict__ X, int R, int C, long sr, long sc, int Rp,
                            int Kp, uint8_t *__restrict__ hi, uint8_t *__restrict__ lo) {
     typedef TcMode<TF32> Md;
-    const long n = (long)Rp * Kp;
+    const int ng = Kp / 8;
+    const long n = (long)Rp * ng;
     for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
          q += (long)gridDim.x * blockDim.x) {
-        const int r = (int)(q / Kp), k = (int)(q % Kp);
-        const double x = (r < R && k < C) ? X[r * sr + k * sc] : 0.0;
-        const long off = ((long)(r / kTcN) * (Kp / kTcK) + k / kTcK) * Md::tileB +
-                         Md::off(r % kTcN, k % kTcK);
+        const int r = (int)(q % Rp), k0 = (int)(q / Rp) * 8;
+        double x[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            x[j] = (r < R && k0 + j < C) ? X[r * sr + (long)(k0 + j) * sc] : 0.0;
+        const long tile = ((long)(r / kTcN) * (Kp / kTcK) + k0 / kTcK) * Md::tileB;
+        const int rr = r % kTcN, kk = k0 % kTcK;
         if constexpr (TF32) {
-            *(uint32_t *)(hi + off) = tc_tf32((float)x);
+            uint4 a, b;
+            a.x = tc_tf32((float)x[0]); a.y = tc_tf32((float)x[1]);
+            a.z = tc_tf32((float)x[2]); a.w = tc_tf32((float)x[3]);
+            b.x = tc_tf32((float)x[4]); b.y = tc_tf32((float)x[5]);
+            b.z = tc_tf32((float)x[6]); b.w = tc_tf32((float)x[7]);
+            *(uint4 *)(hi + tile + Md::off(rr, kk)) = a;
+            *(uint4 *)(hi + tile + Md::off(rr, kk + 4)) = b;
         } else {
-            const __nv_bfloat16 h = __double2bfloat16(x);
-            const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
-            *(__nv_bfloat16 *)(hi + off) = h;
-            *(__nv_bfloat16 *)(lo + off) = l;
+            __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                h[j] = __double2bfloat16(x[j]);
+                l[j] = __double2bfloat16(x[j] - (double)__bfloat162float(h[j]));
+            }
+            *(uint4 *)(hi + tile + Md::off(rr, kk)) = *(const uint4 *)h;
+            *(uint4 *)(lo + tile + Md::off(rr, kk)) = *(const uint4 *)l;
         }
     }
 }
 
 template <bool TF32>
-__global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi, int rows,
-                                                  int nk, const uint8_t *__restrict__ Bhi,
+__global__ void __launch_bounds__(128, 3) k_ft_tc(const uint8_t *__restrict__ Ahi,
+                                                  const uint8_t *__restrict__ Alo, int rows,
+                                                  const uint8_t *__restrict__ Bhi,
                                                   const uint8_t *__restrict__ Blo, int nkt,
                                                   int ncol, double *__restrict__ out,
                                                   int *__restrict__ err) {
@@ -204,82 +220,69 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
 
-    const long tstride = (long)nkt * Md::tileB;              // one row of basis tiles
+    const long tstride = (long)nkt * Md::tileB;              // one row of tiles
     const uint8_t *b_hi = Bhi + nt * tstride, *b_lo = Blo + nt * tstride;
+    const uint8_t *a_hi = Ahi + mt * tstride, *a_lo = Alo + mt * tstride;
     const int row0 = mt * kTcM;
-    int issued[kTcStages] = {0, 0}, landed[kTcStages] = {0, 0};
-    for (int kt = 0; kt < nkt; ++kt) {
-        const int s = kt & 1;
-        const uint32_t par = (uint32_t)((kt >> 1) & 1);
-        uint8_t *st = ring + (size_t)s * Md::stage;
-        // the stage's previous MMAs (chunk kt - 2) must be done before it is refilled
-        if (kt >= kTcStages && !s_fail) {
-            if (tid == 0 && !tc_mbar_wait(&freed[s], par ^ 1)) s_fail = 1;
-        }
-        __syncthreads();
-        if (s_fail) break;
-        if (tid == 0) {
-            // stage: A parts (tileA each), then B parts (tileB each)
-            uint8_t *sb = st + Md::parts * Md::tileA;
-            tc_expect(&full[s], Md::parts * Md::tileB);
-            tc_load_tile(sb, b_hi + (long)kt * Md::tileB, Md::tileB, &full[s]);
-            if (!TF32) tc_load_tile(sb + Md::tileB, b_lo + (long)kt * Md::tileB, Md::tileB, &full[s]);
-            ++issued[s];
-        }
-        // chi chunk, 128 rows x 32 k: lane = k, warp w takes rows w, w + 4, ...,
-        // so every warp load reads 256 contiguous bytes of one row
-        {
-            const int gk = kt * kTcK + lane;
-            const bool kin = gk < nk;
-            double v[kTcM / 4];
-#pragma unroll
-            for (int i = 0; i < kTcM / 4; ++i) {
-                const int grow = row0 + warp + 4 * i;
-                v[i] = (kin && grow < rows) ? __ldg(chi + (long)grow * nk + gk) : 0.0;
-            }
-#pragma unroll
-            for (int i = 0; i < kTcM / 4; ++i) {
-                const uint32_t off = Md::off(warp + 4 * i, lane);
-                if constexpr (TF32) {
-                    *(uint32_t *)(st + off) = tc_tf32((float)v[i]);
-                } else {
-                    const __nv_bfloat16 h = __double2bfloat16(v[i]);
-                    const __nv_bfloat16 l = __double2bfloat16(v[i] - (double)__bfloat162float(h));
-                    *(__nv_bfloat16 *)(st + off) = h;
-                    *(__nv_bfloat16 *)(st + Md::tileA + off) = l;
-                }
-            }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            if (!tc_mbar_wait(&full[s], par)) {
-                s_fail = 1;
-            } else {
-                ++landed[s];
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t base = tc_smem(st);
-                const uint32_t bbase = base + Md::parts * Md::tileA;
-#pragma unroll
-                for (int kk = 0; kk < kTcK / Md::kmma; ++kk) {
-                    const uint32_t ko = kk * 2 * kTcLBO;   // one MMA's K = two core matrices
-                    const uint64_t ahi = tc_desc(base + ko, Md::sbo);
-                    const uint64_t bhi = tc_desc(bbase + ko, Md::sbo);
-                    tc_mma<TF32>(tmem, ahi, bhi, (kt | kk) != 0);
-                    if constexpr (!TF32) {
-                        const uint64_t alo = tc_desc(base + Md::tileA + ko, Md::sbo);
-                        const uint64_t blo = tc_desc(bbase + Md::tileB + ko, Md::sbo);
-                        tc_mma<TF32>(tmem, ahi, blo, 1u);
-                        tc_mma<TF32>(tmem, alo, bhi, 1u);
-                    }
-                }
-                tc_commit(&freed[s]);
-            }
-        }
-    }
+    // Thread 0 runs the pipeline: the operand parts of chunk kt (A and B, hi
+    // and lo, split in advance into the tiles' shared-memory image) arrive by
+    // bulk copies into stage kt % S, the MMAs of chunk kt are issued when they
+    // have landed, and the stage is refilled with chunk kt + S as soon as
+    // those MMAs are done, so the copies of the next S - 1 chunks overlap the
+    // MMAs of this one. Every wait is bounded; a failed wait ends the loop and
+    // the copies still owed are waited for before the CTA moves on.
     if (tid == 0) {
+        int issued[kTcStages] = {}, landed[kTcStages] = {};
+        auto issue = [&](int kt) {
+            const int s = kt % kTcStages;
+            uint8_t *st = ring + (size_t)s * Md::stage;
+            uint8_t *sb = st + Md::parts * Md::tileA;
+            tc_expect(&full[s], Md::parts * (Md::tileA + Md::tileB));
+            tc_load_tile(st, a_hi + (long)kt * Md::tileA, Md::tileA, &full[s]);
+            tc_load_tile(sb, b_hi + (long)kt * Md::tileB, Md::tileB, &full[s]);
+            if (!TF32) {
+                tc_load_tile(st + Md::tileA, a_lo + (long)kt * Md::tileA, Md::tileA, &full[s]);
+                tc_load_tile(sb + Md::tileB, b_lo + (long)kt * Md::tileB, Md::tileB, &full[s]);
+            }
+            ++issued[s];
+        };
+        for (int kt = 0; kt < nkt && kt < kTcStages; ++kt) issue(kt);
+        int ok = 1;
+        for (int kt = 0; kt < nkt && ok; ++kt) {
+            const int s = kt % kTcStages;
+            const uint32_t par = (uint32_t)((kt / kTcStages) & 1);
+            if (!tc_mbar_wait(&full[s], par)) {
+                ok = 0;
+                break;
+            }
+            ++landed[s];
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = tc_smem(ring + (size_t)s * Md::stage);
+            const uint32_t bbase = base + Md::parts * Md::tileA;
+#pragma unroll
+            for (int kk = 0; kk < kTcK / Md::kmma; ++kk) {
+                const uint32_t ko = kk * 2 * kTcLBO;       // one MMA's K = two core matrices
+                const uint64_t ahi = tc_desc(base + ko, Md::sbo);
+                const uint64_t bhi = tc_desc(bbase + ko, Md::sbo);
+                tc_mma<TF32>(tmem, ahi, bhi, (kt | kk) != 0);
+                if constexpr (!TF32) {
+                    const uint64_t alo = tc_desc(base + Md::tileA + ko, Md::sbo);
+                    const uint64_t blo = tc_desc(bbase + Md::tileB + ko, Md::sbo);
+                    tc_mma<TF32>(tmem, ahi, blo, 1u);
+                    tc_mma<TF32>(tmem, alo, bhi, 1u);
+                }
+            }
+            tc_commit(&freed[s]);
+            if (kt + kTcStages < nkt) {
+                if (!tc_mbar_wait(&freed[s], par)) {
+                    ok = 0;
+                    break;
+                }
+                issue(kt + kTcStages);
+            }
+        }
+        if (!ok) s_fail = 1;
         tc_commit(&done);
-        // copies still owed to a stage (after a failed wait): wait for them, bounded
         for (int s = 0; s < kTcStages; ++s)
             for (int w = landed[s]; w < issued[s]; ++w)
                 if (!tc_mbar_wait(&full[s], (uint32_t)(w & 1))) break;
@@ -334,16 +337,18 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const double *__restrict__ chi
 
 struct TcPlan {
     int Mp, Np, Kp;
-    size_t b_bytes, total;
+    size_t a_bytes, b_bytes, total;
 };
-// chi is split inside the main kernel; the basis parts go to scratch
+// scratch: an error word, then the operand parts of the basis and of chi,
+// each split into the tiles' shared-memory image
 static TcPlan tc_plan(int rows, int nk, int nR, bool tf32) {
     TcPlan p;
     p.Mp = (rows + kTcM - 1) / kTcM * kTcM;
     p.Np = (2 * nR + kTcN - 1) / kTcN * kTcN;
     p.Kp = (nk + kTcK - 1) / kTcK * kTcK;
+    p.a_bytes = (size_t)p.Mp * p.Kp * (tf32 ? 4 : 2);
     p.b_bytes = (size_t)p.Np * p.Kp * (tf32 ? 4 : 2);
-    p.total = 256 + (tf32 ? 1 : 2) * p.b_bytes;
+    p.total = 256 + (tf32 ? 1 : 2) * (p.a_bytes + p.b_bytes);
     return p;
 }
 
@@ -361,18 +366,23 @@ static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *b
     CHX_REQUIRE(((uintptr_t)scratch & 255) == 0, "ft_batch: scratch must be 256-byte aligned");
     uint8_t *base = (uint8_t *)scratch;
     int *err = (int *)base;
+    const int parts = TF32 ? 1 : 2;
     uint8_t *bhi = base + 256, *bl = bhi + p.b_bytes;
+    uint8_t *ahi = base + 256 + parts * p.b_bytes, *al = ahi + p.a_bytes;
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch memset");
     const int ncol = 2 * nR;
-    const long nb = (long)p.Np * p.Kp;
+    const long nb = (long)p.Np * p.Kp / 8;
     k_tc_split<TF32><<<(unsigned)std::min<long>((nb + 255) / 256, 592), 256, 0, st>>>(
         basis, ncol, nk, 1, ncol, p.Np, p.Kp, bhi, bl);
+    const long na = (long)p.Mp * p.Kp / 8;
+    k_tc_split<TF32><<<(unsigned)std::min<long>((na + 255) / 256, 1184), 256, 0, st>>>(
+        chi, rows, nk, nk, 1, p.Mp, p.Kp, ahi, al);
     e = cudaFuncSetAttribute(k_ft_tc<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)Md::smem);
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc attribute");
     dim3 grid(p.Np / kTcN, p.Mp / kTcM);
-    k_ft_tc<TF32><<<grid, 128, Md::smem, st>>>(chi, rows, nk, bhi, bl, p.Kp / kTcK, ncol, out,
+    k_ft_tc<TF32><<<grid, 128, Md::smem, st>>>(ahi, al, rows, bhi, bl, p.Kp / kTcK, ncol, out,
                                                err);
     CHX_CHECK_LAUNCH("ft_batch tc");
     return CHX_OK;

@@ -67,13 +67,14 @@ def test_surrogate_entries_check_their_arguments():
 
 def test_tensor_core_transform_sizes_its_scratch():
     """Precisions 2 (split-BF16) and 3 (TF32) need a scratch of the basis
-    parts plus an error word; a smaller one is refused with a message."""
+    and chi operand parts plus an error word; a smaller one is refused with a
+    message."""
     from chimera_b200 import _native as N
     lib = N.lib()
     rows, nk, nR = 4096, 241, 200
-    Np, Kp = -(-2 * nR // 128) * 128, -(-nk // 32) * 32
-    assert lib.chx_ft_batch_scratch_bytes(rows, nk, nR, 2) == 256 + 2 * Np * Kp * 2
-    assert lib.chx_ft_batch_scratch_bytes(rows, nk, nR, 3) == 256 + Np * Kp * 4
+    Mp, Np, Kp = -(-rows // 128) * 128, -(-2 * nR // 128) * 128, -(-nk // 32) * 32
+    assert lib.chx_ft_batch_scratch_bytes(rows, nk, nR, 2) == 256 + 2 * (Mp + Np) * Kp * 2
+    assert lib.chx_ft_batch_scratch_bytes(rows, nk, nR, 3) == 256 + (Mp + Np) * Kp * 4
     assert lib.chx_ft_batch_scratch_bytes(rows, nk, nR, 0) == 0
     fake = ctypes.c_void_p(1 << 20)
     for prec in (2, 3):
