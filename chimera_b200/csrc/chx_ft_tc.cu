@@ -141,20 +141,40 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
         : "memory");
 }
 
-// the operand parts of X (R x C, element (r, c) at X[r*sr + c*sc]) zero-padded
-// to Rp x Kp, written as 128 x 32 tiles (tile (rt, kt) at (rt * Kp/32 + kt)):
-// hi and lo BF16, or TF32 into hi. One thread takes 8 consecutive k of one
-// row (a 16-byte row of a core matrix in BF16, two in TF32) and threads run
+// One operand of the contraction: X (R x C, element (r, c) at X[r*sr + c*sc])
+// zero-padded to Rp x Kp, and where its parts go.
+struct TcSplitJob {
+    const double *X;
+    int R, C, Rp;
+    long sr, sc;
+    uint8_t *hi, *lo;
+};
+
+// The operand parts of both jobs (the basis in blocks [0, nblk_a), chi in the
+// rest), written as 128 x 32 tiles (tile (rt, kt) at (rt * Kp/32 + kt)): hi
+// and lo BF16, or TF32 into hi. One thread takes 8 consecutive k of one row (a
+// 16-byte row of a core matrix in BF16, two in TF32) and threads run
 // row-fastest, so that rows of chi (k contiguous) and columns of the basis
 // (rows contiguous) are both read coalesced and every store is 16 bytes.
+// Block 0 also clears the error word of the contraction that follows, which
+// is launched as a programmatic dependent of this grid.
 template <bool TF32>
-__global__ void k_tc_split(const double *__restrict__ X, int R, int C, long sr, long sc, int Rp,
-                           int Kp, uint8_t *__restrict__ hi, uint8_t *__restrict__ lo) {
+__global__ void k_tc_split(TcSplitJob ja, TcSplitJob jb, int Kp, int nblk_a, int *err) {
     typedef TcMode<TF32> Md;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (blockIdx.x == 0 && threadIdx.x == 0) *err = 0;
+    const bool first = (int)blockIdx.x < nblk_a;
+    const TcSplitJob &J = first ? ja : jb;
+    const long blk = first ? blockIdx.x : blockIdx.x - nblk_a;
+    const long nblk = first ? nblk_a : gridDim.x - nblk_a;
+    const double *__restrict__ X = J.X;
+    const int R = J.R, C = J.C, Rp = J.Rp;
+    const long sr = J.sr, sc = J.sc;
+    uint8_t *__restrict__ hi = J.hi;
+    uint8_t *__restrict__ lo = J.lo;
     const int ng = Kp / 8;
     const long n = (long)Rp * ng;
-    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
-         q += (long)gridDim.x * blockDim.x) {
+    for (long q = blk * blockDim.x + threadIdx.x; q < n; q += nblk * blockDim.x) {
         const int r = (int)(q % Rp), k0 = (int)(q / Rp) * 8;
         double x[8];
 #pragma unroll
@@ -219,6 +239,9 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const uint8_t *__restrict__ Ah
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
+    // the operand parts and the cleared error word come from the split grid
+    // this launch may overlap: everything below waits for it to complete
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 
     const long tstride = (long)nkt * Md::tileB;              // one row of tiles
     const uint8_t *b_hi = Bhi + nt * tstride, *b_lo = Blo + nt * tstride;
@@ -369,21 +392,36 @@ static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *b
     const int parts = TF32 ? 1 : 2;
     uint8_t *bhi = base + 256, *bl = bhi + p.b_bytes;
     uint8_t *ahi = base + 256 + parts * p.b_bytes, *al = ahi + p.a_bytes;
-    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), st);
-    if (e != cudaSuccess) return cuda_fail(e, "ft_batch memset");
     const int ncol = 2 * nR;
-    const long nb = (long)p.Np * p.Kp / 8;
-    k_tc_split<TF32><<<(unsigned)std::min<long>((nb + 255) / 256, 592), 256, 0, st>>>(
-        basis, ncol, nk, 1, ncol, p.Np, p.Kp, bhi, bl);
-    const long na = (long)p.Mp * p.Kp / 8;
-    k_tc_split<TF32><<<(unsigned)std::min<long>((na + 255) / 256, 1184), 256, 0, st>>>(
-        chi, rows, nk, nk, 1, p.Mp, p.Kp, ahi, al);
-    e = cudaFuncSetAttribute(k_ft_tc<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)Md::smem);
+    // both operands split by one launch: the basis (its columns are the rows
+    // of B) in the first blocks, chi in the rest
+    const TcSplitJob jb = {basis, ncol, nk, p.Np, 1, ncol, bhi, bl};
+    const TcSplitJob ja = {chi, rows, nk, p.Mp, nk, 1, ahi, al};
+    const long nb = (long)p.Np * p.Kp / 8, na = (long)p.Mp * p.Kp / 8;
+    const int gb = (int)std::min<long>((nb + 255) / 256, 592);
+    const int ga = (int)std::min<long>((na + 255) / 256, 1184);
+    k_tc_split<TF32><<<gb + ga, 256, 0, st>>>(jb, ja, p.Kp, gb, err);
+    CHX_CHECK_LAUNCH("ft_batch split");
+    cudaError_t e = cudaFuncSetAttribute(k_ft_tc<TF32>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Md::smem);
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc attribute");
-    dim3 grid(p.Np / kTcN, p.Mp / kTcM);
-    k_ft_tc<TF32><<<grid, 128, Md::smem, st>>>(ahi, al, rows, bhi, bl, p.Kp / kTcK, ncol, out,
-                                               err);
+    // a programmatic dependent of the split: its prologue (barriers, tensor
+    // memory) overlaps the split's tail, its loads wait for the split's end
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(p.Np / kTcN, p.Mp / kTcM);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = Md::smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, k_ft_tc<TF32>, (const uint8_t *)ahi, (const uint8_t *)al, rows,
+                           (const uint8_t *)bhi, (const uint8_t *)bl, p.Kp / kTcK, ncol, out,
+                           err);
+    if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc launch");
     CHX_CHECK_LAUNCH("ft_batch tc");
     return CHX_OK;
 }
