@@ -29,16 +29,22 @@
 // Every wait is bounded (kTcSpin polls); a wait that runs out sets the error
 // word in the first 4 bytes of scratch (CHX_DEVERR_INDEX), waits (bounded)
 // for the copies and MMAs it started, frees its tensor memory and returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include "chx_common.cuh"
 
 namespace chx {
 
 constexpr int kTcM = 128, kTcN = 128, kTcK = 32;        // CTA tile and K chunk
-constexpr int kTcStages = 2;                           // copy/MMA ring depth
+constexpr int kTcStages = 5;                           // ring depth, both operands streamed
+constexpr int kTcStagesRes = 4;                        // ring depth, chi only (basis resident)
+constexpr int kTcResKp = 256;                          // largest padded nk kept resident
+constexpr int kTcBox = 32 * 16 * 8;                     // one staged chi(R) box: 32 rows x 16 FP64
+constexpr int kTcAcc = 2;                              // accumulators in tensor memory
+constexpr int kTcThreads = 192;                        // 4 epilogue warps, producer, MMA
 constexpr uint32_t kTcLBO = 128;                        // core matrices along K (bytes)
 constexpr int kTcSpin = 1 << 24;
-constexpr int kTcTmemCols = kTcN;                       // FP32 accumulator columns
+constexpr int kTcTmemCols = kTcAcc * kTcN;              // FP32 accumulator columns
 
 // Operand modes: split-BF16 (two BF16 parts of 2 bytes, MMA K = 16, kind::f16
 // with A and B BF16) and TF32 (one 4-byte part, MMA K = 8, kind::tf32); both
@@ -48,11 +54,18 @@ struct TcMode {
     static constexpr int esz = TF32 ? 4 : 2, parts = TF32 ? 1 : 2, kmma = TF32 ? 8 : 16;
     static constexpr uint32_t sbo = (uint32_t)(kTcK * esz / 16) * 128;   // row group stride
     static constexpr uint32_t tileA = kTcM * kTcK * esz, tileB = kTcN * kTcK * esz;
-    static constexpr uint32_t stage = parts * (tileA + tileB);
+    static constexpr uint32_t stage = parts * (tileA + tileB);   // both operands of a chunk
+    static constexpr uint32_t stage_a = parts * tileA;           // chi's parts of a chunk
     static constexpr uint32_t fmt = TF32 ? 2u : 1u;
     static constexpr uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) |
                                       ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
-    static constexpr size_t smem = (size_t)kTcStages * stage + 1024;
+    // shared memory: the stage ring, two staged chi(R) boxes per epilogue
+    // warp, the resident basis tile (all nkt chunks) when RES, alignment
+    static size_t smem(bool res, int nkt) {
+        return res ? (size_t)kTcStagesRes * stage_a + 4 * 2 * kTcBox +
+                         (size_t)parts * nkt * tileB + 1024
+                   : (size_t)kTcStages * stage + 4 * 2 * kTcBox + 1024;
+    }
     // byte offset of element (r, k) inside one operand tile of kTcK values
     static __host__ __device__ __forceinline__ uint32_t off(int r, int k) {
         return (uint32_t)((r >> 3) * sbo + (k * esz / 16) * kTcLBO + (r & 7) * 16 +
@@ -71,8 +84,9 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t sbo) {
            ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
 }
 
-__device__ __forceinline__ void tc_mbar_init(uint64_t *bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(bar)) : "memory");
+__device__ __forceinline__ void tc_mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem(bar)), "r"(count)
+                 : "memory");
 }
 
 __device__ __forceinline__ bool tc_mbar_wait(uint64_t *bar, uint32_t parity) {
@@ -153,9 +167,10 @@ struct TcSplitJob {
 // The operand parts of both jobs (the basis in blocks [0, nblk_a), chi in the
 // rest), written as 128 x 32 tiles (tile (rt, kt) at (rt * Kp/32 + kt)): hi
 // and lo BF16, or TF32 into hi. One thread takes 8 consecutive k of one row (a
-// 16-byte row of a core matrix in BF16, two in TF32) and threads run
-// row-fastest, so that rows of chi (k contiguous) and columns of the basis
-// (rows contiguous) are both read coalesced and every store is 16 bytes.
+// 16-byte row of a core matrix in BF16, two in TF32); one warp takes 8 rows x
+// 32 k (lane = row + 8 x k group), so that it reads 256-byte runs of the rows
+// of chi (64-byte runs of the basis columns) and writes one row group of one
+// tile, 512 contiguous bytes in BF16 (1 KB in TF32).
 // Block 0 also clears the error word of the contraction that follows, which
 // is launched as a programmatic dependent of this grid.
 template <bool TF32>
@@ -172,10 +187,12 @@ __global__ void k_tc_split(TcSplitJob ja, TcSplitJob jb, int Kp, int nblk_a, int
     const long sr = J.sr, sc = J.sc;
     uint8_t *__restrict__ hi = J.hi;
     uint8_t *__restrict__ lo = J.lo;
-    const int ng = Kp / 8;
-    const long n = (long)Rp * ng;
+    const long n = (long)Rp * (Kp / 8);                      // Rp, Kp: multiples of 128, 32
+    const int nrg = Rp / 8;
     for (long q = blk * blockDim.x + threadIdx.x; q < n; q += nblk * blockDim.x) {
-        const int r = (int)(q % Rp), k0 = (int)(q / Rp) * 8;
+        const long w = q >> 5;
+        const int l = (int)(q & 31);
+        const int r = (int)(w % nrg) * 8 + (l & 7), k0 = (int)(w / nrg) * 32 + (l >> 3) * 8;
         double x[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j)
@@ -203,21 +220,72 @@ __global__ void k_tc_split(TcSplitJob ja, TcSplitJob jb, int Kp, int nblk_a, int
     }
 }
 
-template <bool TF32>
-__global__ void __launch_bounds__(128, 3) k_ft_tc(const uint8_t *__restrict__ Ahi,
-                                                  const uint8_t *__restrict__ Alo, int rows,
-                                                  const uint8_t *__restrict__ Bhi,
-                                                  const uint8_t *__restrict__ Blo, int nkt,
-                                                  int ncol, double *__restrict__ out,
-                                                  int *__restrict__ err) {
+// Bounded wait that also gives up as soon as another role of the CTA has
+// recorded a failure in *fail.
+__device__ __forceinline__ bool tc_mbar_wait_or_fail(uint64_t *bar, uint32_t parity,
+                                                     const volatile int *fail) {
+    const uint32_t a = tc_smem(bar);
+    for (int it = 0; it < kTcSpin; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (*fail) return false;
+    }
+    return false;
+}
+
+// Persistent contraction: one CTA per SM walks the output tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... (tile t = row tile t / ntn, column tile t % ntn).
+// Warp 4 lane 0 (producer) streams the operand chunks of all its tiles through
+// the stage ring, warp 5 lane 0 (MMA) accumulates tile i into tensor-memory
+// accumulator i % 2, and warps 0-3 drain accumulator (i - 1) % 2 into chi(R)
+// meanwhile, so that the FP64 stores of one tile overlap the MMAs of the next.
+// Barriers: full[s] (chunk landed, producer -> MMA), freed[s] (its MMAs done,
+// MMA -> producer), acc_full[b] (tile accumulated, MMA -> epilogue) and
+// acc_empty[b] (accumulator read out, the four epilogue warps -> MMA).
+// RES: every CTA keeps one column tile (tc_tile) and its basis parts, loaded
+// with the chunks of its first tile, stay resident in shared memory; only
+// chi's parts stream through the ring after that, which halves the bytes a
+// tile moves from L2 into the SM (the bound of the main loop).
+template <bool RES>
+__device__ __forceinline__ bool tc_tile(int i, int ntn, int mtiles, int &mt, int &nt) {
+    const int G = gridDim.x, c = blockIdx.x;
+    if (RES) {
+        nt = c % ntn;
+        mt = c / ntn + i * ((G - 1 - nt) / ntn + 1);         // this column's CTAs share its rows
+        return mt < mtiles;
+    }
+    const int t = c + i * G;
+    mt = t / ntn;
+    nt = t % ntn;
+    return t < ntn * mtiles;
+}
+
+template <bool TF32, bool RES>
+__global__ void __launch_bounds__(kTcThreads, 1) k_ft_tc(const uint8_t *__restrict__ Ahi,
+                                                         const uint8_t *__restrict__ Alo,
+                                                         int rows,
+                                                         const uint8_t *__restrict__ Bhi,
+                                                         const uint8_t *__restrict__ Blo,
+                                                         int nkt, int ncol, int ntn, int mtiles,
+                                                         const __grid_constant__ CUtensorMap tm_out,
+                                                         int *__restrict__ err) {
     extern __shared__ uint8_t tc_raw[];
-    __shared__ __align__(8) uint64_t full[kTcStages], freed[kTcStages], done;
+    __shared__ __align__(8) uint64_t full[kTcStages], freed[kTcStages], acc_full[kTcAcc],
+        acc_empty[kTcAcc], done;
     __shared__ uint32_t s_tmem;
-    __shared__ int s_fail;
+    __shared__ volatile int s_fail;
     uint8_t *ring = (uint8_t *)(((uintptr_t)tc_raw + 1023) & ~(uintptr_t)1023);
     typedef TcMode<TF32> Md;
+    constexpr int S = RES ? kTcStagesRes : kTcStages;
+    constexpr uint32_t SB = RES ? Md::stage_a : Md::stage;    // bytes of one ring stage
+    uint8_t *bres = ring + (size_t)S * SB + 4 * 2 * kTcBox;   // resident basis (RES)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int nt = blockIdx.x, mt = blockIdx.y;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -226,12 +294,16 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const uint8_t *__restrict__ Ah
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (tid == 0) {
-        for (int s = 0; s < kTcStages; ++s) {
-            tc_mbar_init(&full[s]);
-            tc_mbar_init(&freed[s]);
+    if (tid == 128) {
+        for (int s = 0; s < S; ++s) {
+            tc_mbar_init(&full[s], 1);
+            tc_mbar_init(&freed[s], 1);
         }
-        tc_mbar_init(&done);
+        for (int b = 0; b < kTcAcc; ++b) {
+            tc_mbar_init(&acc_full[b], 1);
+            tc_mbar_init(&acc_empty[b], 4);
+        }
+        tc_mbar_init(&done, 1);
         s_fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -243,115 +315,177 @@ __global__ void __launch_bounds__(128, 3) k_ft_tc(const uint8_t *__restrict__ Ah
     // this launch may overlap: everything below waits for it to complete
     asm volatile("griddepcontrol.wait;" ::: "memory");
 
-    const long tstride = (long)nkt * Md::tileB;              // one row of tiles
-    const uint8_t *b_hi = Bhi + nt * tstride, *b_lo = Blo + nt * tstride;
-    const uint8_t *a_hi = Ahi + mt * tstride, *a_lo = Alo + mt * tstride;
-    const int row0 = mt * kTcM;
-    // Thread 0 runs the pipeline: the operand parts of chunk kt (A and B, hi
-    // and lo, split in advance into the tiles' shared-memory image) arrive by
-    // bulk copies into stage kt % S, the MMAs of chunk kt are issued when they
-    // have landed, and the stage is refilled with chunk kt + S as soon as
-    // those MMAs are done, so the copies of the next S - 1 chunks overlap the
-    // MMAs of this one. Every wait is bounded; a failed wait ends the loop and
-    // the copies still owed are waited for before the CTA moves on.
-    if (tid == 0) {
-        int issued[kTcStages] = {}, landed[kTcStages] = {};
-        auto issue = [&](int kt) {
-            const int s = kt % kTcStages;
-            uint8_t *st = ring + (size_t)s * Md::stage;
-            uint8_t *sb = st + Md::parts * Md::tileA;
-            tc_expect(&full[s], Md::parts * (Md::tileA + Md::tileB));
-            tc_load_tile(st, a_hi + (long)kt * Md::tileA, Md::tileA, &full[s]);
-            tc_load_tile(sb, b_hi + (long)kt * Md::tileB, Md::tileB, &full[s]);
-            if (!TF32) {
-                tc_load_tile(st + Md::tileA, a_lo + (long)kt * Md::tileA, Md::tileA, &full[s]);
-                tc_load_tile(sb + Md::tileB, b_lo + (long)kt * Md::tileB, Md::tileB, &full[s]);
-            }
-            ++issued[s];
-        };
-        for (int kt = 0; kt < nkt && kt < kTcStages; ++kt) issue(kt);
-        int ok = 1;
-        for (int kt = 0; kt < nkt && ok; ++kt) {
-            const int s = kt % kTcStages;
-            const uint32_t par = (uint32_t)((kt / kTcStages) & 1);
-            if (!tc_mbar_wait(&full[s], par)) {
-                ok = 0;
-                break;
-            }
-            ++landed[s];
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t base = tc_smem(ring + (size_t)s * Md::stage);
-            const uint32_t bbase = base + Md::parts * Md::tileA;
-#pragma unroll
-            for (int kk = 0; kk < kTcK / Md::kmma; ++kk) {
-                const uint32_t ko = kk * 2 * kTcLBO;       // one MMA's K = two core matrices
-                const uint64_t ahi = tc_desc(base + ko, Md::sbo);
-                const uint64_t bhi = tc_desc(bbase + ko, Md::sbo);
-                tc_mma<TF32>(tmem, ahi, bhi, (kt | kk) != 0);
-                if constexpr (!TF32) {
-                    const uint64_t alo = tc_desc(base + Md::tileA + ko, Md::sbo);
-                    const uint64_t blo = tc_desc(bbase + Md::tileB + ko, Md::sbo);
-                    tc_mma<TF32>(tmem, ahi, blo, 1u);
-                    tc_mma<TF32>(tmem, alo, bhi, 1u);
+    const long tstride = (long)nkt * Md::tileB;              // one row of tiles (tileA == tileB)
+    if (warp == 4) {
+        if (lane == 0) {
+            // producer: chunk c (over all tiles of this CTA) into stage c % S,
+            // once the MMAs of the chunk S before it have released the stage
+            int issued[kTcStages] = {};
+            long c = 0;
+            bool ok = true;
+            int mt, nt;
+            for (int i = 0; ok && tc_tile<RES>(i, ntn, mtiles, mt, nt); ++i) {
+                const uint8_t *a_hi = Ahi + mt * tstride, *a_lo = Alo + mt * tstride;
+                const uint8_t *b_hi = Bhi + nt * tstride, *b_lo = Blo + nt * tstride;
+                const bool with_b = !RES || i == 0;           // the basis chunk comes along
+                for (int kt = 0; kt < nkt; ++kt, ++c) {
+                    const int s = (int)(c % S);
+                    const long u = c / S;
+                    if (u > 0 && !tc_mbar_wait_or_fail(&freed[s], (uint32_t)((u - 1) & 1), &s_fail)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t *st = ring + (size_t)s * SB;
+                    uint8_t *sb = RES ? bres + (size_t)kt * Md::parts * Md::tileB
+                                      : st + Md::parts * Md::tileA;
+                    tc_expect(&full[s], Md::parts * (Md::tileA + (with_b ? Md::tileB : 0u)));
+                    tc_load_tile(st, a_hi + (long)kt * Md::tileA, Md::tileA, &full[s]);
+                    if (!TF32)
+                        tc_load_tile(st + Md::tileA, a_lo + (long)kt * Md::tileA, Md::tileA,
+                                     &full[s]);
+                    if (with_b) {
+                        tc_load_tile(sb, b_hi + (long)kt * Md::tileB, Md::tileB, &full[s]);
+                        if (!TF32)
+                            tc_load_tile(sb + Md::tileB, b_lo + (long)kt * Md::tileB, Md::tileB,
+                                         &full[s]);
+                    }
+                    ++issued[s];
                 }
             }
-            tc_commit(&freed[s]);
-            if (kt + kTcStages < nkt) {
-                if (!tc_mbar_wait(&freed[s], par)) {
-                    ok = 0;
+            if (!ok) s_fail = 1;
+            // at most the last fill of each stage can still be in flight
+            for (int s = 0; s < S; ++s)
+                if (issued[s] && !tc_mbar_wait(&full[s], (uint32_t)((issued[s] - 1) & 1)))
+                    s_fail = 1;
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {
+            long c = 0;
+            bool ok = true;
+            int mt, nt;
+            for (int i = 0; ok && tc_tile<RES>(i, ntn, mtiles, mt, nt); ++i) {
+                const int b = i & 1, ub = i >> 1;
+                if (ub > 0 &&
+                    !tc_mbar_wait_or_fail(&acc_empty[b], (uint32_t)((ub - 1) & 1), &s_fail)) {
+                    ok = false;
                     break;
                 }
-                issue(kt + kTcStages);
-            }
-        }
-        if (!ok) s_fail = 1;
-        tc_commit(&done);
-        for (int s = 0; s < kTcStages; ++s)
-            for (int w = landed[s]; w < issued[s]; ++w)
-                if (!tc_mbar_wait(&full[s], (uint32_t)(w & 1))) break;
-        if (!tc_mbar_wait(&done, 0)) s_fail = 1;
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-    if (!s_fail) {
-        // each warp turns its 32 x 32 block around in shared memory (the ring
-        // is free now) so that every store writes 32 consecutive doubles
-        float *tb = (float *)ring + warp * 32 * 33;
-#pragma unroll 1
-        for (int c0 = 0; c0 < kTcN; c0 += 32) {
-            uint32_t v[32];
-            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
-                "%10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, "
-                "%26, %27, %28, %29, %30, %31}, [%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
-                  "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-                  "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
-                  "=r"(v[30]), "=r"(v[31])
-                : "r"(ta)
-                : "memory");
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(b * kTcN);
+                for (int kt = 0; kt < nkt; ++kt, ++c) {
+                    const int s = (int)(c % S);
+                    const long u = c / S;
+                    if (!tc_mbar_wait_or_fail(&full[s], (uint32_t)(u & 1), &s_fail)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t base = tc_smem(ring + (size_t)s * SB);
+                    const uint32_t bbase =
+                        RES ? tc_smem(bres + (size_t)kt * Md::parts * Md::tileB)
+                            : base + Md::parts * Md::tileA;
 #pragma unroll
-            for (int j = 0; j < 32; ++j) tb[lane * 33 + j] = __uint_as_float(v[j]);
-            __syncwarp();
-            const int col = nt * kTcN + c0 + lane;
-#pragma unroll 4
-            for (int r = 0; r < 32; ++r) {
-                const int row = row0 + warp * 32 + r;
-                if (row < rows && col < ncol) out[(long)row * ncol + col] = (double)tb[r * 33 + lane];
+                    for (int kk = 0; kk < kTcK / Md::kmma; ++kk) {
+                        const uint32_t ko = kk * 2 * kTcLBO;   // one MMA's K = two core matrices
+                        const uint64_t ahi = tc_desc(base + ko, Md::sbo);
+                        const uint64_t bhi = tc_desc(bbase + ko, Md::sbo);
+                        tc_mma<TF32>(acc, ahi, bhi, (kt | kk) != 0);
+                        if constexpr (!TF32) {
+                            const uint64_t alo = tc_desc(base + Md::tileA + ko, Md::sbo);
+                            const uint64_t blo = tc_desc(bbase + Md::tileB + ko, Md::sbo);
+                            tc_mma<TF32>(acc, ahi, blo, 1u);
+                            tc_mma<TF32>(acc, alo, bhi, 1u);
+                        }
+                    }
+                    tc_commit(&freed[s]);
+                }
+                if (ok) tc_commit(&acc_full[b]);
             }
-            __syncwarp();
+            if (!ok) s_fail = 1;
+            // every MMA this thread issued is complete before the CTA moves on
+            tc_commit(&done);
+            if (!tc_mbar_wait(&done, 0)) s_fail = 1;
         }
-    } else if (tid == 0) {
-        atomicOr(err, CHX_DEVERR_INDEX);
+    } else {
+        // epilogue, warp w (0-3) owns accumulator lanes (rows) 32w..32w+31: the
+        // tile's 128 columns into registers, the accumulator released, then
+        // eight 32-row x 16-column FP64 boxes staged in shared memory (128-byte
+        // swizzle, two slots) and written by TMA stores; rows and columns past
+        // the ends of chi(R) are clipped by the tensor map
+        uint8_t *stg = ring + (size_t)S * SB + (size_t)warp * 2 * kTcBox;
+        int mt, nt;
+        for (int i = 0; tc_tile<RES>(i, ntn, mtiles, mt, nt); ++i) {
+            const int b = i & 1, ub = i >> 1;
+            int got = 0;
+            if (lane == 0) got = tc_mbar_wait_or_fail(&acc_full[b], (uint32_t)(ub & 1), &s_fail);
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) {
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t v[4][32];
+            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * kTcN);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, "
+                    "%9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, "
+                    "%24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                    : "=r"(v[q][0]), "=r"(v[q][1]), "=r"(v[q][2]), "=r"(v[q][3]), "=r"(v[q][4]),
+                      "=r"(v[q][5]), "=r"(v[q][6]), "=r"(v[q][7]), "=r"(v[q][8]), "=r"(v[q][9]),
+                      "=r"(v[q][10]), "=r"(v[q][11]), "=r"(v[q][12]), "=r"(v[q][13]),
+                      "=r"(v[q][14]), "=r"(v[q][15]), "=r"(v[q][16]), "=r"(v[q][17]),
+                      "=r"(v[q][18]), "=r"(v[q][19]), "=r"(v[q][20]), "=r"(v[q][21]),
+                      "=r"(v[q][22]), "=r"(v[q][23]), "=r"(v[q][24]), "=r"(v[q][25]),
+                      "=r"(v[q][26]), "=r"(v[q][27]), "=r"(v[q][28]), "=r"(v[q][29]),
+                      "=r"(v[q][30]), "=r"(v[q][31])
+                    : "r"(ta + (uint32_t)(q * 32))
+                    : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                 tc_smem(&acc_empty[b]))
+                             : "memory");
+            const int y = mt * kTcM + warp * 32;
+#pragma unroll
+            for (int g = 0; g < kTcN / 16; ++g) {
+                const int x = nt * kTcN + g * 16;             // even: 16-byte aligned
+                uint8_t *box = stg + (g & 1) * kTcBox;
+                // the slot's previous store has finished reading it
+                if (lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                __syncwarp();
+                // row = lane, 128 bytes; 16-byte chunk c at position c ^ (row & 7)
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    const double2 d = make_double2((double)__uint_as_float(v[g >> 1][(g & 1) * 16 + 2 * c]),
+                                                   (double)__uint_as_float(v[g >> 1][(g & 1) * 16 + 2 * c + 1]));
+                    *(double2 *)(box + lane * 128 + ((c ^ (lane & 7)) << 4)) = d;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    if (x < ncol && y < rows)
+                        asm volatile(
+                            "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], "
+                            "[%3];" ::"l"((uint64_t)&tm_out),
+                            "r"(x), "r"(y), "r"(tc_smem(box))
+                            : "memory");
+                    // one group per box, empty for a box past the ends, so that
+                    // "all but the last group read" always means the other slot
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                }
+            }
+        }
+        // the stores are complete before the CTA leaves
+        if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+        __syncwarp();
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    if (tid == 0 && s_fail) atomicOr(err, CHX_DEVERR_INDEX);
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
                      "r"(kTcTmemCols)
@@ -379,6 +513,50 @@ int64_t ft_batch_tc_scratch(int rows, int nk, int nR, bool tf32) {
     return (int64_t)tc_plan(rows, nk, nR, tf32).total;
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link against the driver library)
+typedef CUresult (*TcEncodeFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                               const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                               const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                               CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static TcEncodeFn tc_encode_fn() {
+    static TcEncodeFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000,
+                                             cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (TcEncodeFn)p;
+    }
+    return fn;
+}
+
+// the contraction as a programmatic dependent of the split: its prologue
+// (barriers, tensor memory) overlaps the split's tail, its loads wait for the
+// split's end
+template <bool TF32, bool RES>
+static cudaError_t tc_launch(int grid, size_t smem, cudaStream_t st, const uint8_t *ahi,
+                             const uint8_t *al, int rows, const uint8_t *bhi, const uint8_t *bl,
+                             int nkt, int ncol, int ntn, int mtiles, const CUtensorMap &tm,
+                             int *err) {
+    cudaError_t e = cudaFuncSetAttribute(k_ft_tc<TF32, RES>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kTcThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_ft_tc<TF32, RES>, ahi, al, rows, bhi, bl, nkt, ncol, ntn,
+                              mtiles, tm, err);
+}
+
 template <bool TF32>
 static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *basis, int nR,
                             double *out, void *scratch, int64_t scratch_bytes, cudaStream_t st) {
@@ -387,12 +565,31 @@ static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *b
     CHX_REQUIRE(scratch && scratch_bytes >= (int64_t)p.total,
                 "ft_batch: the tensor-core path needs %zu bytes of scratch", p.total);
     CHX_REQUIRE(((uintptr_t)scratch & 255) == 0, "ft_batch: scratch must be 256-byte aligned");
+    CHX_REQUIRE(((uintptr_t)out & 15) == 0,
+                "ft_batch: precisions 2 and 3 need out 16-byte aligned");
+    const int ncol = 2 * nR;
+    // chi(R) (rows x ncol FP64, rows ncol * 8 bytes apart) as the TMA store
+    // target, in boxes of 32 rows x 16 columns, 128-byte swizzle
+    const TcEncodeFn enc = tc_encode_fn();
+    CHX_REQUIRE(enc != nullptr, "ft_batch: cuTensorMapEncodeTiled is not available");
+    CUtensorMap tm;
+    const cuuint64_t gdim[2] = {(cuuint64_t)ncol, (cuuint64_t)rows};
+    const cuuint64_t gstride[1] = {(cuuint64_t)ncol * sizeof(double)};
+    const cuuint32_t box[2] = {16, 32}, estr[2] = {1, 1};
+    const CUresult cr = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)out, gdim, gstride,
+                            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CHX_REQUIRE(cr == CUDA_SUCCESS, "ft_batch: chi(R) tensor map refused (CUresult %d)", (int)cr);
+    int dev = 0, nsm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "ft_batch device query");
+
     uint8_t *base = (uint8_t *)scratch;
     int *err = (int *)base;
     const int parts = TF32 ? 1 : 2;
     uint8_t *bhi = base + 256, *bl = bhi + p.b_bytes;
     uint8_t *ahi = base + 256 + parts * p.b_bytes, *al = ahi + p.a_bytes;
-    const int ncol = 2 * nR;
     // both operands split by one launch: the basis (its columns are the rows
     // of B) in the first blocks, chi in the rest
     const TcSplitJob jb = {basis, ncol, nk, p.Np, 1, ncol, bhi, bl};
@@ -402,25 +599,17 @@ static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *b
     const int ga = (int)std::min<long>((na + 255) / 256, 1184);
     k_tc_split<TF32><<<gb + ga, 256, 0, st>>>(jb, ja, p.Kp, gb, err);
     CHX_CHECK_LAUNCH("ft_batch split");
-    cudaError_t e = cudaFuncSetAttribute(k_ft_tc<TF32>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)Md::smem);
-    if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc attribute");
-    // a programmatic dependent of the split: its prologue (barriers, tensor
-    // memory) overlaps the split's tail, its loads wait for the split's end
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(p.Np / kTcN, p.Mp / kTcM);
-    cfg.blockDim = dim3(128);
-    cfg.dynamicSmemBytes = Md::smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, k_ft_tc<TF32>, (const uint8_t *)ahi, (const uint8_t *)al, rows,
-                           (const uint8_t *)bhi, (const uint8_t *)bl, p.Kp / kTcK, ncol, out,
-                           err);
+
+    // persistent: one CTA per SM; the basis tile stays resident when it fits
+    // and every column tile has a CTA of its own
+    const int ntn = p.Np / kTcN, mtiles = p.Mp / kTcM, nkt = p.Kp / kTcK;
+    const int grid = std::min(ntn * mtiles, nsm);
+    const bool res = p.Kp <= kTcResKp && ntn <= grid;
+    const size_t smem = Md::smem(res, nkt);
+    e = res ? tc_launch<TF32, true>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol, ntn,
+                                    mtiles, tm, err)
+            : tc_launch<TF32, false>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol, ntn,
+                                     mtiles, tm, err);
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc launch");
     CHX_CHECK_LAUNCH("ft_batch tc");
     return CHX_OK;

@@ -56,3 +56,32 @@ def test_split_bf16_batch_of_the_series_configuration(cuda):
         # per-bin relative error stays small where chi(R) is not tiny
         big = np.abs(z0) > 0.05 * scale
         assert (np.abs(z2 - z0)[big] / np.abs(z0)[big]).max() <= 5e-3
+
+
+@pytest.mark.parametrize("precision", [2, 3])
+def test_tensor_core_batch_wider_than_one_wave(cuda, precision):
+    """More output tiles than SMs, so that every CTA of the persistent
+    contraction walks two or three tiles through both accumulators, and
+    column counts (1,200 and 1,210 real columns) whose last tile has staged
+    boxes wholly and partly past the end of chi(R), with the basis tile
+    resident in shared memory (241 k points) and streamed beside chi (321 k
+    points): each of three repeated calls into the same output equals the
+    FP64 contraction within the precision's tolerance, bin by bin where
+    chi(R) is not tiny."""
+    import torch
+    from chimera_b200.fourier import FourierTransform, apply_basis
+    from chimera_b200.tables import uniform_k
+    rng = np.random.default_rng(11)
+    for rows, nb, kmax in ((4096, 600, 14.0), (6000, 605, 14.0), (4096, 600, 18.0)):
+        k = uniform_k(2.0, kmax)
+        f = FourierTransform(k, 3.0, 13.0, 2, window="kaiser")
+        B = f.basis(np.arange(nb) % 250)
+        chi = rng.normal(0, 1, (rows, k.size)) * np.exp(-0.1 * k)[None]
+        x = torch.from_numpy(chi).cuda()
+        z0 = apply_basis(x, B, 0).cpu().numpy()
+        scale = np.abs(z0).max()
+        big = np.abs(z0) > 0.05 * scale
+        for _ in range(3):
+            z = apply_basis(x, B, precision).cpu().numpy()
+            assert np.abs(z - z0).max() <= TOL[precision] * scale, (rows, nb)
+            assert (np.abs(z - z0)[big] / np.abs(z0)[big]).max() <= 50 * TOL[precision]
