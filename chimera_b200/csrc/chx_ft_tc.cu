@@ -9,22 +9,22 @@
 // keeps 8. TF32 (precision 3): the operands rounded to TF32 (10-bit
 // mantissa), one MMA (kind::tf32) per product, FP32 accumulation.
 //
-// Layout. Both operands are split by a pre-pass (k_tc_split: the basis,
-// 2 nR x nk transposed, and chi, rows x nk) into 128 x 32 tiles in scratch
-// (hi and lo BF16, or TF32), each already in the no-swizzle K-major
-// shared-memory layout the MMA reads: 8 x 16-byte core matrices, 128 B apart
-// along K and one row group (K bytes / 16 core matrices) apart along rows;
-// one thread of the pre-pass writes one 16-byte core-matrix row.
-// The main kernel (k_ft_tc, one 128 x 128 output tile per CTA, three CTAs per
-// SM) runs a two-stage ring over 32-wide K chunks driven by one thread: the
-// chunk's A and B tiles arrive by bulk-async copies (cp.async.bulk, no
-// multicast) completing on the stage's mbarrier, the chunk's MMAs (6 of
-// 128 x 128 x 16 BF16, or 4 of 128 x 128 x 8 TF32) go into one 128 x 128 FP32
-// accumulator in tensor memory and commit to the stage's second mbarrier,
-// and the stage is refilled with the chunk two ahead once they are done.
-// Four warps finally read the accumulator (lane = row) with tcgen05.ld, turn
-// each 32 x 32 block around in shared memory and write FP64 rows with
-// coalesced stores.
+// Layout. Both operands are split by a pre-pass (k_tc_split, one launch for
+// both: the basis, 2 nR x nk transposed, and chi, rows x nk) into 128 x 32
+// tiles in scratch (hi and lo BF16, or TF32), each already in the no-swizzle
+// K-major shared-memory layout the MMA reads: 8 x 16-byte core matrices,
+// 128 B apart along K and one row group (K bytes / 16 core matrices) apart
+// along rows.
+// The contraction (k_ft_tc) is persistent, one CTA per SM over the 128 x 128
+// output tiles, and launched as a programmatic dependent of the split. One
+// thread streams 32-wide K chunks by bulk-async copies (cp.async.bulk, no
+// multicast) through a ring of stages; one thread issues each chunk's MMAs
+// (6 of 128 x 128 x 16 BF16, or 4 of 128 x 128 x 8 TF32) into one of two
+// 128-column FP32 accumulators in tensor memory; four warps read the other
+// accumulator (lane = row, tcgen05.ld), stage 32 x 16 FP64 boxes in shared
+// memory and write chi(R) by TMA tensor stores, so that one tile's stores
+// overlap the next tile's MMAs. With nk <= 256 every CTA keeps one column
+// tile of the basis resident in shared memory and streams only chi.
 //
 // Every wait is bounded (kTcSpin polls); a wait that runs out sets the error
 // word in the first 4 bytes of scratch (CHX_DEVERR_INDEX), waits (bounded)

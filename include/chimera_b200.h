@@ -409,7 +409,9 @@ CHX_API int chx_apply_exchange(const chx_ladder_t *d_ladders, int ladder, const 
  *    precision: 0 FP64 (SIMT), 1 FP32 (SIMT), 2 split-BF16 three-product on
  *    the tcgen05 tensor cores with FP32 accumulation, 3 TF32 on the tcgen05
  *    tensor cores (one product, FP32 accumulation). Precisions 2 and 3 write
- *    a device error word (CHX_DEVERR_*) into the first 4 bytes of scratch.
+ *    a device error word (CHX_DEVERR_*) into the first 4 bytes of scratch
+ *    (256-byte aligned) and need out 16-byte aligned (it is written by TMA
+ *    tensor stores).
  * ------------------------------------------------------------------------ */
 CHX_API int chx_ft_batch(const double *chi, int rows, int nk, const double *basis, int nR,
                  int precision, double *out, void *scratch, int64_t scratch_bytes,

@@ -67,8 +67,8 @@ def test_surrogate_entries_check_their_arguments():
 
 def test_tensor_core_transform_sizes_its_scratch():
     """Precisions 2 (split-BF16) and 3 (TF32) need a scratch of the basis
-    and chi operand parts plus an error word; a smaller one is refused with a
-    message."""
+    and chi operand parts plus an error word, and a 16-byte aligned output;
+    a smaller scratch or a misaligned output is refused with a message."""
     from chimera_b200 import _native as N
     lib = N.lib()
     rows, nk, nR = 4096, 241, 200
@@ -81,6 +81,10 @@ def test_tensor_core_transform_sizes_its_scratch():
         need = lib.chx_ft_batch_scratch_bytes(rows, nk, nR, prec)
         rc = lib.chx_ft_batch(fake, rows, nk, fake, nR, prec, fake, fake, need - 1, None)
         assert rc == -1 and "scratch" in N.last_error()
+        # chi(R) is written by TMA tensor stores: out must be 16-byte aligned
+        odd = ctypes.c_void_p((1 << 20) + 8)
+        rc = lib.chx_ft_batch(fake, rows, nk, fake, nR, prec, odd, fake, need, None)
+        assert rc == -1 and "16-byte" in N.last_error()
     assert lib.chx_ft_batch(fake, rows, nk, fake, nR, 7, fake, fake, 0, None) == -1
 
 
