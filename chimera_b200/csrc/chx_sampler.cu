@@ -427,71 +427,71 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real
             *s_c2 = tot / L.nfit;
         }
         __syncthreads();
-        return;
-    }
-    // profiled chi^2, the reference's two passes (FP64)
-    for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
-        double nu = 0.0, dn = 0.0;
-        for (int q = lane; q < nwin; q += 32) {
-            real2 m = s_x[ch * nwin + q];
-            double tr = L.tm_re[ch * nwin + q];
-            if (L.cplx) {
-                double ti = L.tm_im[ch * nwin + q];
-                nu += (double)m.x * tr + (double)m.y * ti;
-                dn += (double)m.x * m.x + (double)m.y * m.y;
-            } else {
-                double mag = sqrt((double)m.x * m.x + (double)m.y * m.y);
-                nu += mag * tr;
-                dn += mag * mag;
-            }
-        }
-        nu = warp_sum(nu);
-        dn = warp_sum(dn);
-        if (lane == 0) {
-            s_num[ch] = nu;
-            s_den[ch] = dn;
-        }
-    }
-    __syncthreads();
-    if (tid < NSP) {
-        double s = 1.0;
-        if (L.profile) {
+    } else {
+        // profiled chi^2, the reference's two passes (FP64)
+        for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
             double nu = 0.0, dn = 0.0;
-            for (int q = 0; q < nkw; ++q) {
-                nu += s_num[tid * nkw + q];
-                dn += s_den[tid * nkw + q];
+            for (int q = lane; q < nwin; q += 32) {
+                real2 m = s_x[ch * nwin + q];
+                double tr = L.tm_re[ch * nwin + q];
+                if (L.cplx) {
+                    double ti = L.tm_im[ch * nwin + q];
+                    nu += (double)m.x * tr + (double)m.y * ti;
+                    dn += (double)m.x * m.x + (double)m.y * m.y;
+                } else {
+                    double mag = sqrt((double)m.x * m.x + (double)m.y * m.y);
+                    nu += mag * tr;
+                    dn += mag * mag;
+                }
             }
-            s = nu / fmax(dn, 1e-30);
-        }
-        s_scale[tid] = s;
-    }
-    __syncthreads();
-    for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
-        double s = s_scale[ch / nkw], acc = 0.0;
-        for (int q = lane; q < nwin; q += 32) {
-            real2 m = s_x[ch * nwin + q];
-            long g = (long)ch * nwin + q;
-            double sg = L.sm[g];
-            if (L.cplx) {
-                double dr = ((double)m.x * s - L.tm_re[g]) / sg;
-                double di = ((double)m.y * s - L.tm_im[g]) / sg;
-                acc += dr * dr + di * di;
-            } else {
-                double mag = sqrt((double)m.x * m.x + (double)m.y * m.y);
-                double dr = (mag * s - L.tm_re[g]) / sg;
-                acc += dr * dr;
+            nu = warp_sum(nu);
+            dn = warp_sum(dn);
+            if (lane == 0) {
+                s_num[ch] = nu;
+                s_den[ch] = dn;
             }
         }
-        acc = warp_sum(acc);
-        if (lane == 0) s_sq[ch] = acc;
+        __syncthreads();
+        if (tid < NSP) {
+            double s = 1.0;
+            if (L.profile) {
+                double nu = 0.0, dn = 0.0;
+                for (int q = 0; q < nkw; ++q) {
+                    nu += s_num[tid * nkw + q];
+                    dn += s_den[tid * nkw + q];
+                }
+                s = nu / fmax(dn, 1e-30);
+            }
+            s_scale[tid] = s;
+        }
+        __syncthreads();
+        for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
+            double s = s_scale[ch / nkw], acc = 0.0;
+            for (int q = lane; q < nwin; q += 32) {
+                real2 m = s_x[ch * nwin + q];
+                long g = (long)ch * nwin + q;
+                double sg = L.sm[g];
+                if (L.cplx) {
+                    double dr = ((double)m.x * s - L.tm_re[g]) / sg;
+                    double di = ((double)m.y * s - L.tm_im[g]) / sg;
+                    acc += dr * dr + di * di;
+                } else {
+                    double mag = sqrt((double)m.x * m.x + (double)m.y * m.y);
+                    double dr = (mag * s - L.tm_re[g]) / sg;
+                    acc += dr * dr;
+                }
+            }
+            acc = warp_sum(acc);
+            if (lane == 0) s_sq[ch] = acc;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double tot = 0.0;
+            for (int ch = 0; ch < L.nchan; ++ch) tot += s_sq[ch];
+            *s_c2 = tot / L.nfit;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    if (tid == 0) {
-        double tot = 0.0;
-        for (int ch = 0; ch < L.nchan; ++ch) tot += s_sq[ch];
-        *s_c2 = tot / L.nfit;
-    }
-    __syncthreads();
 }
 
 // Stage 1 of delayed acceptance for a swap of a and b (species differ),
