@@ -66,6 +66,13 @@ struct TcMode {
                          (size_t)parts * nkt * tileB + 1024
                    : (size_t)kTcStages * stage + 4 * 2 * kTcBox + 1024;
     }
+    // both layouts at their largest fit the 227 KB a CTA may opt into (less
+    // the static barriers)
+    static_assert((size_t)kTcStagesRes * stage_a + 4 * 2 * kTcBox +
+                          (size_t)parts * (kTcResKp / kTcK) * tileB + 1024 <= 232448 - 256,
+                  "resident-basis layout exceeds shared memory");
+    static_assert((size_t)kTcStages * stage + 4 * 2 * kTcBox + 1024 <= 232448 - 256,
+                  "streaming layout exceeds shared memory");
     // byte offset of element (r, k) inside one operand tile of kTcK values
     static __host__ __device__ __forceinline__ uint32_t off(int r, int k) {
         return (uint32_t)((r >> 3) * sbo + (k * esz / 16) * kTcLBO + (r & 7) * 16 +
