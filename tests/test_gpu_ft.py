@@ -85,3 +85,26 @@ def test_tensor_core_batch_wider_than_one_wave(cuda, precision):
             z = apply_basis(x, B, precision).cpu().numpy()
             assert np.abs(z - z0).max() <= TOL[precision] * scale, (rows, nb)
             assert (np.abs(z - z0)[big] / np.abs(z0)[big]).max() <= 50 * TOL[precision]
+
+
+@pytest.mark.parametrize("precision", [2, 3])
+def test_tensor_core_edge_shapes(cuda, precision):
+    """Shapes at the edges of the tensor-core path: one spectrum, rows one past
+    a 128-row tile, one and eight R points (2 and 16 real columns: a single
+    chi(R) box clipped in both directions), a short k grid (one 32-wide K
+    chunk) and nk = 257 (the smallest padded nk that streams the basis
+    instead of keeping it resident): each equals the FP64 contraction within
+    the precision's tolerance."""
+    import torch
+    from chimera_b200.fourier import apply_basis
+    rng = np.random.default_rng(23)
+    for rows, nk, nb in ((1, 241, 1), (129, 241, 8), (300, 20, 64), (257, 257, 100),
+                         (128, 256, 128)):
+        k = 2.0 + 0.05 * np.arange(nk)
+        B = np.exp(-2j * np.outer(k, 0.1 + 0.03 * np.arange(nb))) * (k ** 2)[:, None] * 0.05
+        chi = rng.normal(0, 1, (rows, nk)) * np.exp(-0.1 * k)[None]
+        x = torch.from_numpy(chi).cuda()
+        z0 = apply_basis(x, B, 0).cpu().numpy()
+        z = apply_basis(x, B, precision).cpu().numpy()
+        assert z.shape == (rows, nb)
+        assert np.abs(z - z0).max() <= TOL[precision] * np.abs(z0).max(), (rows, nk, nb)
