@@ -937,14 +937,25 @@ def main():
         smp2 = make_sampler(prob, rank)
         smp2.lad.threads, smp2.lad.min_blocks = smp.lad.threads, smp.lad.min_blocks
         smp2.init_state(sp0, prob.cell.ideal)
-        smp2.run_blocks(e2e_blocks)
+        # every exchange period's result, every ladder's best chi^2 so far,
+        # gathered and read back into pinned host memory (asynchronously, so
+        # that the replays stay queued back to back)
+        bests = [bb["best_chi2"] for lad in smp2.groups for bb in lad.bufs]
+        res_dev = torch.empty(sum(int(x.numel()) for x in bests), dtype=torch.float64,
+                              device="cuda")
+        res_host = torch.empty(res_dev.shape, dtype=torch.float64).pin_memory()
+        for _ in range(e2e_blocks):
+            smp2.run_blocks(1)
+            torch.cat(bests, out=res_dev)
+            res_host.copy_(res_dev, non_blocking=True)
+        per_period = res_dev.numel() * 8
     else:
-        smp2 = smp
+        smp2, per_period = smp, 0
     best = [smp2.best(li) for li in range(NPOS)]
     torch.cuda.synchronize()
     e2e_dt = time.perf_counter() - t0
     h2d = smp2.nslots * prob.cell.natoms * (4 + 24)
-    d2h = NPOS * (prob.cell.natoms * 4 + 8)
+    d2h = NPOS * (prob.cell.natoms * 4 + 8) + e2e_blocks * per_period
     e2e_val = smp2.nslots * EXCH * (e2e_blocks + 1) / e2e_dt
     err = smp.lad.device_error()
     # chi error vs FP64: the running FP32C chi of every replica against an
@@ -985,8 +996,9 @@ def main():
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": h2d / (e2e_blocks + 1),
                     "d2h_bytes_per_step": d2h / (e2e_blocks + 1),
-                    "note": "fresh sampler from host arrays: upload, init, run, best configs "
-                            "back; bytes amortised over the run's bench steps"},
+                    "note": "fresh sampler from host arrays: upload, init, run with every "
+                            "ladder's best chi^2 read back after each exchange period, best "
+                            "configs back at the end; bytes averaged over the bench steps"},
             "gpu_launches": args.steps * 2,
             "clocks": clocks,
             "device_error": err,
