@@ -884,9 +884,20 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 const int v = i < ms1 ? s_hist[i] : 0;
                 const unsigned m = __ballot_sync(0xffffffffu, v != 0);
                 if (v != 0) l_ms[off + __popc(m & ((1u << lane) - 1))] = make_int2(i, v);
+                // list position of each absorber block's first entry, by the
+                // warp whose run holds the block's first index
+                if (lane < NSP) {
+                    const int key = lane * L.ms_nblk, d = key - i0;
+                    if (d >= 0 && d < 32 && key < ms1)
+                        s_msb[lane] = off + __popc(m & ((1u << d) - 1));
+                }
                 off += __popc(m);
             }
-            if (warp == nwarp - 1 && lane == 0) s_nhist = off;
+            if (warp == nwarp - 1) {
+                if (lane == 0) s_nhist = off;
+                // the end of the last block; with no MS changes, every block empty
+                if (lane <= NSP && (lane == NSP || mseg == 0)) s_msb[lane] = off;
+            }
         }
         if (warp == 0) {
             int n = warp_compact(2 * maxaff, [&](int i) { return s_dirv[i] != 0; }, l_dir);
@@ -894,19 +905,6 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         } else if (warp == 1) {
             int n = warp_compact_pairs(ndn, s_dn, l_dn);
             if (lane == 0) s_ndn = n;
-        }
-        __syncthreads();
-        if (warp == 2) {   // first list position of each absorber block
-            const int n = s_nhist;
-            for (int a_ = lane; a_ <= NSP; a_ += 32) {
-                int lo = 0, hi = n, key = a_ * L.ms_nblk;
-                while (lo < hi) {
-                    int mid = (lo + hi) >> 1;
-                    if (l_ms[mid].x < key) lo = mid + 1;
-                    else hi = mid;
-                }
-                s_msb[a_] = lo;
-            }
         }
         __syncthreads();
 
