@@ -25,8 +25,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import configs
-from .fourier import FourierTransform
-from .multift import MultiEdgeFT
+from .fourier import EdgeTransforms
 
 ETOK = 0.2624682843
 
@@ -89,9 +88,8 @@ class Variant:
 
 
 def _fts(prob, k_model, kmin, kmax, kweights, window):
-    fts = [FourierTransform(k_model[e], kmin, kmax, w, window=window)
-           for e in range(prob.nsp) for w in kweights]
-    return MultiEdgeFT(fts, chan_edge=np.repeat(np.arange(prob.nsp), len(kweights)))
+    return EdgeTransforms.build([k_model[e] for e in range(prob.nsp)], kmin, kmax, kweights,
+                                window=window)
 
 
 def build_variants(base_kw, variants=CALIB_VARIANTS, window=None):

@@ -20,8 +20,7 @@ import numpy as np
 
 from . import lattice as L
 from . import mspaths as MP
-from .fourier import FourierTransform
-from .multift import MultiEdgeFT
+from .fourier import EdgeTransforms
 from .tables import smooth_tables, uniform_k
 
 
@@ -108,9 +107,8 @@ class Problem:
                                                self.tables.delta, self.tables.lam, sigma2,
                                                float(self.top.r_shell[0]),
                                                MP.length_unit(lattice, a0), s02=s02)
-        fts = [FourierTransform(self.k, kmin, kmax, w, window=window)
-               for e in range(self.nsp) for w in kweights]
-        self.ft = MultiEdgeFT(fts, chan_edge=np.repeat(np.arange(self.nsp), len(kweights)))
+        self.ft = EdgeTransforms.build(self.k, kmin, kmax, kweights, nsp=self.nsp,
+                                       window=window)
         self.mask = self.ft.window_mask(*rwin)
         self.noise = noise
         self.target_species = order_to_alpha(self.top, self.composition, alpha1, alpha_pair,

@@ -13,12 +13,16 @@
 // Host code cannot use the array's name as a device address (on the host it
 // names a host-side stand-in), so the first call on each device asks the
 // runtime for the array's device address (cudaGetSymbolAddress, with that
-// device current) and keeps it; later calls on that device reuse it. Because
+// device current) and keeps it; later calls on that device reuse it, so calls
+// must not span a reset of the device (the module may load elsewhere). Because
 // that first call may load the module, it should come before any stream
 // capture. All calls on a device share the one array and it keeps the last
 // call's contents: the error word that must start at zero is cleared by each
 // call, and calls that overlap on the GPU (different streams, or different
-// host threads) race on the array and must be serialised by the caller.
+// host threads) race on the array and must be serialised by the caller. The
+// error word sits in the array, where the caller cannot read it, so a device
+// error reaches the caller as NaN in every chi value of the call (the final
+// reduction of chx_chi_full checks the word).
 #include <mutex>
 #include "chx_common.cuh"
 

@@ -41,15 +41,24 @@ __global__ void k_pair_records(const double *__restrict__ pos, const int *__rest
         rec[tid] = PairRec{1.0, 0.0, 0.0, 0.0f, -1};
         return;
     }
+    int nsp = P.nsp, nn = nsp * nsp;
+    const int si = species[(long)ic * P.natoms + i], sj = species[(long)ic * P.natoms + j];
+    const int sh = P.shell[p];
+    // species and shell index the per-type tables: out of range, the pair is
+    // dropped (sentinel record) and the call's error word is set
+    if ((unsigned)si >= (unsigned)nsp || (unsigned)sj >= (unsigned)nsp ||
+        (unsigned)sh >= (unsigned)P.nshell) {
+        atomicOr(err, CHX_DEVERR_INDEX);
+        rec[tid] = PairRec{1.0, 0.0, 0.0, 0.0f, -1};
+        return;
+    }
     const double *pi = pos + ((long)ic * P.natoms + i) * 3;
     const double *pj = pos + ((long)ic * P.natoms + j) * 3;
     double dx = pj[0] + P.shift[3 * p + 0] - pi[0];
     double dy = pj[1] + P.shift[3 * p + 1] - pi[1];
     double dz = pj[2] + P.shift[3 * p + 2] - pi[2];
     double r = sqrt(dx * dx + dy * dy + dz * dz);
-    int nsp = P.nsp, nn = nsp * nsp;
-    int t = species[(long)ic * P.natoms + i] * nsp + species[(long)ic * P.natoms + j];
-    int sh = P.shell[p];
+    int t = si * nsp + sj;
     double reff = r + P.drtab[sh * nn + t];
     PairRec o;
     o.reff = reff;
@@ -139,10 +148,14 @@ __global__ void __launch_bounds__(512) k_pathsum(const PairRec *__restrict__ rec
     double acc[NSP];
 #pragma unroll
     for (int s = 0; s < NSP; ++s) acc[s] = 0.0;
+    int cfail = -1;   // the chunk whose wait ran out
     for (int ci = 0; ci < nch; ++ci) {
         if (!mbar_wait(&bar[ci & 1], (uint32_t)((ci >> 1) & 1))) s_fail = 1;
         __syncthreads();
-        if (s_fail) break;
+        if (s_fail) {
+            cfail = ci;
+            break;
+        }
         int n = min(kChunk, P.npairs - (c0 + ci) * kChunk);
         const PairRec *rr = ring[ci & 1];
         if (active) {
@@ -156,7 +169,14 @@ __global__ void __launch_bounds__(512) k_pathsum(const PairRec *__restrict__ rec
         if (threadIdx.x == 0 && ci + 2 < nch) issue(ci + 2);
     }
     if (s_fail) {
-        if (threadIdx.x == 0) atomicOr(err, CHX_DEVERR_INDEX);
+        if (threadIdx.x == 0) {
+            atomicOr(err, CHX_DEVERR_INDEX);
+            // before the CTA's shared memory is released, wait (bounded) for
+            // the copies that may still be in flight: the failed chunk and
+            // the one issued after it into the other ring slot
+            for (int c = cfail; c < min(nch, cfail + 2); ++c)
+                (void)mbar_wait(&bar[c & 1], (uint32_t)((c >> 1) & 1));
+        }
         return;
     }
     if (active) {
@@ -167,11 +187,19 @@ __global__ void __launch_bounds__(512) k_pathsum(const PairRec *__restrict__ rec
 }
 
 // chi[ic][s][k] = sum over CTAs (in order) of partial[ic][cta][s][k]
+// A call whose error word is set (an index out of range, or a bulk-copy wait
+// that ran out and left partials unwritten) writes NaN to every chi value, so
+// the failure shows in the output even where the caller cannot read the word.
 __global__ void k_reduce_partials(const double *__restrict__ partial, int ncta, int nsp, int nk,
-                                  int nconf, double *__restrict__ chi) {
+                                  int nconf, const int *__restrict__ err,
+                                  double *__restrict__ chi) {
     long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     long per = (long)nsp * nk;
     if (tid >= per * nconf) return;
+    if (*(volatile const int *)err != 0) {
+        chi[tid] = __longlong_as_double(0x7FF8000000000000LL);
+        return;
+    }
     int ic = (int)(tid / per);
     long sk = tid % per;
     const double *p = partial + (long)ic * ncta * per + sk;
@@ -355,7 +383,7 @@ int chx_chi_full(const chx_pairs_t *P, const double *pos, const int *species, in
     CHX_CHECK_LAUNCH("chi_full pathsum");
     long m = (long)nconf * P->nsp * P->nk;
     k_reduce_partials<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(partial, pl.ncta, P->nsp,
-                                                                   P->nk, nconf, chi);
+                                                                   P->nk, nconf, err, chi);
     CHX_CHECK_LAUNCH("chi_full reduce");
     return CHX_OK;
 }

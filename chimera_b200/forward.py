@@ -173,15 +173,20 @@ class ForwardModel:
             chi /= cnt.clamp(min=1).to(torch.float64)[:, :, None]
         return chi
 
-    def chi_full(self, pos, species, precision=FP64, out=None, max_scratch=1 << 30):
+    def chi_full(self, pos, species, precision=FP64, out=None, max_scratch=1 << 30,
+                 check=True):
         """Unnormalised path sum of every configuration (chx_chi_full),
-        batched so the pair-record scratch stays under max_scratch bytes."""
+        batched so the pair-record scratch stays under max_scratch bytes.
+        With check (the default) the device error word of each batch is read
+        back (one synchronisation) and a set word raises ChxError; a failed
+        batch's chi is NaN either way."""
         import torch
         nconf = pos.shape[0]
         if out is None:
             out = torch.empty((nconf, self.nsp, self.nk), dtype=torch.float64, device="cuda")
         P = self.pairs_desc()
         per = max(1, int(max_scratch // max(1, self.npairs * 40)))
+        words = []
         for c0 in range(0, nconf, per):
             c1 = min(nconf, c0 + per)
             n = c1 - c0
@@ -190,6 +195,13 @@ class ForwardModel:
             N.call("chx_chi_full", N.C.byref(P), N.ptr(pos[c0:c1].contiguous()),
                    N.ptr(species[c0:c1].contiguous()), n, int(precision),
                    N.ptr(out[c0:c1]), N.ptr(scr), need, N.stream())
+            if check:   # the error word: the int32 at need - 256
+                words.append(scr[need - 256:need - 252].view(torch.int32))
+        if words:
+            w = int(torch.cat(words).max().item())
+            if w:
+                raise N.ChxError(f"chx_chi_full: device error word {w:#x} (an index, species "
+                                 f"or shell out of range, or a bulk-copy wait that ran out)")
         return out
 
 

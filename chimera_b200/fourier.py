@@ -176,3 +176,82 @@ def apply_basis(chi, B, precision=0, Bd=None):
         raise N.ChxError("chx_ft_batch: the tensor-core contraction gave up a bounded wait")
     z = torch.view_as_complex(out.view(rows, nb, 2)).reshape(lead + (nb,))
     return z.cpu().numpy() if host else z
+
+
+class EdgeTransforms:
+    """The k -> R channels of a multi-edge fit, ordered edge-major: for each
+    absorber edge, one FourierTransform per k weight, all on one R grid.
+
+    Evaluation is one device contraction per edge: that edge's chi(k) rows
+    against the bases of all its channels laid side by side, (nk, nkw * nbins),
+    so a whole spectrum set costs nsp launches instead of one per channel.
+    An optional fixed chi_extra (nsp, nk) is added before transforming (the
+    composition-averaged multiple-scattering term of the reference's fits).
+
+    The samplers read the flat channel list `fts` and the channel -> edge map
+    `chan_edge`; the reference's own adapter (chimera/multift.py) exposes the
+    same two names, so either object can be handed to them."""
+
+    def __init__(self, per_edge, chi_extra=None):
+        per_edge = [list(ch) for ch in per_edge]
+        if not per_edge or any(not ch for ch in per_edge):
+            raise ValueError("every edge needs at least one channel")
+        self.per_edge = per_edge
+        self.fts = [f for ch in per_edge for f in ch]
+        self.nsp = len(per_edge)
+        self.nchan = len(self.fts)
+        self.chan_edge = np.repeat(np.arange(self.nsp, dtype=np.int32),
+                                   [len(ch) for ch in per_edge]).astype(np.int32)
+        self.R = np.asarray(self.fts[0].R)
+        if any(f.nfft != self.fts[0].nfft or f.dk != self.fts[0].dk for f in self.fts):
+            raise ValueError("all channels must share one R grid (nfft, dk)")
+        self.chi_extra = (None if chi_extra is None
+                          else np.ascontiguousarray(chi_extra, np.float64))
+        self._edge_dev = {}
+
+    @classmethod
+    def build(cls, k_axes, kmin, kmax, kweights, nsp=None, window="hanning", dk_win=1.0,
+              beta=4.0, chi_extra=None):
+        """Channels for every edge and k weight. k_axes: one model k axis for
+        all edges, or a list with one per edge (edges fitted with their own
+        E0 shift)."""
+        if isinstance(k_axes, (list, tuple)):
+            axes = [np.asarray(k, float) for k in k_axes]
+        else:
+            if nsp is None:
+                raise ValueError("nsp is needed with a single k axis")
+            axes = [np.asarray(k_axes, float)] * int(nsp)
+        per_edge = [[FourierTransform(k, kmin, kmax, w, dk_win=dk_win, window=window, beta=beta)
+                     for w in kweights] for k in axes]
+        return cls(per_edge, chi_extra=chi_extra)
+
+    def edge_basis(self, e, bins=None):
+        """Complex (nk, nkw * nbins): the edge's channels side by side."""
+        return np.concatenate([f.basis(bins) for f in self.per_edge[e]], axis=1)
+
+    def to_R(self, chi, bins=None, precision=0):
+        """chi (..., nsp, nk) -> complex chi(R) (..., nchan, nbins)."""
+        import torch
+        host = not (isinstance(chi, torch.Tensor) and chi.is_cuda)
+        x = torch.as_tensor(np.asarray(chi) if host else chi).to("cuda", torch.float64)
+        if self.chi_extra is not None:
+            x = x + torch.as_tensor(self.chi_extra, device="cuda")
+        key = None if bins is None else tuple(np.asarray(bins).tolist())
+        nb = self.fts[0].nfft // 2 if bins is None else len(key)
+        parts = []
+        for e, ch in enumerate(self.per_edge):
+            B = self.edge_basis(e, bins)
+            if (e, key) not in self._edge_dev:
+                self._edge_dev[(e, key)] = basis_to_device(B)
+            z = apply_basis(x[..., e, :].contiguous(), B, precision, Bd=self._edge_dev[(e, key)])
+            parts.append(z.reshape(z.shape[:-1] + (len(ch), nb)))
+        out = torch.cat(parts, dim=-2)
+        return out.cpu().numpy() if host else out
+
+    def window_mask(self, rmin, rmax):
+        return (self.R >= rmin) & (self.R <= rmax)
+
+    def n_independent(self, rmin, rmax):
+        kmin = min(f.kmin for f in self.fts)
+        kmax = max(f.kmax for f in self.fts)
+        return 2 * (kmax - kmin) * (rmax - rmin) / np.pi + 2

@@ -57,8 +57,10 @@ def _fp32_rows(t):
 
 
 def _ft_setup(ft, nsp):
-    """Per-channel window coefficients of a MultiEdgeFT-like object (or one
-    FourierTransform): n0, idx, frac, w padded to a common length."""
+    """Per-channel window coefficients of a channel set (fourier.EdgeTransforms,
+    the reference's chimera/multift.py adapter run through the cupy import
+    shim, or one FourierTransform): n0, idx, frac, w padded to a common
+    length."""
     fts = getattr(ft, "fts", None) or [ft]
     chan_edge = np.asarray(getattr(ft, "chan_edge", np.arange(len(fts))), np.int32)
     nkw = len(fts) // nsp

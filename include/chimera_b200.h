@@ -141,7 +141,11 @@ typedef struct {
 } chx_pairs_t;
 
 CHX_API int64_t chx_chi_full_scratch_bytes(const chx_pairs_t *P, int nconf);
-/* chi (nconf, nsp, nk) unnormalised; precision CHX_FP64 or CHX_FP32C */
+/* chi (nconf, nsp, nk) unnormalised; precision CHX_FP64 or CHX_FP32C.
+ * Device errors (an index, species or shell out of range; a bulk-copy wait
+ * that ran out) set the int32 error word at byte offset
+ * chx_chi_full_scratch_bytes(P, nconf) - 256 of the scratch, and make every
+ * chi value of the call NaN. */
 CHX_API int chx_chi_full(const chx_pairs_t *P, const double *pos, const int *species, int nconf,
                  int precision, double *chi, void *scratch, int64_t scratch_bytes,
                  void *stream);
@@ -155,8 +159,12 @@ CHX_API int chx_chi_full(const chx_pairs_t *P, const double *pos, const int *spe
  * the process exits; the call allocates nothing. Requests needing more
  * scratch than that are rejected with CHX_ERR_SCRATCH. The first call on a
  * device looks up the array's device address (and may load the module), so
- * make it before any stream capture. All calls on a device share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * make it before any stream capture. The address is kept per device for the
+ * life of the process, so calls must not span a reset of that device. All
+ * calls on a device share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller. The error word lives in the shared array,
+ * out of the caller's reach; a device error shows as NaN in every chi value
+ * of the call (as for chx_chi_full). */
 CHX_API int64_t chx_chi_full_noalloc_max_bytes(void);
 CHX_API int chx_chi_full_noalloc(const chx_pairs_t *P, const double *pos, const int *species,
                                  int nconf, int precision, double *chi, void *stream);

@@ -58,7 +58,7 @@ def device_objects(d, precision=0, reproduce=True, use_table=True):
     """(RMCSampler, ForwardModel) on the device for a golden trace."""
     from chimera_b200.forward import ForwardModel
     from chimera_b200.fourier import FourierTransform
-    from chimera_b200.multift import MultiEdgeFT
+    from chimera_b200.fourier import EdgeTransforms
     from chimera_b200.sampler import RMCSampler
     from chimera_b200.tables import ScatteringTables
     from chimera_b200 import mspaths as MP
@@ -69,13 +69,13 @@ def device_objects(d, precision=0, reproduce=True, use_table=True):
     fm = ForwardModel(cell, tabs, d["i"], d["j"], d["shift"], sigma2=d["sig2"], shell=d["shell"])
     nchan = d["ft_idx"].shape[0]
     nkw = nchan // nsp
-    fts = []
+    per_edge = [[] for _ in range(nsp)]
     for c in range(nchan):
         f = FourierTransform(d["ft_kmodel"][c], 3.0, 13.0, (1, 2, 3)[c % nkw])
         assert np.array_equal(f._idx, d["ft_idx"][c]) and np.array_equal(f._frac, d["ft_frac"][c])
         assert np.array_equal(f._w, d["ft_w"][c])
-        fts.append(f)
-    ft = MultiEdgeFT(fts, chan_edge=np.repeat(np.arange(nsp), nkw))
+        per_edge[c // nkw].append(f)
+    ft = EdgeTransforms(per_edge)
     ms = None
     if "ms_table_seed" in d:
         _, paths = ms_classes_paths(d, nsp)

@@ -1,6 +1,6 @@
 """Golden vectors of the systematic-band reduction, from the reference.
 
-    python tests/golden/make_band_golden.py [/path/to/reference]
+    python tests/golden/make_band_golden.py /path/to/reference   (or CHIMERA_REFERENCE=...)
 
 Runs the reference's own chimera.fitrun.band_from_variants (fitrun.py:491-536)
 on seeded synthetic variant rows (Warren-Cowley vectors, R-factors on the
@@ -17,7 +17,10 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_path  # noqa: E402
+
+REF = reference_path()
 sys.path.insert(0, os.path.join(HERE, "_stub"))
 sys.path.insert(0, REF)
 

@@ -1,9 +1,9 @@
 """Generate the golden vectors in tests/golden/ from the reference itself.
 
 Run in a container that has the reference checked out (its path is the first
-argument, default /root/reference):
+argument, or the CHIMERA_REFERENCE environment variable):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference   (or CHIMERA_REFERENCE=...)
 
 The reference's own Python modules are imported with `cupy` resolved to the
 NumPy stand-in in tests/golden/_stub (its RawModule runs the C oracle's
@@ -30,7 +30,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_path  # noqa: E402
+
+REF = reference_path()
 sys.path.insert(0, os.path.join(HERE, "_stub"))
 sys.path.insert(0, REPO)
 sys.path.insert(0, REF)
@@ -148,6 +151,17 @@ def fourier():
             out[key + "_norm"] = np.float64(ft._norm)
             out[key + "_chi"] = chi
             out[key + "_R256"] = z[:, :256]
+    # the reference's multi-edge adapter (chimera/multift.py) over its own
+    # channels: edge 0 on the model axis, edge 1 on an E0-shifted axis, k^1..k^3,
+    # with a fixed chi_extra added before the transform
+    per_edge = [[FourierTransform(grids[g], 3.0, 13.0, kw, dk_win=1.0, xp=np) for kw in (1, 2, 3)]
+                for g in ("model", "shifted")]
+    mft = MultiEdgeFT([f for ch in per_edge for f in ch], chan_edge=np.repeat(np.arange(2), 3),
+                      chi_extra=rng.normal(0, 0.01, (2, M.NKMODEL)))
+    mchi = rng.normal(0, 0.05, (3, 2, M.NKMODEL)) * np.sin(5 * grids["model"])
+    out["multi_chi"] = mchi
+    out["multi_extra"] = np.asarray(mft.chi_extra)
+    out["multi_R256"] = np.asarray(mft.to_R(mchi))[..., :256]
     ft = FourierTransform(grids["uniform"], 3.0, 13.0, 2, xp=np)
     out["R"] = ft.R
     out["mask_14_50"] = ft.window_mask(1.4, 5.0)

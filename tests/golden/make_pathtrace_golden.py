@@ -1,6 +1,6 @@
 """Golden vectors of the curved-wave path trace, from the reference.
 
-    python tests/golden/make_pathtrace_golden.py [/path/to/reference]
+    python tests/golden/make_pathtrace_golden.py /path/to/reference   (or CHIMERA_REFERENCE=...)
 
 Builds a `PhaseShifts` (exafs_gpu/abinitio/phaseshift.py:54-67) of two
 scatterer types with smooth synthetic complex phase shifts on 24 energies
@@ -19,7 +19,10 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_path  # noqa: E402
+
+REF = reference_path()
 sys.path.insert(0, os.path.join(HERE, "_stub"))
 sys.path.insert(0, REF)
 

@@ -1,9 +1,9 @@
 """Golden vectors of the pair-count calibration objective, from the reference.
 
-Run where the reference is checked out (its path is the first argument,
-default /root/reference):
+Run where the reference is checked out (its path is the first argument
+or the CHIMERA_REFERENCE environment variable):
 
-    python tests/golden/make_shellmodel_golden.py [/path/to/reference]
+    python tests/golden/make_shellmodel_golden.py /path/to/reference   (or CHIMERA_REFERENCE=...)
 
 It builds the reference's own `model.Spectrum` (fcc Fe-Ni, 4x4x4 cells,
 rmax 6.2 A, its analytic Z-parameterised tables, no multiple-scattering
@@ -27,7 +27,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_path  # noqa: E402
+
+REF = reference_path()
 sys.path.insert(0, os.path.join(HERE, "_stub"))
 sys.path.insert(0, REF)
 

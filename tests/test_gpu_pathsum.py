@@ -80,3 +80,24 @@ def test_ms_counts_delta_chi_of(cuda):
         ref = np.stack([g[key + "counts"][:, a * paths.nblk:(a + 1) * paths.nblk]
                         @ T[a * paths.nblk:(a + 1) * paths.nblk] for a in range(nsp)], axis=1)
         assert np.allclose(full, ref, rtol=0, atol=1e-12)
+
+
+def test_chi_full_reports_device_errors(cuda):
+    """Out-of-range species and pair indices are caught on the device: the
+    error word is set (ChxError from ForwardModel.chi_full) and chi is NaN."""
+    import torch
+    from chimera_b200 import _native as N
+    from chimera_b200.forward import FP64
+    g = golden("forward.npz")
+    fm = _fm(g, False)
+    sp = np.array(g["species"], np.int32).copy()
+    sp[0, 3] = fm.nsp
+    with pytest.raises(N.ChxError, match="error word"):
+        fm.chi_full(torch.from_numpy(np.asarray(g["pos"])).cuda(), torch.from_numpy(sp).cuda(),
+                    precision=FP64)
+    out = fm.chi_full(torch.from_numpy(np.asarray(g["pos"])).cuda(),
+                      torch.from_numpy(sp).cuda(), precision=FP64, check=False)
+    assert torch.isnan(out).all()
+    good = fm.chi_full(torch.from_numpy(np.asarray(g["pos"])).cuda(),
+                       torch.from_numpy(np.array(g["species"], np.int32)).cuda(), precision=FP64)
+    assert torch.isfinite(good).all()

@@ -76,3 +76,32 @@ def test_noalloc_refuses_requests_beyond_its_array(cuda):
                                       N.ptr(out), N.stream())
     assert rc == -4
     assert "fixed array" in N.last_error()
+
+
+def test_noalloc_reports_device_errors_as_nan(cuda):
+    """A species value outside the tables and a pair index beyond the cell are
+    caught on the device (no fault): the error word lives in the library's
+    array, so the call reports it as NaN in every chi value; the next good
+    call on the same array is clean again (each call clears the word)."""
+    torch = cuda
+    from chimera_b200 import _native as N
+    fm, pos, sp = _problem()
+    gpos = torch.from_numpy(pos).to("cuda")
+    nconf = pos.shape[0]
+    good = torch.from_numpy(sp.astype(np.int32)).to("cuda")
+    bad_sp = good.clone()
+    bad_sp[1, 7] = fm.nsp                     # one species beyond the tables
+    bad_i = fm.d_i.clone()
+    bad_i[5] = fm.natoms                      # one pair index beyond the cell
+    for gsp, iidx in ((bad_sp, None), (good, bad_i)):
+        Pb = fm.pairs_desc()
+        if iidx is not None:
+            Pb.iidx = N.dptr(iidx)
+        out = torch.zeros((nconf, fm.nsp, fm.nk), dtype=torch.float64, device="cuda")
+        N.call("chx_chi_full_noalloc", ctypes.byref(Pb), N.ptr(gpos), N.ptr(gsp), nconf, 0,
+               N.ptr(out), N.stream())
+        assert torch.isnan(out).all()
+        P = fm.pairs_desc()
+        N.call("chx_chi_full_noalloc", ctypes.byref(P), N.ptr(gpos), N.ptr(good), nconf, 0,
+               N.ptr(out), N.stream())
+        assert torch.isfinite(out).all()
