@@ -11,8 +11,9 @@ chi(R) fitted on 1.4-5.0 A; 16 sample positions (seeded noise) x 32 PT rungs =
 reduction and accumulation, FP64 re-anchoring every 1,000 accepted moves.
 
 One bench "step" is one exchange period: 25 sampler steps of every replica
-(one persistent fused launch) and one device replica exchange, replayed as a
-CUDA graph. value = swap attempts per second over all ranks. With --gpus N every
+(one persistent fused launch), one device replica exchange and the FP64
+re-anchoring of the slots that reached 1,000 accepted moves, replayed as a
+CUDA graph. The chains are aged by an untimed burn-in (--burnin) first. value = swap attempts per second over all ranks. With --gpus N every
 rank runs its own 16 ladders (weak scaling, no collective in the timed loop).
 
 --impl reference times the CPU restatement of the reference sampler (oracle/,
@@ -45,7 +46,8 @@ def workload_config():
                         "k^1/k^2/k^3 Kaiser complex chi(R) 1.4-5.0 A",
             "positions": NPOS, "rungs": NREP, "replicas_per_gpu": NPOS * NREP,
             "steps_per_bench_step": EXCH, "precision": "FP32 terms/transform, FP64 phase+accum",
-            "l2": "inputs larger than L2 (MS incidence records 205 MB per supercell)"}
+            "l2": "flushed between timed periods (256 MB write outside each period's "
+                  "CUDA events)"}
 
 
 def build_problem():
@@ -198,29 +200,38 @@ def cpu_baseline(prob, nsteps=40, nrep=NREP, p=0):
 
 
 def run_reference(args):
-    """--impl reference: the CPU restatement, one process per ladder."""
+    """--impl reference: the CPU restatement of the reference sampler, one
+    process per ladder on the host cores. A bench step is one exchange period
+    (25 sampler steps of every rung, then the exchange) when the whole
+    --warmup W --steps K run fits in about two minutes of host time, else a
+    bounded sample of fewer sampler steps per bench step; the rate (swap
+    attempts per second) is what is compared."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import multiprocessing as mp
     ncores = os.cpu_count() or 1
     nproc = max(1, min(NPOS, ncores))
-    steps = max(5, min(args.steps, 40))
+    W, K = max(0, args.warmup), max(1, args.steps)
+    per_step = max(1, min(EXCH, int(120.0 / (0.065 * (W + K)))))   # ~65 ms per sampler step
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(nproc) as pool:
-        res = pool.map(_ref_worker, [(p, steps) for p in range(nproc)])
+        res = pool.map(_ref_worker, [(p, W, K, per_step) for p in range(nproc)])
     wall = time.perf_counter() - t0
     attempts = sum(r["attempts"] for r in res)
     busy = max(r["seconds"] for r in res)
     val = attempts / busy
+    sample = (f"{nproc} ladders x {NREP} replicas, {per_step} sampler steps per bench step "
+              f"({'one exchange period' if per_step == EXCH else 'bounded sample'}), {W} "
+              f"untimed + {K} timed bench steps, one process per ladder (oracle C kernels + "
+              f"NumPy FFT)")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0,
-            "steps": steps, "warmup": 1, "ms_per_step": busy / steps * 1e3,
+            "steps": K, "warmup": W, "ms_per_step": busy / K * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": workload_config(),
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": nproc, "kind": "port",
-                             "sample": f"{nproc} ladders x {NREP} replicas x {steps} steps, one "
-                                       f"process per ladder (oracle C kernels + NumPy FFT)"},
+                             "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
     print(json.dumps(line), flush=True)
@@ -228,12 +239,27 @@ def run_reference(args):
 
 
 def _ref_worker(arg):
-    p, steps = arg
+    p, W, K, per_step = arg
     sys.path.insert(0, ROOT)
     os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from oracle import sampler as OS
     prob = build_problem()
-    r = cpu_baseline(prob, nsteps=steps, p=p)
-    return {"attempts": steps * NREP, "seconds": steps * NREP / r["value"]}
+    pr = oracle_problem(prob, p)
+    smp = OS.PlainSampler(pr, NREP, 1e-4, 1e-1, p, 1.0, 0.012, 0.10)
+    smp.init_state(prob.random_config(p), prob.cell.ideal)
+
+    def bench_step():
+        for _ in range(per_step):
+            smp.step()
+        smp.replica_exchange()
+
+    for _ in range(W):
+        bench_step()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        bench_step()
+    dt = time.perf_counter() - t0
+    return {"attempts": K * per_step * NREP, "seconds": dt}
 
 
 def bench_ft(args):
@@ -845,6 +871,12 @@ def main():
     ap.add_argument("--positions", type=int, default=16,
                     help="ladders per GPU (fewer for a small profiling case)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--burnin", type=int, default=2000,
+                    help="untimed exchange periods before tuning and timing (2,000 = 5e4 "
+                         "attempts per replica, the middle of the configuration's run)")
+    ap.add_argument("--e2e-periods", type=int, default=3999,
+                    help="exchange periods of the end-to-end run after its first (4,000 "
+                         "periods x 25 steps = the configuration's 1e5 attempts per replica)")
     ap.add_argument("--kernel", default="sampler",
                     choices=["sampler", "ft", "da", "uneven", "calib", "band", "pathtrace",
                              "pathsum"],
@@ -886,6 +918,14 @@ def main():
     rng = np.random.default_rng(rank)
     sp0 = [prob.random_config(int(rng.integers(1 << 30))) for _ in range(NPOS)]
     smp.init_state(sp0, prob.cell.ideal)
+    # clocks are sampled from the burn-in through the timed region (the timed
+    # periods alone are shorter than the sampling interval)
+    clk = Clocks(local).__enter__()
+    # untimed burn-in: the chains are aged to the middle of the configuration's
+    # run (displaced atoms accumulate and make later steps slower), then the
+    # launch shape is tuned on those states and the warm-up periods run
+    smp.capture()
+    smp.run_blocks(args.burnin)
     tuning = smp.autotune()
     smp.capture()
     smp.run_blocks(max(3, args.warmup))
@@ -896,14 +936,21 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     s = torch.cuda.current_stream()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        ev0.record(s)
-        smp.run_blocks(args.steps)
-        ev1.record(s)
-        ev1.synchronize()
+    # each exchange period is timed by its own pair of events; between
+    # periods a 256 MB write (twice the L2) flushes the cache, outside the
+    # events, so no period starts from the previous one's cached state
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for a, b in evs:
+        flush.fill_(1)
+        a.record(s)
+        smp.run_blocks(1)
+        b.record(s)
+    evs[-1][1].synchronize()
     torch.cuda.synchronize()
-    dt = ev0.elapsed_time(ev1) / 1e3
+    clk.__exit__(None, None, None)
+    dt = sum(a.elapsed_time(b) for a, b in evs) / 1e3
     if world > 1:
         t = torch.tensor([dt], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -929,14 +976,23 @@ def main():
         # DRAM bytes per replica-step from the capture, scaled to this launch
         traffic = t["dram_bytes_per_replica_step"] * smp.nslots * EXCH
 
-    # ---- end to end through the public API with host buffers
+    # ---- end to end through the public API with host buffers: the whole
+    # configuration's job (a fresh sampler from host arrays, 1e5 swap attempts
+    # per replica, every period's best chi^2 read back, the best states back)
     torch.cuda.synchronize()
-    e2e_blocks = max(4, args.steps // 4)
+    e2e_blocks = args.e2e_periods
+    phases = {}
     t0 = time.perf_counter()
     if not args.no_e2e:
         smp2 = make_sampler(prob, rank)
         smp2.lad.threads, smp2.lad.min_blocks = smp.lad.threads, smp.lad.min_blocks
+        phases["build_s"] = time.perf_counter() - t0
         smp2.init_state(sp0, prob.cell.ideal)
+        torch.cuda.synchronize()
+        phases["init_s"] = time.perf_counter() - t0 - sum(phases.values())
+        smp2.capture()
+        torch.cuda.synchronize()
+        phases["capture_s"] = time.perf_counter() - t0 - sum(phases.values())
         # every exchange period's result, every ladder's best chi^2 so far,
         # gathered and read back into pinned host memory (asynchronously, so
         # that the replays stay queued back to back)
@@ -949,14 +1005,18 @@ def main():
             torch.cat(bests, out=res_dev)
             res_host.copy_(res_dev, non_blocking=True)
         per_period = res_dev.numel() * 8
+        e2e_steps = smp2.nslots * EXCH * (e2e_blocks + 1)       # capture ran one period
     else:
-        smp2, per_period = smp, 0
+        smp2, per_period, e2e_steps = smp, 0, 0
     best = [smp2.best(li) for li in range(NPOS)]
     torch.cuda.synchronize()
     e2e_dt = time.perf_counter() - t0
-    h2d = smp2.nslots * prob.cell.natoms * (4 + 24)
+    phases["run_and_readback_s"] = e2e_dt - sum(phases.values())
+    # host -> device: one species array per ladder and the shared start
+    # positions; device -> host: the per-period best chi^2 and the best states
+    h2d = NPOS * prob.cell.natoms * 4 + prob.cell.natoms * 24
     d2h = NPOS * (prob.cell.natoms * 4 + 8) + e2e_blocks * per_period
-    e2e_val = smp2.nslots * EXCH * (e2e_blocks + 1) / e2e_dt
+    e2e_val = e2e_steps / e2e_dt if e2e_steps else None
     err = smp.lad.device_error()
     # chi error vs FP64: the running FP32C chi of every replica against an
     # FP64 recompute of its state (per absorber), after the timed run
@@ -996,10 +1056,13 @@ def main():
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": h2d / (e2e_blocks + 1),
                     "d2h_bytes_per_step": d2h / (e2e_blocks + 1),
-                    "note": "fresh sampler from host arrays: upload, init, run with every "
-                            "ladder's best chi^2 read back after each exchange period, best "
-                            "configs back at the end; bytes averaged over the bench steps"},
-            "gpu_launches": args.steps * 2,
+                    "periods": e2e_blocks + 1, "wall_s": e2e_dt, "phases": phases,
+                    "note": "the configuration's whole job from host arrays (1e5 swap "
+                            "attempts per replica): build, upload, init, capture, run with "
+                            "every ladder's best chi^2 read back after each exchange period, "
+                            "best configs back at the end; bytes averaged over its periods"},
+            "gpu_launches": args.steps * 4,
+            "burn_in_periods": args.burnin,
             "clocks": clocks,
             "device_error": err,
             "chi_err_vs_fp64": {"value": chi_err, "unit": "max |chi - chi_FP64| per absorber",

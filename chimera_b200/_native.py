@@ -123,7 +123,10 @@ _SIGS = {
     "chx_sampler_smem_bytes": ([c_p, c_i, c_i], c_i),
     "chx_shell_table": ([c_p, c_p, c_p, c_p, c_p], c_i),
     "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
-    "chx_reanchor": ([c_p, c_p, c_i, c_p, c_i, c_p, c_p, c_p], c_i),
+    "chx_reanchor_scratch_bytes": ([c_p, c_i, c_i], C.c_int64),
+    "chx_reanchor": ([c_p, c_p, c_i, c_p, c_i, c_p, c_p, C.c_int64, c_p, c_p], c_i),
+    "chx_reanchor_due": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_p, c_p, c_p, C.c_int64, c_p,
+                          c_p], c_i),
     "chx_replica_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_apply_exchange": ([c_p, c_i, c_p, c_p], c_i),
     "chx_ft_batch": ([c_p, c_i, c_i, c_p, c_i, c_i, c_p, c_p, c_i64, c_p], c_i),

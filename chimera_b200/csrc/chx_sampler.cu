@@ -1172,13 +1172,15 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
                                                            StepSmem so,
                                                            const double *__restrict__ chi_in,
                                                            const double *__restrict__ count_in,
-                                                           double *__restrict__ out) {
+                                                           double *__restrict__ out,
+                                                           const uint8_t *__restrict__ mask) {
     typedef typename Real<PREC>::T real;
     typedef typename Real<PREC>::T2 real2;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ chx_ladder_t L;
     __shared__ double s_num[32], s_den[32], s_sq[40], s_scale[8], s_c2;
     const int tid = threadIdx.x, slot = blockIdx.x;
+    if (mask && !mask[slot]) return;
     {
         const int *src = (const int *)&Ls[slot_ladder[slot]];
         int *dst = (int *)&L;
@@ -1198,7 +1200,10 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
     }
     __syncthreads();
     ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
-    if (tid == 0) out[slot] = s_c2;
+    if (tid == 0) {
+        if (out) out[slot] = s_c2;
+        else L.chi2[c] = s_c2;      // masked refresh: the slot's own chi^2
+    }
 }
 
 
@@ -1209,21 +1214,123 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
 // (shell, type) term table (the pair sum of the reference's pair-count model,
 // chimera/shellmodel.py:411-413, which equals the per-pair sum to rounding),
 // displaced pairs take the reference's FP64 term directly (kernels.py:22-29),
-// and the MS part is sum_e C_e T_e in FP64 (mslibrary.py:453-457). Only slots
-// with mask[slot] set are recomputed; their accepted-move counters are reset.
-constexpr int kReanchorChunk = 1024;   // pairs examined per round
+// and the MS part is sum_e C_e T_e in FP64 (mslibrary.py:453-457).
+//
+// The work of one slot is spread over the GPU: k_reanchor_select lists the
+// slots to re-anchor (a mask, every slot, or those whose accepted-move
+// counter reached a threshold, decided on the device), k_reanchor_part
+// computes one (listed slot, chunk of kRaChunk pairs) item per CTA into a
+// partial spectrum, and k_reanchor_fin sums a slot's partials in chunk order,
+// adds the MS part, writes chi and resets the slot's counter. Late in a run
+// displaced atoms make many pairs direct (each an FP64 exp and sin at every
+// k), which one CTA per slot would take milliseconds to evaluate.
+constexpr int kReanchorChunk = 1024;   // pairs examined per round of a CTA
+constexpr int kRaChunk = 1024;         // pairs per work item
+constexpr int kRaWindow = 64;          // slots per round of chx_reanchor
 
+struct RaScratch {
+    int *due_list, *due_count;
+    double *partial;
+};
+
+static int ra_nchunks(const chx_ladder_t *H, int nladders) {
+    int mx = 0;
+    for (int i = 0; i < nladders; ++i) mx = std::max(mx, (H[i].npairs + kRaChunk - 1) / kRaChunk);
+    return mx;
+}
+
+static size_t ra_partial_stride(const chx_ladder_t *H, int nladders) {
+    int nk = 0;
+    for (int i = 0; i < nladders; ++i) nk = std::max(nk, H[i].nk);
+    return (size_t)H[0].nsp * nk;
+}
+
+// partial spectra: per listed slot, its pair chunks then one MS item per
+// absorber block
+static int64_t ra_bytes(const chx_ladder_t *H, int nladders, int max_due) {
+    size_t b = 256 * (size_t)((max_due * sizeof(int) + 255) / 256) + 256;
+    b += sizeof(double) * (size_t)max_due * (ra_nchunks(H, nladders) + H[0].nsp) *
+         ra_partial_stride(H, nladders);
+    return (int64_t)b;
+}
+
+static RaScratch ra_carve(void *scratch, int max_due) {
+    RaScratch r;
+    char *p = (char *)scratch;
+    r.due_list = (int *)p;
+    p += 256 * ((max_due * sizeof(int) + 255) / 256);
+    r.due_count = (int *)p;
+    p += 256;
+    r.partial = (double *)p;
+    return r;
+}
+
+// One CTA: the listed slots of [slot_lo, slot_hi) in ascending order, at most
+// max_due of them (a due slot beyond the cap waits for the next call). mask
+// given: the masked slots; else every > 0: the slots whose counter reached
+// it; else all.
+__global__ void __launch_bounds__(1024) k_reanchor_select(const chx_ladder_t *__restrict__ Ls,
+                                                          const int *__restrict__ slot_ladder,
+                                                          int slot_lo, int slot_hi,
+                                                          const uint8_t *__restrict__ mask,
+                                                          int every, int max_due,
+                                                          uint8_t *__restrict__ due, RaScratch R,
+                                                          unsigned long long *__restrict__ count) {
+    __shared__ int s_warp[32], s_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_base = 0;
+    __syncthreads();
+    for (int s0 = slot_lo; s0 < slot_hi; s0 += blockDim.x) {
+        const int slot = s0 + tid;
+        bool go = false;
+        if (slot < slot_hi) {
+            if (mask) {
+                go = mask[slot] != 0;
+            } else if (every > 0) {
+                const chx_ladder_t *L = &Ls[slot_ladder[slot]];
+                go = L->n_acc[slot - L->slot0] >= every;
+            } else {
+                go = true;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, go);
+        if (lane == 0) s_warp[warp] = __popc(m);
+        __syncthreads();
+        int off = s_base;
+        for (int w = 0; w < warp; ++w) off += s_warp[w];
+        const int pos = off + __popc(m & ((1u << lane) - 1));
+        const bool take = go && pos < max_due;
+        if (take) R.due_list[pos] = slot;
+        if (due && slot < slot_hi) due[slot] = (uint8_t)take;
+        __syncthreads();
+        if (tid == 0) {
+            int tot = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += s_warp[w];
+            s_base += tot;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const int n = min(s_base, max_due);
+        *R.due_count = n;
+        if (count) *count += (unsigned long long)n;
+    }
+}
+
+// grid (max_due * (nchunks + NSP)): item = (listed slot di, ch), ch < nchunks a
+// chunk of kRaChunk pairs, ch = nchunks + a the MS part of absorber block a
 template <int NSP>
-__global__ void __launch_bounds__(256) k_reanchor(const chx_ladder_t *__restrict__ Ls,
-                                                  const int *__restrict__ slot_ladder,
-                                                  const uint8_t *__restrict__ mask,
-                                                  int *__restrict__ err) {
+__global__ void __launch_bounds__(256) k_reanchor_part(const chx_ladder_t *__restrict__ Ls,
+                                                       const int *__restrict__ slot_ladder,
+                                                       RaScratch R, int nchunks, int stride,
+                                                       int *__restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ chx_ladder_t L;
     __shared__ int s_ndir;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int slot = blockIdx.x;
-    if (mask && !mask[slot]) return;
+    const int di = blockIdx.x / (nchunks + NSP), ch = blockIdx.x - di * (nchunks + NSP);
+    if (di >= *(volatile const int *)R.due_count) return;
+    const int slot = R.due_list[di];
     {
         const int *src = (const int *)&Ls[slot_ladder[slot]];
         int *dst = (int *)&L;
@@ -1232,16 +1339,51 @@ __global__ void __launch_bounds__(256) k_reanchor(const chx_ladder_t *__restrict
     __syncthreads();
     const int c = slot - L.slot0;
     const int natoms = L.natoms, z = L.ncoord, nk = L.nk, nn = NSP * NSP;
+    if (ch >= nchunks) {
+        // the MS part of absorber block a: sum_e C_e T_e over its entries, in
+        // entry order, the counts staged in shared memory first
+        const int a = ch - nchunks, nblk = L.ms_nblk;
+        if (!nblk) return;                 // no MS: fin adds nothing
+        int *s_cnt = (int *)smem;
+        const int *C = L.ms_C + (long)c * NSP * nblk + (long)a * nblk;
+        for (int e = tid; e < nblk; e += blockDim.x) s_cnt[e] = C[e];
+        __syncthreads();
+        double *out = R.partial + ((long)di * (nchunks + NSP) + ch) * stride;
+        const double *T = L.ms_T + (long)a * nblk * nk;
+        for (int ik = tid; ik < nk; ik += blockDim.x) {
+            double acc = 0.0;
+#pragma unroll 8
+            for (int e = 0; e < nblk; ++e) {
+                const int n = s_cnt[e];
+                if (n) acc += (double)n * T[(long)e * nk + ik];
+            }
+            out[ik] = acc;
+        }
+        return;
+    }
+    const int p0 = ch * kRaChunk;
+    if (p0 >= L.npairs) return;            // beyond this ladder's pairs: fin skips it
+    const int p1 = min(L.npairs, p0 + kRaChunk);
     const int nbins = L.nshell * nn;
     const int nwarps = blockDim.x / 32;
-    int *s_hist = (int *)smem;                               // (nwarps, nbins)
-    int *s_dir = s_hist + nwarps * nbins;                    // direct pairs of a chunk
+    PairRec *s_rec = (PairRec *)smem;                        // direct pairs of a round
+    int *s_hist = (int *)(s_rec + kReanchorChunk);           // (nwarps, nbins)
+    int *s_dir = s_hist + nwarps * nbins;                    // their pair offsets
     uint8_t *s_flag = (uint8_t *)(s_dir + kReanchorChunk);   // 1: the pair is direct
     uint8_t *s_sp = s_flag + kReanchorChunk;                 // species | moved << 7
     const int *Sg = L.species + (long)c * natoms;
     const uint8_t *MVg = L.moved + (long)c * natoms;
     const double *P = L.pos + (long)c * natoms * 3;
     for (int q = tid; q < nwarps * nbins; q += blockDim.x) s_hist[q] = 0;
+    // the k-point constants of the (up to two) k points of this thread
+    KConst<NSP> kc[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int ik = tid + h * blockDim.x;
+        if (ik < nk) load_kconst<NSP>(kc[h], L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, ik);
+    }
+    // the species of the atoms this chunk's pairs touch: all of them (a chunk
+    // spans ~kRaChunk / z absorbers, but its neighbours reach anywhere)
     for (int i = tid; i < natoms; i += blockDim.x)
         s_sp[i] = (uint8_t)((Sg[i] & 0x7F) | (MVg[i] ? 0x80 : 0));
     __syncthreads();
@@ -1253,8 +1395,8 @@ __global__ void __launch_bounds__(256) k_reanchor(const chx_ladder_t *__restrict
     for (int h = 0; h < 2; ++h)
 #pragma unroll
         for (int s = 0; s < NSP; ++s) acc[h][s] = 0.0;
-    for (int c0 = 0; c0 < L.npairs; c0 += kReanchorChunk) {
-        const int n = min(kReanchorChunk, L.npairs - c0);
+    for (int c0 = p0; c0 < p1; c0 += kReanchorChunk) {
+        const int n = min(kReanchorChunk, p1 - c0);
         for (int q = tid; q < n; q += blockDim.x) {
             int p = c0 + q, i = p / z, j = L.jidx[p];
             uint8_t direct = 0;
@@ -1270,29 +1412,39 @@ __global__ void __launch_bounds__(256) k_reanchor(const chx_ladder_t *__restrict
             s_flag[q] = direct;
         }
         __syncthreads();
-        if (warp == 0) {                       // in-order list of the chunk's direct pairs
+        if (warp == 0) {                       // in-order list of the round's direct pairs
             int cnt = warp_compact(n, [&](int q) { return s_flag[q] != 0; }, s_dir);
             if (lane == 0) s_ndir = cnt;
         }
         __syncthreads();
         const int nd = s_ndir;
+        // one record per direct pair, built in parallel (geometry and the
+        // per-(shell, type) offsets: everything that does not depend on k)
+        for (int q = tid; q < nd; q += blockDim.x) {
+            const int p = c0 + s_dir[q];
+            const int i = p / z, j = L.jidx[p];
+            const double *sh3 = L.shift + 3 * (long)p;
+            const double *pi = P + 3 * (long)i, *pj = P + 3 * (long)j;
+            const double dx = pj[0] + sh3[0] - pi[0], dy = pj[1] + sh3[1] - pi[1],
+                         dz = pj[2] + sh3[2] - pi[2];
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            const int t = (s_sp[i] & 0x7F) * NSP + (s_sp[j] & 0x7F), sh = L.shell[p];
+            PairRec d;
+            d.reff = r + L.drtab[sh * nn + t];
+            d.s2 = L.sig2[p] + L.s2tab[sh * nn + t];
+            d.c3 = L.c3tab[sh];
+            d.inv_r2 = (float)(1.0 / (d.reff * d.reff));
+            d.t = t;
+            s_rec[q] = d;
+        }
+        __syncthreads();
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int ik = tid + h * blockDim.x;
             if (ik >= nk || nd == 0) continue;
-            KPoint kp{L.ktab[ik], L.lamtab[ik]};
             for (int q = 0; q < nd; ++q) {
-                int p = c0 + s_dir[q];
-                int i = p / z, j = L.jidx[p];
-                const double *sh3 = L.shift + 3 * (long)p;
-                const double *pi = P + 3 * (long)i, *pj = P + 3 * (long)j;
-                double dx = pj[0] + sh3[0] - pi[0], dy = pj[1] + sh3[1] - pi[1],
-                       dz = pj[2] + sh3[2] - pi[2];
-                double r = sqrt(dx * dx + dy * dy + dz * dz);
-                int t = (s_sp[i] & 0x7F) * NSP + (s_sp[j] & 0x7F);
-                add_by_species<NSP>(acc[h], t / NSP,
-                                    term64(r, t, L.shell[p], L.sig2[p], ik, nk, NSP, kp, L.ftab,
-                                           L.dtab, L.drtab, L.c3tab, L.s2tab, L.s02));
+                const PairRec d = s_rec[q];
+                add_by_species<NSP>(acc[h], d.t / NSP, rec_term<NSP, CHX_FP64>(d, kc[h]));
             }
         }
         __syncthreads();
@@ -1303,9 +1455,7 @@ __global__ void __launch_bounds__(256) k_reanchor(const chx_ladder_t *__restrict
         s_hist[bb] = v;
     }
     __syncthreads();
-    const int nent = L.ms_nblk ? NSP * L.ms_nblk : 0;
-    const int *C = L.ms_C + (long)c * nent;
-    double *CHg = L.chi + (long)c * NSP * nk;
+    double *out = R.partial + ((long)di * (nchunks + NSP) + ch) * stride;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const int ik = tid + h * blockDim.x;
@@ -1317,40 +1467,98 @@ __global__ void __launch_bounds__(256) k_reanchor(const chx_ladder_t *__restrict
                     add_by_species<NSP>(acc[h], (bb % nn) / NSP,
                                         (double)n * L.sstab[(long)bb * nk + ik]);
             }
-        for (int e = 0; e < nent; ++e) {
-            int n = C[e];
-            if (n) add_by_species<NSP>(acc[h], e / L.ms_nblk, (double)n * L.ms_T[(long)e * nk + ik]);
-        }
 #pragma unroll
-        for (int s = 0; s < NSP; ++s) CHg[s * nk + ik] = acc[h][s];
+        for (int s = 0; s < NSP; ++s) out[s * nk + ik] = acc[h][s];
     }
-    if (tid == 0) L.n_acc[c] = 0;
+}
+
+// grid (max_due): chi of listed slot di = its partials in chunk order + the
+// MS part; the slot's accepted-move counter restarts
+template <int NSP>
+__global__ void __launch_bounds__(256) k_reanchor_fin(const chx_ladder_t *__restrict__ Ls,
+                                                      const int *__restrict__ slot_ladder,
+                                                      RaScratch R, int nchunks, int stride) {
+    const int di = blockIdx.x;
+    if (di >= *(volatile const int *)R.due_count) return;
+    const int slot = R.due_list[di];
+    __shared__ chx_ladder_t L;
+    {
+        const int *src = (const int *)&Ls[slot_ladder[slot]];
+        int *dst = (int *)&L;
+        for (int q = threadIdx.x; q < (int)(sizeof(chx_ladder_t) / 4); q += blockDim.x)
+            dst[q] = src[q];
+    }
+    __syncthreads();
+    const int c = slot - L.slot0, nk = L.nk;
+    const int nch = (L.npairs + kRaChunk - 1) / kRaChunk;
+    double *CHg = L.chi + (long)c * NSP * nk;
+    const double *part = R.partial + (long)di * (nchunks + NSP) * stride;
+    for (int ik = threadIdx.x; ik < nk; ik += blockDim.x) {
+        double acc[NSP];
+#pragma unroll
+        for (int s = 0; s < NSP; ++s) acc[s] = 0.0;
+#pragma unroll 8
+        for (int q = 0; q < nch; ++q)
+#pragma unroll
+            for (int s = 0; s < NSP; ++s) acc[s] += part[(long)q * stride + s * nk + ik];
+        if (L.ms_nblk)                     // the MS items, one per absorber block
+#pragma unroll
+            for (int a = 0; a < NSP; ++a) acc[a] += part[(long)(nchunks + a) * stride + ik];
+#pragma unroll
+        for (int s = 0; s < NSP; ++s) CHg[s * nk + ik] = acc[s];
+    }
+    if (threadIdx.x == 0) L.n_acc[c] = 0;
 }
 
 // ------------------------------------------------------- replica exchange
 // One thread per ladder (method_a_rmc.py:332-373 with the uniforms from a
 // counter stream): rung pairs (i, i+1) from a random parity, d >= 0 or
 // u < exp(max(d, -60)); an accepted pair swaps which slots the two rungs hold.
-__global__ void k_exchange(const chx_ladder_t *__restrict__ Ls, int nladders,
-                           const uint64_t *__restrict__ round_key) {
-    int li = blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int kMaxExchRungs = 1024;
+
+// One CTA per ladder: the rungs' slots and the pairs' d are gathered in
+// parallel, one thread walks the pairs in order drawing a uniform only where
+// d < 0 (the order of the stream), and the accepted pairs are applied in
+// parallel (pairs of one parity touch disjoint rungs and slots).
+__global__ void __launch_bounds__(128) k_exchange(const chx_ladder_t *__restrict__ Ls,
+                                                  int nladders,
+                                                  const uint64_t *__restrict__ round_key) {
+    __shared__ int s_slot[kMaxExchRungs];
+    __shared__ double s_d[kMaxExchRungs];
+    __shared__ uint8_t s_ok[kMaxExchRungs];
+    __shared__ int s_start;
+    const int li = blockIdx.x, tid = threadIdx.x;
     if (li >= nladders) return;
-    uint64_t round = *(volatile const uint64_t *)round_key;
     const chx_ladder_t &L = Ls[li];
-    uint64_t h = splitmix64(splitmix64(L.seed ^ 0x5851F42D4C957F2DULL) ^
-                            (round * 0x9E3779B97F4A7C15ULL));
-    h = splitmix64(h);
-    int start = (u01(h) < 0.5) ? 0 : 1;
-    for (int i = start; i < L.nrep - 1; i += 2) {
-        int si = L.slot_of[i], sj = L.slot_of[i + 1];
-        double d = (L.beta_rung[i] - L.beta_rung[i + 1]) * (L.chi2[si] - L.chi2[sj]) * L.nfit;
-        bool ok = d >= 0.0;
-        if (!ok) {
-            h = splitmix64(h);
-            ok = u01(h) < exp(fmax(d, -60.0));
+    const int n = min(L.nrep, kMaxExchRungs);
+    for (int i = tid; i < n; i += blockDim.x) s_slot[i] = L.slot_of[i];
+    __syncthreads();
+    for (int i = tid; i < n - 1; i += blockDim.x)
+        s_d[i] = (L.beta_rung[i] - L.beta_rung[i + 1]) * (L.chi2[s_slot[i]] - L.chi2[s_slot[i + 1]]) *
+                 L.nfit;
+    __syncthreads();
+    if (tid == 0) {
+        const uint64_t round = *(volatile const uint64_t *)round_key;
+        uint64_t h = splitmix64(splitmix64(L.seed ^ 0x5851F42D4C957F2DULL) ^
+                                (round * 0x9E3779B97F4A7C15ULL));
+        h = splitmix64(h);
+        const int start = (u01(h) < 0.5) ? 0 : 1;
+        s_start = start;
+        for (int i = start; i < n - 1; i += 2) {
+            const double d = s_d[i];
+            bool ok = d >= 0.0;
+            if (!ok) {
+                h = splitmix64(h);
+                ok = u01(h) < exp(fmax(d, -60.0));
+            }
+            s_ok[i] = (uint8_t)ok;
         }
+    }
+    __syncthreads();
+    for (int i = s_start + 2 * tid; i < n - 1; i += 2 * blockDim.x) {
         L.exch_att[i] += 1;
-        if (ok) {
+        if (s_ok[i]) {
+            const int si = s_slot[i], sj = s_slot[i + 1];
             L.exch_acc[i] += 1;
             L.slot_of[i] = sj;
             L.slot_of[i + 1] = si;
@@ -1434,12 +1642,13 @@ static int launch_step(const chx_ladder_t *d_ladders, const int *slot_ladder, in
 template <int NSP, int PREC>
 static int launch_eval(const chx_ladder_t *d_ladders, const int *slot_ladder, int nslots,
                        const StepSmem &so, size_t smem, const double *chi_in,
-                       const double *count_in, double *out, cudaStream_t st) {
+                       const double *count_in, double *out, const uint8_t *mask,
+                       cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(k_eval_chi2<NSP, PREC>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(e, "eval_chi2 attribute");
     k_eval_chi2<NSP, PREC><<<nslots, kStepThreads, smem, st>>>(d_ladders, slot_ladder, so,
-                                                               chi_in, count_in, out);
+                                                               chi_in, count_in, out, mask);
     CHX_CHECK_LAUNCH("eval_chi2");
     return CHX_OK;
 }
@@ -1459,6 +1668,8 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
                         L.nkw <= 3 && L.nchan == L.nsp * L.nkw && (L.nfft & (L.nfft - 1)) == 0 &&
                         L.natoms < (1 << 20) && L.nwin > 0,
                     "sampler: ladder %d outside the built limits", i);
+        CHX_REQUIRE(L.nrep >= 1 && L.nrep <= kMaxExchRungs,
+                    "sampler: ladder %d has %d rungs (1..%d)", i, L.nrep, kMaxExchRungs);
         CHX_REQUIRE(!L.mlp || (L.da_on && L.da_stat),
                     "sampler: ladder %d has a surrogate but no da_on word or da_stat", i);
         CHX_REQUIRE(!(L.mlp || L.log_cap > 0) ||
@@ -1579,7 +1790,7 @@ int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladder
     if (rc != CHX_OK) return rc;
     cudaStream_t st = as_stream(stream);
     int nsp = host_ladders[0].nsp;
-#define CHX_EV(N, PR) launch_eval<N, PR>(d_ladders, slot_ladder, nslots, so, smem, chi_in, count_in, out, st)
+#define CHX_EV(N, PR) launch_eval<N, PR>(d_ladders, slot_ladder, nslots, so, smem, chi_in, count_in, out, nullptr, st)
     if (precision == CHX_FP64) {
         switch (nsp) {
             case 2: return CHX_EV(2, CHX_FP64);
@@ -1598,45 +1809,118 @@ int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladder
     return CHX_ERR_UNSUPPORTED;
 }
 
-int chx_reanchor(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders, int nladders,
-                 const int *slot_ladder, int nslots, const uint8_t *mask, int *d_err,
-                 void *stream) {
-    CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && d_err && nladders > 0 && nslots > 0,
-                "reanchor: bad arguments");
+static int reanchor_launch(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                           int nladders, const int *slot_ladder, int nslots, const uint8_t *mask,
+                           int every, int max_due, uint8_t *due, unsigned long long *count,
+                           void *scratch, int64_t scratch_bytes, int *d_err, cudaStream_t st) {
     int nsp = host_ladders[0].nsp;
     size_t smem = 0;
     for (int i = 0; i < nladders; ++i) {
         const chx_ladder_t &L = host_ladders[i];
         CHX_REQUIRE(L.nsp == nsp, "reanchor: one launch needs one species count");
         CHX_REQUIRE(L.nk <= 512, "reanchor: nk %d above 512", L.nk);
-        size_t b = sizeof(int) * ((size_t)8 * L.nshell * nsp * nsp + kReanchorChunk) +
+        size_t b = sizeof(PairRec) * kReanchorChunk +
+                   sizeof(int) * ((size_t)8 * L.nshell * nsp * nsp + kReanchorChunk) +
                    (size_t)kReanchorChunk + (size_t)L.natoms;
         smem = std::max(smem, b);
+        smem = std::max(smem, sizeof(int) * (size_t)L.ms_nblk);
     }
     CHX_REQUIRE(smem <= 200 * 1024, "reanchor: %zu bytes of shared memory needed", smem);
-    cudaStream_t st = as_stream(stream);
+    CHX_REQUIRE(max_due > 0 && max_due <= nslots, "reanchor: max_due %d outside 1..%d", max_due,
+                nslots);
+    const int64_t need = ra_bytes(host_ladders, nladders, max_due);
+    if (!scratch || scratch_bytes < need) {
+        set_error("reanchor: scratch of %lld bytes needed, %lld given", (long long)need,
+                  (long long)scratch_bytes);
+        return CHX_ERR_SCRATCH;
+    }
+    const RaScratch R = ra_carve(scratch, max_due);
+    const int nchunks = ra_nchunks(host_ladders, nladders);
+    const int stride = (int)ra_partial_stride(host_ladders, nladders);
+    const unsigned nitems = (unsigned)max_due * (unsigned)(nchunks + nsp);
+    // a threshold picks up to max_due slots of the whole batch per call; a
+    // mask (or every slot) is worked through in windows of max_due slots
+    const int win = every > 0 ? nslots : max_due;
+    for (int lo = 0; lo < nslots; lo += win) {
+        const int hi = std::min(nslots, lo + win);
+        k_reanchor_select<<<1, 1024, 0, st>>>(d_ladders, slot_ladder, lo, hi, mask, every,
+                                              max_due, due, R, count);
+        CHX_CHECK_LAUNCH("reanchor select");
 #define CHX_RA(N)                                                                              \
     do {                                                                                       \
-        cudaFuncSetAttribute(k_reanchor<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
+        cudaFuncSetAttribute(k_reanchor_part<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
                              (int)smem);                                                       \
-        k_reanchor<N><<<nslots, 256, smem, st>>>(d_ladders, slot_ladder, mask, d_err);          \
+        k_reanchor_part<N><<<nitems, 256, smem, st>>>(d_ladders, slot_ladder, R, nchunks,      \
+                                                      stride, d_err);                          \
+        CHX_CHECK_LAUNCH("reanchor part");                                                     \
+        k_reanchor_fin<N><<<max_due, 256, 0, st>>>(d_ladders, slot_ladder, R, nchunks, stride); \
     } while (0)
-    switch (nsp) {
-        case 2: CHX_RA(2); break;
-        case 3: CHX_RA(3); break;
-        case 4: CHX_RA(4); break;
-        default: set_error("reanchor: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
-    }
+        switch (nsp) {
+            case 2: CHX_RA(2); break;
+            case 3: CHX_RA(3); break;
+            case 4: CHX_RA(4); break;
+            default: set_error("reanchor: nsp %d not built", nsp); return CHX_ERR_UNSUPPORTED;
+        }
 #undef CHX_RA
-    CHX_CHECK_LAUNCH("reanchor");
+        CHX_CHECK_LAUNCH("reanchor fin");
+    }
     return CHX_OK;
+}
+
+int64_t chx_reanchor_scratch_bytes(const chx_ladder_t *host_ladders, int nladders, int max_due) {
+    if (!host_ladders || nladders <= 0 || max_due <= 0) return -1;
+    return ra_bytes(host_ladders, nladders, std::min(max_due, kRaWindow));
+}
+
+int chx_reanchor(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders, int nladders,
+                 const int *slot_ladder, int nslots, const uint8_t *mask, void *scratch,
+                 int64_t scratch_bytes, int *d_err, void *stream) {
+    CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && d_err && nladders > 0 && nslots > 0,
+                "reanchor: bad arguments");
+    return reanchor_launch(d_ladders, host_ladders, nladders, slot_ladder, nslots, mask, 0,
+                           std::min(nslots, kRaWindow), nullptr, nullptr, scratch, scratch_bytes,
+                           d_err, as_stream(stream));
+}
+
+int chx_reanchor_due(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                     int nladders, const int *slot_ladder, int nslots, int every, int max_due,
+                     int precision, uint8_t *due, unsigned long long *count, void *scratch,
+                     int64_t scratch_bytes, int *d_err, void *stream) {
+    CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && d_err && due && nladders > 0 &&
+                    nslots > 0 && every > 0,
+                "reanchor_due: bad arguments");
+    cudaStream_t st = as_stream(stream);
+    int rc = reanchor_launch(d_ladders, host_ladders, nladders, slot_ladder, nslots, nullptr,
+                             every, max_due, due, count, scratch, scratch_bytes, d_err, st);
+    if (rc != CHX_OK) return rc;
+    StepSmem so;
+    size_t smem = 0;
+    rc = plan_ladders(host_ladders, nladders, precision, &so, &smem);
+    if (rc != CHX_OK) return rc;
+    int nsp = host_ladders[0].nsp;
+#define CHX_EV(N, PR) launch_eval<N, PR>(d_ladders, slot_ladder, nslots, so, smem, nullptr, nullptr, nullptr, due, st)
+    if (precision == CHX_FP64) {
+        switch (nsp) {
+            case 2: return CHX_EV(2, CHX_FP64);
+            case 3: return CHX_EV(3, CHX_FP64);
+            case 4: return CHX_EV(4, CHX_FP64);
+        }
+    } else {
+        switch (nsp) {
+            case 2: return CHX_EV(2, CHX_FP32C);
+            case 3: return CHX_EV(3, CHX_FP32C);
+            case 4: return CHX_EV(4, CHX_FP32C);
+        }
+    }
+#undef CHX_EV
+    set_error("reanchor_due: nsp %d not built", nsp);
+    return CHX_ERR_UNSUPPORTED;
 }
 
 int chx_replica_exchange(const chx_ladder_t *d_ladders, int nladders, const uint64_t *round_key,
                          void *stream) {
     CHX_REQUIRE(d_ladders && round_key && nladders > 0, "replica_exchange: bad arguments");
-    k_exchange<<<(nladders + 63) / 64, 64, 0, as_stream(stream)>>>(d_ladders, nladders,
-                                                                    round_key);
+    k_exchange<<<nladders, 128, 0, as_stream(stream)>>>(d_ladders, nladders, round_key);
     CHX_CHECK_LAUNCH("replica_exchange");
     return CHX_OK;
 }

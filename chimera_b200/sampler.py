@@ -56,6 +56,15 @@ def _fp32_rows(t):
     return out
 
 
+def _on_device(x, dtype):
+    """x as a contiguous CUDA tensor of dtype (one host->device copy, none
+    for a device tensor of that type)."""
+    import torch
+    if isinstance(x, torch.Tensor):
+        return x.to("cuda", dtype).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(x)).to("cuda", dtype)
+
+
 def _ft_setup(ft, nsp):
     """Per-channel window coefficients of a channel set (fourier.EdgeTransforms,
     the reference's chimera/multift.py adapter run through the cupy import
@@ -151,9 +160,14 @@ class Ladders:
         """Per-supercell device data shared by every ladder on the same
         ForwardModel: reverse pair index, ideal sites, shifts, sigma^2, the
         pairs that may use the (shell, type) table and the shell radii."""
-        cache = self.__dict__.setdefault("_cell_cache", {})
-        key = id(fm)
-        if key in cache:
+        # kept on the forward model, so every sampler built on it shares the
+        # host-side work and the device arrays
+        # (an entry is valid while the model's geometry and cumulant tables
+        # are the same tensors: set_dr/set_c3/set_sig2_types replace them)
+        cache = fm.__dict__.setdefault("_ladder_cell_cache", {})
+        key = "cell"
+        src = (fm.d_shift, fm.d_sig2, fm.d_dr, fm.d_c3, fm.d_s2tab)
+        if key in cache and all(a is b for a, b in zip(cache[key]["src"], src)):
             return cache[key]
         i_np, j_np = fm.i_idx, fm.j_idx
         natoms = fm.natoms
@@ -174,7 +188,7 @@ class Ladders:
         pair_tab = ((np.abs(d0 - r_shell[shell]) <= 1e-12 * r_shell[shell])
                     & (sig2 == s2_shell[shell]))
         pair_tab = (pair_tab & pair_tab[rev]).astype(np.uint8)   # a pair and its reverse agree
-        c = dict(ncoord=ncoord, r_shell=r_shell, s2_shell=s2_shell, fm=fm,
+        c = dict(ncoord=ncoord, r_shell=r_shell, s2_shell=s2_shell, src=src,
                  dev=dict(rev=self._t(rev), ideal=self._t(ideal), shift=self._t(shift),
                           sig2=self._t(sig2), pair_tab=self._t(pair_tab)))
         cache[key] = c
@@ -246,7 +260,10 @@ class Ladders:
         else:
             L.etab, L.energy_beta = 0, 0.0
         # transform and target (the set-up once per transform object)
-        fcache = self.__dict__.setdefault("_ft_cache", {})
+        try:        # kept on the transform object when it allows attributes
+            fcache = s.ft.__dict__.setdefault("_ladder_ft_cache", {})
+        except AttributeError:
+            fcache = self.__dict__.setdefault("_ft_cache", {})
         if id(s.ft) not in fcache:
             f = _ft_setup(s.ft, nsp)
             fcache[id(s.ft)] = (s.ft, f, dict(ft_n0=self._t(f["n0"]), ft_idx=self._t(f["idx"]),
@@ -342,12 +359,14 @@ class Ladders:
         s, b = self.specs[li], self.bufs[li]
         fm = s.fm
         nrep = s.nrep
-        sp = np.repeat(np.asarray(species0, np.int32)[None], nrep, 0)
-        pos = np.repeat(np.asarray(pos0, np.float64)[None], nrep, 0)
-        b["species"].copy_(torch.from_numpy(sp))
-        b["pos"].copy_(torch.from_numpy(pos))
-        ideal = _host(fm.cell.ideal)
-        b["moved"].copy_(torch.from_numpy(np.any(pos != ideal[None], axis=-1).astype(np.uint8)))
+        # one copy of the start state crosses to the device (a device tensor
+        # is used as it is) and is broadcast to every rung there
+        dsp = _on_device(species0, torch.int32)
+        dpos = _on_device(pos0, torch.float64)
+        b["species"].copy_(dsp[None].expand(nrep, -1))
+        b["pos"].copy_(dpos[None].expand(nrep, -1, -1))
+        ideal = self._supercell(fm)["dev"]["ideal"]
+        b["moved"].copy_((dpos != ideal).any(dim=-1).to(torch.uint8)[None].expand(nrep, -1))
         # every rung starts from the same configuration: evaluate it once
         if s.ms is not None:
             C_ = s.ms.counts(b["species"][:1].contiguous())
@@ -361,8 +380,8 @@ class Ladders:
             if s.ms is not None:
                 chi = chi + s.ms.chi_of(C_)
             b["chi"].copy_(chi.expand(nrep, -1, -1))
-        cnt = np.stack([(sp == q).sum(1) for q in range(self.nsp)], axis=1).astype(np.float64)
-        b["count"].copy_(torch.from_numpy(cnt))
+        cnt = torch.bincount(dsp.long(), minlength=self.nsp)[:self.nsp].to(torch.float64)
+        b["count"].copy_(cnt[None].expand(nrep, -1))
         b["rung_of"].copy_(torch.arange(nrep, dtype=torch.int32))
         b["slot_of"].copy_(torch.arange(nrep, dtype=torch.int32))
         b["acc"].zero_()
@@ -400,10 +419,13 @@ class Ladders:
         torch = self.torch
         if self.use_table:
             m = None if mask is None else torch.as_tensor(mask).to("cuda", torch.uint8).contiguous()
+            need = int(N.lib().chx_reanchor_scratch_bytes(C.byref(self.host), self.nladders,
+                                                          self.nslots))
+            scr = torch.empty(need, dtype=torch.uint8, device="cuda")
             N.call("chx_reanchor", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
                    N.ptr(self.slot_ladder), self.nslots, N.ptr(m) if m is not None else None,
-                   N.ptr(self.err), N.stream())
-            self._reanchor_mask = m
+                   N.ptr(scr), need, N.ptr(self.err), N.stream())
+            self._reanchor_keep = (m, scr)      # alive until the launches have run
         else:
             for s, b in zip(self.specs, self.bufs):
                 chi = s.fm.chi_full(b["pos"], b["species"], precision=FP64)
@@ -424,6 +446,31 @@ class Ladders:
             s0 = self.host[li].slot0
             mask[s0:s0 + self.specs[li].nrep] = True
         self.reanchor(mask)
+
+    def reanchor_due(self, every):
+        """Re-anchor, inside the current stream (capturable), every slot
+        whose accepted-move counter reached `every`: the device decides
+        (chx_reanchor_due), recomputes those slots' chi in FP64, refreshes
+        their chi^2 and counts them in `self.reanchor_count`."""
+        torch = self.torch
+        if getattr(self, "due", None) is None:
+            self.due = torch.zeros(self.nslots, dtype=torch.uint8, device="cuda")
+            self.reanchor_count = torch.zeros(1, dtype=torch.int64, device="cuda")
+            # at most this many slots per period (the rest follow a period
+            # later); the batch workload averages about two
+            self.max_due = min(self.nslots, int(getattr(self, "reanchor_cap", 8)))
+            need = int(N.lib().chx_reanchor_scratch_bytes(C.byref(self.host), self.nladders,
+                                                          self.max_due))
+            self.ra_scratch = torch.empty(need, dtype=torch.uint8, device="cuda")
+        N.call("chx_reanchor_due", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
+               N.ptr(self.slot_ladder), self.nslots, int(every), self.max_due, self.precision,
+               N.ptr(self.due), N.ptr(self.reanchor_count), N.ptr(self.ra_scratch),
+               int(self.ra_scratch.numel()), N.ptr(self.err), N.stream())
+
+    def slot_reanchors(self):
+        """Slots re-anchored on the device so far (chx_reanchor_due)."""
+        rc = getattr(self, "reanchor_count", None)
+        return 0 if rc is None else int(rc.item())
 
     def accepted_since_anchor(self):
         """(nslots,) accepted moves since each slot's last re-anchoring."""
@@ -815,7 +862,11 @@ class BatchedSampler:
     """Many independent ladders in one launch per step, replayed as CUDA
     graphs (one graph = `exchange_every` steps + a device replica exchange),
     with FP64 re-anchoring of the running chi every `reanchor_every`
-    accepted moves (checked every `check_every` blocks).
+    accepted moves. By default (`device_reanchor`) the re-anchoring is part of
+    every exchange period's graph: the device re-anchors the slots whose
+    counter reached the threshold (at most `reanchor_cap` per period, the
+    rest a period later), with no host round trip; otherwise the host checks
+    the counters every `check_every` blocks.
 
     The step kernel is compiled per species count, so a batch that mixes
     binaries and ternaries is held as one group of ladders per count (in order
@@ -826,7 +877,8 @@ class BatchedSampler:
     `specs`)."""
 
     def __init__(self, specs, precision=FP32C, exchange_every=25, use_table=True,
-                 reanchor_every=1000, check_every=40, threads=256, min_blocks=3):
+                 reanchor_every=1000, check_every=40, threads=256, min_blocks=3,
+                 device_reanchor=True, reanchor_cap=8):
         import torch
         self.torch = torch
         specs = list(specs)
@@ -847,9 +899,12 @@ class BatchedSampler:
         self.exchange_every = int(exchange_every)
         self.reanchor_every = int(reanchor_every)
         self.check_every = int(check_every)
+        self.device_reanchor = bool(device_reanchor) and self.reanchor_every > 0
+        for lad in self.groups:     # slots re-anchored per period at most
+            lad.reanchor_cap = int(reanchor_cap)
         self.graph = None
         self.blocks = 0
-        self.reanchors = 0
+        self.host_reanchors = 0
         self.steps = 0
 
     @property
@@ -874,7 +929,14 @@ class BatchedSampler:
         return sum(g.nslots for g in self.groups)
 
     def init_state(self, species0, pos0):
-        """species0 / pos0: one array per ladder (or one shared by all)."""
+        """species0 / pos0: one array per ladder (or one shared by all, then
+        copied to the device once)."""
+        from .forward import _dev
+        torch = self.torch
+        if not isinstance(species0, (list, tuple)):
+            species0 = _dev(species0, torch.int32)
+        if not isinstance(pos0, (list, tuple)):
+            pos0 = _dev(pos0, torch.float64)
         for li in range(self.nladders):
             sp = species0[li] if isinstance(species0, (list, tuple)) else species0
             ps = pos0[li] if isinstance(pos0, (list, tuple)) else pos0
@@ -901,12 +963,24 @@ class BatchedSampler:
             e |= lad.device_error()
         return e
 
+    @property
+    def reanchors(self):
+        """Re-anchorings so far: slots re-anchored in the graph (device
+        counters) plus host-side re-anchor launches."""
+        return sum(lad.slot_reanchors() for lad in self.groups) + self.host_reanchors
+
+    def _period(self, lad):
+        lad.step(self.exchange_every)
+        lad.exchange_device()
+        if self.device_reanchor:
+            lad.reanchor_due(self.reanchor_every)
+
     def block(self):
         """One exchange period: exchange_every steps in one launch, then the
-        device exchange (per group, the groups on parallel streams)."""
+        device exchange and the due re-anchorings (per group, the groups on
+        parallel streams)."""
         if len(self.groups) == 1:
-            self.groups[0].step(self.exchange_every)
-            self.groups[0].exchange_device()
+            self._period(self.groups[0])
             return
         torch = self.torch
         if self._streams is None:
@@ -915,8 +989,7 @@ class BatchedSampler:
         for lad, st in zip(self.groups, self._streams):
             st.wait_stream(cur)
             with torch.cuda.stream(st):
-                lad.step(self.exchange_every)
-                lad.exchange_device()
+                self._period(lad)
         for st in self._streams:
             cur.wait_stream(st)
 
@@ -943,12 +1016,12 @@ class BatchedSampler:
             self.blocks += 1
             self.steps += self.exchange_every
             if self.blocks % self.check_every == 0:
-                if self.reanchor_every:
+                if self.reanchor_every and not self.device_reanchor:
                     for lad in self.groups:
                         due = lad.accepted_since_anchor() >= self.reanchor_every
                         if bool(due.any()):
                             lad.reanchor(due)
-                            self.reanchors += 1
+                            self.host_reanchors += 1
                 if self.surrogate is not None:
                     self._check_screen()
 

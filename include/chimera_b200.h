@@ -390,11 +390,28 @@ CHX_API int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *hos
  * recompute from its species, positions and MS entry counts, in the
  * pair-count form (pairs on ideal sites counted per (shell, type) and
  * contracted with the FP64 term table sstab; displaced pairs by the FP64 pair
- * term, visited in fixed order), and reset its accepted-move counter. Uses
- * the counted form where sstab is set; nk <= 512. */
+ * term), and reset its accepted-move counter. Uses the counted form where
+ * sstab is set; nk <= 512. The work of a slot is spread over the GPU in
+ * chunks of 1,024 pairs whose partial spectra are summed in chunk order
+ * (deterministic); scratch (caller-owned) is sized by
+ * chx_reanchor_scratch_bytes(host_ladders, nladders, max_due) with
+ * max_due = nslots for chx_reanchor. */
+CHX_API int64_t chx_reanchor_scratch_bytes(const chx_ladder_t *host_ladders, int nladders,
+                                           int max_due);
 CHX_API int chx_reanchor(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
                          int nladders, const int *slot_ladder, int nslots, const uint8_t *mask,
-                         int *d_err, void *stream);
+                         void *scratch, int64_t scratch_bytes, int *d_err, void *stream);
+/* The same re-anchoring decided on the device, for use inside a captured
+ * exchange period: the slots whose accepted-move counter reached `every`
+ * (config 1: 1,000), at most max_due of them per call in slot order (the rest
+ * wait for the next call), are recomputed in FP64 as above and their chi^2
+ * refreshed in `precision`; due[slot] (device, nslots bytes) records which,
+ * and the device counter *count (may be NULL) grows by their number.
+ * No counterpart in the reference (closest: method_a_rmc.py:436-448). */
+CHX_API int chx_reanchor_due(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                             int nladders, const int *slot_ladder, int nslots, int every,
+                             int max_due, int precision, uint8_t *due, unsigned long long *count,
+                             void *scratch, int64_t scratch_bytes, int *d_err, void *stream);
 
 /* Replica exchange decided on the device (method_a_rmc.py:332-373): alternate
  * adjacent rung pairs from a random start parity, accept d >= 0 or

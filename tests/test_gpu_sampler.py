@@ -294,3 +294,35 @@ def test_systematic_band_variants_in_one_launch_equal_separate_runs(cuda):
     band = B.band_from_variants(rows)
     assert band["excluded_incomparable"] == ["k weight 2"]
     assert all(np.isfinite(r["r_factor"]) and len(r["wc"]) == 3 for r in rows)
+
+
+def test_device_reanchoring_equals_host_reanchoring(cuda):
+    """Re-anchoring decided on the device inside each exchange period's graph
+    (chx_reanchor_due, its per-period cap at the slot count) re-anchors exactly
+    the slots the host-side check finds due after the same period, so the
+    chains are identical bit for bit; the device counter counts the
+    re-anchored slots."""
+    from chimera_b200 import configs
+    from chimera_b200.sampler import BatchedSampler, LadderSpec
+    prob = configs.Problem(ncell=(5, 5, 5), ms=True)
+    specs = []
+    for p in range(2):
+        pos = prob.position(p)
+        specs.append(LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R, nrep=8,
+                                tmin=1e-3, tmax=1e-1, seed=p, swap_frac=0.98,
+                                ms_library=prob.ms))
+    init = [prob.random_config(40 + p) for p in range(2)]
+    out = []
+    for dev in (True, False):
+        bs = BatchedSampler(specs, precision=1, exchange_every=25, reanchor_every=6,
+                            check_every=1, device_reanchor=dev, reanchor_cap=16)
+        bs.init_state(init, prob.cell.ideal)
+        bs.run_blocks(10)
+        assert bs.lad.device_error() == 0
+        keys = ("species", "chi", "chi2", "n_acc", "best_chi2", "rung_of")
+        out.append(({(li, k): bb[k].cpu().numpy().copy() for li, bb in enumerate(bs.lad.bufs)
+                     for k in keys}, bs))
+    (a, bs_dev), (b, bs_host) = out
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert bs_dev.reanchors > 0 and bs_host.host_reanchors > 0
