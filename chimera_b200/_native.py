@@ -66,7 +66,9 @@ class Ladder(C.Structure):
         ("best_sp", c_p), ("best_pos", c_p), ("ms_C", c_p), ("acc_rung", c_p), ("acc_log", c_p), ("n_acc", c_p),
         ("exch_att", c_p), ("exch_acc", c_p),
         ("mlp", c_p), ("feat_nbr", c_p), ("feat_D", c_i), ("da_on", c_p), ("da_stat", c_p),
-        ("log_codes", c_p), ("log_y", c_p), ("log_cap", c_i64), ("best_stale", c_p)]
+        ("log_codes", c_p), ("log_y", c_p), ("log_cap", c_i64), ("best_stale", c_p),
+        ("xr", c_p), ("tie_eps", c_d), ("tie_stat", c_p), ("sstab_max", c_p), ("ms_T_max", c_p),
+        ("tie_gain", c_d)]
 
 
 class Mlp(C.Structure):
@@ -123,6 +125,8 @@ _SIGS = {
     "chx_sampler_smem_bytes": ([c_p, c_i, c_i], c_i),
     "chx_shell_table": ([c_p, c_p, c_p, c_p, c_p], c_i),
     "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
+    "chx_pair_counts": ([c_p, c_i, c_i, c_p, c_p, c_i, c_i, c_p, c_p, c_p], c_i),
+    "chx_refresh_chi2": ([c_p, c_p, c_i, c_p, c_i, c_i, c_p, c_p], c_i),
     "chx_reanchor_scratch_bytes": ([c_p, c_i, c_i], C.c_int64),
     "chx_reanchor": ([c_p, c_p, c_i, c_p, c_i, c_p, c_p, C.c_int64, c_p, c_p], c_i),
     "chx_reanchor_due": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_p, c_p, c_p, C.c_int64, c_p,

@@ -259,6 +259,37 @@ using namespace chx;
 
 extern "C" {
 
+// Pair-type counts over a subset of pairs, one CTA per configuration:
+// counts[c][a * nsp + b] = #{q : species[c][pi[q]] = a, species[c][pj[q]] = b}.
+// These are the statistics of the Warren-Cowley parameters
+// (exafs_gpu/lattice.py:167-185): alpha_AB = 1 - (n_AB / n_A) / c_B.
+__global__ void __launch_bounds__(256) k_pair_counts(const int *__restrict__ species, int natoms,
+                                                     const int *__restrict__ pi,
+                                                     const int *__restrict__ pj, int npair,
+                                                     int nsp, int *__restrict__ counts,
+                                                     int *__restrict__ err) {
+    __shared__ int s_h[64];
+    const int c = blockIdx.x, nn = nsp * nsp;
+    for (int q = threadIdx.x; q < nn; q += blockDim.x) s_h[q] = 0;
+    __syncthreads();
+    const int *S = species + (long)c * natoms;
+    for (int q = threadIdx.x; q < npair; q += blockDim.x) {
+        const int i = pi[q], j = pj[q];
+        if ((unsigned)i >= (unsigned)natoms || (unsigned)j >= (unsigned)natoms) {
+            atomicOr(err, CHX_DEVERR_INDEX);
+            continue;
+        }
+        const int a = S[i], b = S[j];
+        if ((unsigned)a >= (unsigned)nsp || (unsigned)b >= (unsigned)nsp) {
+            atomicOr(err, CHX_DEVERR_INDEX);
+            continue;
+        }
+        atomicAdd(&s_h[a * nsp + b], 1);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nn; q += blockDim.x) counts[(long)c * nn + q] = s_h[q];
+}
+
 int chx_version(void) { return 1000; }
 
 int64_t chx_struct_size(int which) {
@@ -410,6 +441,17 @@ int chx_commit_state(const uint8_t *accept, const int *a_in, const int *b_in,
                                                                newpa, isswap, species, pos,
                                                                natoms, nrep);
     CHX_CHECK_LAUNCH("commit_state");
+    return CHX_OK;
+}
+
+int chx_pair_counts(const int *species, int nconf, int natoms, const int *pi, const int *pj,
+                    int npair, int nsp, int *counts, int *d_err, void *stream) {
+    CHX_REQUIRE(species && pi && pj && counts && d_err && nconf > 0 && natoms > 0 && npair > 0 &&
+                    nsp >= 1 && nsp <= 8,
+                "pair_counts: bad arguments (nsp 1..8)");
+    k_pair_counts<<<nconf, 256, 0, as_stream(stream)>>>(species, natoms, pi, pj, npair, nsp,
+                                                        counts, d_err);
+    CHX_CHECK_LAUNCH("pair_counts");
     return CHX_OK;
 }
 

@@ -41,17 +41,25 @@ constexpr int kMaxCoord = 256;
 constexpr int kReseed = 32;      // taps between exact twiddles in the transform
 constexpr int kMaxSplit = 2;     // threads sharing one bin's taps
 constexpr int kUndo = 32;        // accepted moves kept after a slot's best point
+// relative error bounds of the FP32 parts of a move's change, for the near-tie
+// test: a direct record's term (FP32 exp, sin of an FP64-reduced phase and
+// amplitude products), and a table row rounded from FP64 to FP32 (2^-24)
+constexpr double kEpsRec = 1e-6;
+constexpr double kEpsTab = 6.0e-8;
 
 // Shared-memory carve-up of one step CTA (all offsets 16-byte aligned).
+// The near-tie FP64 transforms reuse the span u .. dirv (the resampled rows,
+// the transform's output and the direct records, all rebuilt every step).
 struct StepSmem {
-    size_t u, x, tr, dchi, dir, dirv, hist, dn, list, sp, nb, cd, chi, total;
+    size_t u, x, dir, dirv, tr, dchi, hist, dn, list, sp, nb, cd, chi, total;
+    size_t tie;      // bytes the FP64 near-tie buffers need (0: none)
 };
 
 // salt of the stage-1 uniforms of delayed acceptance
 constexpr uint64_t kDaSalt = 0x6A09E667F3BCC909ULL;
 
 template <typename T>
-static inline size_t al16(size_t n) { return ((n * sizeof(T)) + 15) / 16 * 16; }
+__host__ __device__ static inline size_t al16(size_t n) { return ((n * sizeof(T)) + 15) / 16 * 16; }
 
 static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     StepSmem s;
@@ -69,10 +77,15 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     // row, H <= 256) shares the transform's region: they are used in turn
     if (L.mlp) xs = std::max(xs, al16<float>((size_t)(kStepThreads / 32 + 1) * 256));
     s.x = o; o += xs;
-    s.tr = o; o += al16<double>((size_t)L.nsp * L.nk);
-    s.dchi = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.dir = o; o += al16<PairRec>((size_t)2 * maxaff);
     s.dirv = o; o += al16<int>((size_t)2 * maxaff);
+    // FP64 resampled rows and one split of the FP64 window transform
+    s.tie = (!f64 && L.xr)
+                ? al16<double>(nchp * L.ncoef) + al16<double2>((size_t)L.nchan * L.nwin)
+                : 0;
+    if (o - s.u < s.tie) o = s.u + s.tie;   // the span must hold them
+    s.tr = o; o += al16<double>((size_t)L.nsp * L.nk);
+    s.dchi = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.hist = o; o += al16<int>((size_t)std::max(nent, 1));
     s.dn = o; o += al16<int>((size_t)std::max(ndn, 1));
     s.list = o; o += al16<int>((size_t)(2 * maxaff + 2 * ndn + 2 * nent + 64));
@@ -169,7 +182,7 @@ __device__ __forceinline__ double2 twiddle(int j, double inv_half) {
 template <int NSP, int PREC>
 __device__ __noinline__ void ft_window(const chx_ladder_t &L, const double *s_tr,
                                        typename Real<PREC>::T *s_u,
-                                       typename Real<PREC>::T2 *s_x) {
+                                       typename Real<PREC>::T2 *s_x, int max_split = kMaxSplit) {
     typedef typename Real<PREC>::T real;
     typedef typename Real<PREC>::T2 real2;
     constexpr int MAXCH = 3 * NSP;
@@ -278,7 +291,7 @@ __device__ __noinline__ void ft_window(const chx_ladder_t &L, const double *s_tr
         __syncthreads();
         return;
     }
-    const int nsplit = max(1, min(kMaxSplit, (int)blockDim.x / max(nwin, 1)));
+    const int nsplit = max(1, min(max_split, (int)blockDim.x / max(nwin, 1)));
     const int jper = (ncoef + nsplit - 1) / nsplit;
     const int nx = nchan * nwin;
     for (int item = tid; item < nsplit * nwin; item += blockDim.x) {
@@ -359,19 +372,127 @@ __device__ __noinline__ void ft_window(const chx_ladder_t &L, const double *s_tr
     __syncthreads();
 }
 
+// The profiled chi^2 in two passes (method_a_rmc.py:190-227): per channel
+// num = Re<m,t> and den = <m,m> (|m| for a magnitude target), the per-edge
+// scale s = sum num / sum den over the edge's channels, then
+// sum |s m - t|^2 / sigma^2, all in FP64; m(g) comes from getm(g) (g the
+// window point). The second pass sums small residuals, so the result keeps
+// FP64's relative precision (a one-pass s^2 A - 2 s B + C cancels). With dx
+// (a change of chi(R) inside m), *s_d2 = sum s^2 |dx|^2 / sigma^2.
+template <int NSP, typename GetM, typename R2>
+__device__ void chi2_profiled(const chx_ladder_t &L, GetM getm, const R2 *dx, double *s_num,
+                              double *s_den, double *s_sq, double *s_scale, double *s_c2,
+                              double *s_d2) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nchan = L.nchan, nwin = L.nwin, nkw = L.nkw;
+    for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
+        double nu = 0.0, dn = 0.0, D = 0.0;
+        for (int q = lane; q < nwin; q += 32) {
+            const long g = (long)ch * nwin + q;
+            const double2 m = getm(g);
+            const double tr = L.tm_re[g];
+            if (L.cplx) {
+                const double ti = L.tm_im[g];
+                nu += m.x * tr + m.y * ti;
+                dn += m.x * m.x + m.y * m.y;
+            } else {
+                const double mag = sqrt(m.x * m.x + m.y * m.y);
+                nu += mag * tr;
+                dn += mag * mag;
+            }
+            if (dx) {
+                const double a = dx[g].x, b = dx[g].y;
+                D += (a * a + b * b) * L.w2[g];
+            }
+        }
+        nu = warp_sum(nu);
+        dn = warp_sum(dn);
+        if (dx) D = warp_sum(D);
+        if (lane == 0) {
+            s_num[ch] = nu;
+            s_den[ch] = dn;
+            if (dx) s_sq[36 + ch] = D;
+        }
+    }
+    __syncthreads();
+    if (tid < NSP) {
+        double sc = 1.0;
+        if (L.profile) {
+            double nu = 0.0, dn = 0.0;
+            for (int q = 0; q < nkw; ++q) {
+                nu += s_num[tid * nkw + q];
+                dn += s_den[tid * nkw + q];
+            }
+            sc = nu / fmax(dn, 1e-30);
+        }
+        s_scale[tid] = sc;
+    }
+    __syncthreads();
+    for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
+        const double sc = s_scale[ch / nkw];
+        double acc = 0.0;
+        for (int q = lane; q < nwin; q += 32) {
+            const long g = (long)ch * nwin + q;
+            const double2 m = getm(g);
+            const double sg = L.sm[g];
+            if (L.cplx) {
+                const double dr = (m.x * sc - L.tm_re[g]) / sg;
+                const double di = (m.y * sc - L.tm_im[g]) / sg;
+                acc += dr * dr + di * di;
+            } else {
+                const double mag = sqrt(m.x * m.x + m.y * m.y);
+                const double dr = (mag * sc - L.tm_re[g]) / sg;
+                acc += dr * dr;
+            }
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) s_sq[ch] = acc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double tot = 0.0, d2 = 0.0;
+        for (int ch = 0; ch < nchan; ++ch) {
+            tot += s_sq[ch];
+            if (dx) {
+                const double sc = s_scale[ch / nkw];
+                d2 += sc * sc * s_sq[36 + ch];
+            }
+        }
+        *s_c2 = tot / L.nfit;
+        if (s_d2) *s_d2 = d2;
+    }
+    __syncthreads();
+}
+
 // Steps 4-5 (and the whole of k_eval_chi2): trial chi(R) on the window bins
-// (ft_window), then the profiled chi^2 into *s_c2.
+// (ft_window), then the profiled chi^2 into *s_c2. In FP32C with xr_base
+// (the slot's FP64 chi(R) on the window) s_tr holds a move's change alone:
+// the trial chi(R) is xr_base plus its transform, and *s_d2 receives
+// sum |change|^2 / sigma^2 * s^2 (for the near-tie bound). max_split: the
+// FP64 transform's bin splits (1 for the near-tie buffers).
 template <int NSP, int PREC>
 __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real<PREC>::T *s_u,
                         typename Real<PREC>::T2 *s_x, double *s_num, double *s_den,
-                        double *s_sq, double *s_scale, double *s_c2) {
+                        double *s_sq, double *s_scale, double *s_c2,
+                        const double *xr_base = nullptr, double *s_d2 = nullptr,
+                        int max_split = kMaxSplit) {
     typedef typename Real<PREC>::T real;
     typedef typename Real<PREC>::T2 real2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nchan = L.nchan, nwin = L.nwin, nkw = L.nkw;
-    ft_window<NSP, PREC>(L, s_tr, s_u, s_x);
+    ft_window<NSP, PREC>(L, s_tr, s_u, s_x, max_split);
 
     if constexpr (PREC != CHX_FP64) {
+        if (xr_base) {
+            // the trial chi(R) = the slot's FP64 chi(R) + the FP32 transform
+            // of the change (added in the order the commit adds it)
+            auto getm = [&](long g) {
+                const real2 d = s_x[g];
+                return make_double2((double)d.x + xr_base[2 * g], (double)d.y + xr_base[2 * g + 1]);
+            };
+            chi2_profiled<NSP>(L, getm, s_x, s_num, s_den, s_sq, s_scale, s_c2, s_d2);
+            return;
+        }
         // one pass: per channel num = Re<m,t>, den = <m,m> (the profiled scale)
         // and A = <m,m>/s^2, B = Re<m,t>/s^2, C = <t,t>/s^2, so that
         // sum |s m - t|^2 / s^2 = s^2 A - 2 s B + C (sums in FP64)
@@ -429,69 +550,63 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real
         __syncthreads();
     } else {
         // profiled chi^2, the reference's two passes (FP64)
-        for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
-            double nu = 0.0, dn = 0.0;
-            for (int q = lane; q < nwin; q += 32) {
-                real2 m = s_x[ch * nwin + q];
-                double tr = L.tm_re[ch * nwin + q];
-                if (L.cplx) {
-                    double ti = L.tm_im[ch * nwin + q];
-                    nu += (double)m.x * tr + (double)m.y * ti;
-                    dn += (double)m.x * m.x + (double)m.y * m.y;
-                } else {
-                    double mag = sqrt((double)m.x * m.x + (double)m.y * m.y);
-                    nu += mag * tr;
-                    dn += mag * mag;
-                }
-            }
-            nu = warp_sum(nu);
-            dn = warp_sum(dn);
-            if (lane == 0) {
-                s_num[ch] = nu;
-                s_den[ch] = dn;
-            }
-        }
-        __syncthreads();
-        if (tid < NSP) {
-            double s = 1.0;
-            if (L.profile) {
-                double nu = 0.0, dn = 0.0;
-                for (int q = 0; q < nkw; ++q) {
-                    nu += s_num[tid * nkw + q];
-                    dn += s_den[tid * nkw + q];
-                }
-                s = nu / fmax(dn, 1e-30);
-            }
-            s_scale[tid] = s;
-        }
-        __syncthreads();
-        for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
-            double s = s_scale[ch / nkw], acc = 0.0;
-            for (int q = lane; q < nwin; q += 32) {
-                real2 m = s_x[ch * nwin + q];
-                long g = (long)ch * nwin + q;
-                double sg = L.sm[g];
-                if (L.cplx) {
-                    double dr = ((double)m.x * s - L.tm_re[g]) / sg;
-                    double di = ((double)m.y * s - L.tm_im[g]) / sg;
-                    acc += dr * dr + di * di;
-                } else {
-                    double mag = sqrt((double)m.x * m.x + (double)m.y * m.y);
-                    double dr = (mag * s - L.tm_re[g]) / sg;
-                    acc += dr * dr;
-                }
-            }
-            acc = warp_sum(acc);
-            if (lane == 0) s_sq[ch] = acc;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double tot = 0.0;
-            for (int ch = 0; ch < L.nchan; ++ch) tot += s_sq[ch];
-            *s_c2 = tot / L.nfit;
-        }
-        __syncthreads();
+        auto getm = [&](long g) {
+            const real2 m = s_x[g];
+            return make_double2((double)m.x, (double)m.y);
+        };
+        chi2_profiled<NSP>(L, getm, (const real2 *)nullptr, s_num, s_den, s_sq, s_scale, s_c2,
+                           nullptr);
     }
+}
+
+// The change of a move again with FP64 terms, for the near-tie re-check: the
+// direct records' FP64 term, the FP64 (shell, type) rows of the table counts
+// and the FP64 MS rows of the entry changes (lists as the compaction wrote
+// them: direct record indices, then (row, count) pairs of the table, then of
+// the MS entries in absorber runs s_msb) into s_dchi. Out of line: the step
+// keeps its registers for its hot loops.
+template <int NSP>
+__device__ __noinline__ void tie_delta64(const chx_ladder_t &L, const PairRec *s_dir,
+                                         const int *s_list, int ndirmax, int ndn,
+                                         const int *s_msb, int ndir, int ndnz, double *s_dchi) {
+    const int nk = L.nk, nn = NSP * NSP;
+    const int *l_dir = s_list;
+    const int2 *l_dn = (const int2 *)(s_list + ndirmax);
+    const int2 *l_ms = l_dn + ndn;
+    for (int ik = threadIdx.x; ik < nk; ik += blockDim.x) {
+        double acc[NSP];
+#pragma unroll
+        for (int q = 0; q < NSP; ++q) acc[q] = 0.0;
+        if (ndir) {
+            KConst<NSP> kc;
+            load_kconst<NSP>(kc, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, ik);
+            for (int q = 0; q < ndir; ++q) {
+                PairRec d = s_dir[l_dir[q]];
+                const int neg = d.t >> 16;
+                d.t &= 0xFFFF;
+                const double v = rec_term<NSP, CHX_FP64>(d, kc);
+                add_by_species<NSP>(acc, d.t / NSP, neg ? -v : v);
+            }
+        }
+        if (L.sstab)
+            for (int q = 0; q < ndnz; ++q) {
+                const int2 jc = l_dn[q];
+                add_by_species<NSP>(acc, (jc.x % nn) / NSP,
+                                    (double)jc.y * L.sstab[(long)jc.x * nk + ik]);
+            }
+#pragma unroll
+        for (int a_ = 0; a_ < NSP; ++a_) {
+            double sa = 0.0;
+            for (int q = s_msb[a_]; q < s_msb[a_ + 1]; ++q) {
+                const int2 ec = l_ms[q];
+                sa = fma((double)ec.y, L.ms_T[(long)ec.x * nk + ik], sa);
+            }
+            acc[a_] += sa;
+        }
+#pragma unroll
+        for (int q = 0; q < NSP; ++q) s_dchi[q * nk + ik] = acc[q];
+    }
+    __syncthreads();
 }
 
 // Stage 1 of delayed acceptance for a swap of a and b (species differ),
@@ -592,11 +707,16 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     __shared__ Proposal prop;
     __shared__ uint64_t s_step, s_base;
     __shared__ int s_rung, s_ndir, s_ndn, s_nhist, s_acc;
-    __shared__ double s_num[32], s_den[32], s_sq[40], s_scale[8], s_de[NT / 32];
+    __shared__ double s_num[32], s_den[32], s_sq[48], s_scale[8], s_de[NT / 32];
     __shared__ double s_c2;
     __shared__ int s_msb[NSP + 1];
     __shared__ chx_mlp_t s_mlp;
     __shared__ double s_dhat, s_dast[4];
+    __shared__ double s_d2, s_xo, s_xd, s_uu, s_c2t, s_c2c;   // near-tie re-check
+    __shared__ int s_tie;
+    // near-tie bound of the FP32 terms: per warp, sum |count| x row max of the
+    // table / MS rows by absorber, and the squared k-space error bound
+    __shared__ double s_mtab[NT / 32][NSP], s_e2w[NT / 32];
     __shared__ float s_sigma;
     __shared__ int s_daon, s_skip;
     __shared__ long long s_logi;
@@ -690,6 +810,9 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     for (int q = tid; q < NSP * nk; q += blockDim.x) s_chi[q] = CHg[q];
     __syncthreads();
     const bool use_tab = (PREC != CHX_FP64) && L.sstab32 != nullptr;
+    const bool use_xr = (PREC != CHX_FP64) && L.xr != nullptr;
+    const bool tie_terms = use_xr && L.tie_eps > 0.0 && L.tie_gain > 0.0;
+    double *XR = use_xr ? L.xr + (long)c * L.nchan * L.nwin * 2 : nullptr;
     const float *msT32 = L.ms_T32;
     const bool da_on = DA && s_daon != 0;
     const bool log_on = DA && L.log_cap > 0 && L.log_codes != nullptr && L.log_y != nullptr;
@@ -704,6 +827,11 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         }
         for (int e = tid; e < nent; e += blockDim.x) s_hist[e] = 0;
         for (int e = tid; e < ndn; e += blockDim.x) s_dn[e] = 0;
+        if (tid < NT / 32) {
+            s_e2w[tid] = 0.0;
+#pragma unroll
+            for (int q = 0; q < NSP; ++q) s_mtab[tid][q] = 0.0;
+        }
         __syncthreads();
         const int a = prop.a, b = prop.b, nsa = prop.nsa, nsb = prop.nsb, swp = prop.swap;
 
@@ -879,11 +1007,17 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         {
             int off = 0;
             for (int w = 0; w < warp; ++w) off += s_wcnt[w];
+            double mt[NSP];
+#pragma unroll
+            for (int q = 0; q < NSP; ++q) mt[q] = 0.0;
             for (int i0 = ms0; i0 < ms1; i0 += 32) {
                 const int i = i0 + lane;
                 const int v = i < ms1 ? s_hist[i] : 0;
                 const unsigned m = __ballot_sync(0xffffffffu, v != 0);
                 if (v != 0) l_ms[off + __popc(m & ((1u << lane) - 1))] = make_int2(i, v);
+                if (tie_terms && v != 0 && L.ms_T_max)
+                    add_by_species<NSP>(mt, i / L.ms_nblk,
+                                        fabs((double)v) * (double)L.ms_T_max[i]);
                 // list position of each absorber block's first entry, by the
                 // warp whose run holds the block's first index
                 if (lane < NSP) {
@@ -892,6 +1026,13 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                         s_msb[lane] = off + __popc(m & ((1u << d) - 1));
                 }
                 off += __popc(m);
+            }
+            if (tie_terms) {
+#pragma unroll
+                for (int q = 0; q < NSP; ++q) {
+                    const double t = warp_sum(mt[q]);
+                    if (lane == 0) s_mtab[warp][q] += t;
+                }
             }
             if (warp == nwarp - 1) {
                 if (lane == 0) s_nhist = off;
@@ -905,6 +1046,22 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         } else if (warp == 1) {
             int n = warp_compact_pairs(ndn, s_dn, l_dn);
             if (lane == 0) s_ndn = n;
+            if (tie_terms && L.sstab_max) {
+                __syncwarp();
+                double mt[NSP];
+#pragma unroll
+                for (int q = 0; q < NSP; ++q) mt[q] = 0.0;
+                for (int q = lane; q < n; q += 32) {
+                    const int2 jc = l_dn[q];
+                    add_by_species<NSP>(mt, (jc.x % nn) / NSP,
+                                        fabs((double)jc.y) * (double)L.sstab_max[jc.x]);
+                }
+#pragma unroll
+                for (int q = 0; q < NSP; ++q) {
+                    const double t = warp_sum(mt[q]);
+                    if (lane == 0) s_mtab[1][q] += t;    // after this warp's MS share
+                }
+            }
         }
         __syncthreads();
 
@@ -912,6 +1069,16 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         const int ndir = s_ndir, ndnz = s_ndn, nms = s_nhist;
         const double *CH = s_chi;
         const double *CNT = L.count + (long)c * NSP;
+        // what the transform gets at (absorber, k) index o: with the kept
+        // FP64 chi(R) the normalised change alone, else the normalised
+        // trial chi plus chi_extra (exafs_gpu/forward.py:183-187,
+        // chimera/multift.py:60-61)
+        auto trial_k = [&](int o, double d, double inv) {
+            if (use_xr) return d / inv;
+            double v = (CH[o] + d) / inv;
+            if (L.chi_extra) v += L.chi_extra[o];
+            return v;
+        };
         if (PREC != CHX_FP64 && (nent == 0 || msT32 != nullptr)) {
             // FP32 tables: one item per (absorber species, pair of k points),
             // each summing only its absorber's direct records, table rows and
@@ -926,9 +1093,9 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             // sums seed the per-absorber items below.
             if (ndir) {
                 for (int ik = tid; ik < nk; ik += blockDim.x) {
-                    double acc[NSP];
+                    double acc[NSP], gab[NSP];
 #pragma unroll
-                    for (int s = 0; s < NSP; ++s) acc[s] = 0.0;
+                    for (int s = 0; s < NSP; ++s) acc[s] = gab[s] = 0.0;
                     KConst<NSP> kc;
                     load_kconst<NSP>(kc, L.ktab, L.lamtab, L.dtab, L.ftab, L.s02, nk, ik);
                     for (int q = 0; q < ndir; ++q) {
@@ -937,13 +1104,20 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                         d.t &= 0xFFFF;
                         const double v = rec_term<NSP, PREC>(d, kc);
                         add_by_species<NSP>(acc, d.t / NSP, neg ? -v : v);
+                        if (tie_terms) add_by_species<NSP>(gab, d.t / NSP, fabs(v));
                     }
 #pragma unroll
-                    for (int s = 0; s < NSP; ++s) s_dchi[s * nk + ik] = acc[s];
+                    for (int s = 0; s < NSP; ++s) {
+                        s_dchi[s * nk + ik] = acc[s];
+                        // the records' sum of |term|, read back by the item
+                        // of (s, ik) below before it writes the trial there
+                        if (tie_terms) s_tr[s * nk + ik] = gab[s];
+                    }
                 }
                 __syncthreads();
             }
             const int nk2 = (nk + 1) & ~1, npk = nk2 >> 1, npw = (npk + 31) & ~31;
+            double e2acc = 0.0;
             for (int it = tid; it < NSP * npw; it += blockDim.x) {
                 const int sa_ = it / npw, k0 = 2 * (it - sa_ * npw);
                 if (k0 >= nk) continue;
@@ -977,16 +1151,30 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 }
                 const double inv = fmax(CNT[sa_], 1.0);
                 const int o = sa_ * nk + k0;
+                if (tie_terms) {
+                    // |FP32 error| of the change at (sa_, k) <= eps_rec sum |record
+                    // terms| + eps_tab sum |count| x row max
+                    double mt = 0.0;
+                    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mt += s_mtab[w][sa_];
+                    const double g0 = ndir ? s_tr[o] : 0.0;
+                    const double e0 = (kEpsRec * g0 + kEpsTab * mt) / inv;
+                    e2acc += e0 * e0;
+                    if (k1ok) {
+                        const double g1 = ndir ? s_tr[o + 1] : 0.0;
+                        const double e1 = (kEpsRec * g1 + kEpsTab * mt) / inv;
+                        e2acc += e1 * e1;
+                    }
+                }
                 s_dchi[o] = acc0;
-                double v = (CH[o] + acc0) / inv;
-                if (L.chi_extra) v += L.chi_extra[o];
-                s_tr[o] = v;
+                s_tr[o] = trial_k(o, acc0, inv);
                 if (k1ok) {
                     s_dchi[o + 1] = acc1;
-                    v = (CH[o + 1] + acc1) / inv;
-                    if (L.chi_extra) v += L.chi_extra[o + 1];
-                    s_tr[o + 1] = v;
+                    s_tr[o + 1] = trial_k(o + 1, acc1, inv);
                 }
+            }
+            if (tie_terms) {
+                e2acc = warp_sum(e2acc);
+                if (lane == 0) s_e2w[warp] = e2acc;
             }
         } else
         for (int ik = tid; ik < nk; ik += blockDim.x) {
@@ -1038,31 +1226,31 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
 #pragma unroll
             for (int s = 0; s < NSP; ++s) {
                 s_dchi[s * nk + ik] = acc[s];
-                double v = (CH[s * nk + ik] + acc[s]) / fmax(CNT[s], 1.0);
-                if (L.chi_extra) v += L.chi_extra[s * nk + ik];
-                s_tr[s * nk + ik] = v;
+                s_tr[s * nk + ik] = trial_k(s * nk + ik, acc[s], fmax(CNT[s], 1.0));
             }
         }
         __syncthreads();
 
         // ---- 4-5. trial chi(R) on the window and its profiled chi^2
-        ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
+        ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2, XR, &s_d2);
 
         // ---- 6. Metropolis
         if (tid == 0) {
             double c2 = s_c2;
             int rung = s_rung;
-            double x = L.beta_rung[rung] * (c2 - L.chi2[c]) * L.nfit;
+            const double beta = L.beta_rung[rung];
+            double xo = 0.0;      // the exact terms of x beside the chi^2 change
             if (feat && da_on) {
                 // stage 2 of delayed acceptance: the surrogate's error alone
                 // (the prior's change cancels between the two stages)
-                x -= L.beta_rung[rung] * s_dhat * L.nfit;
-                s_dast[3] += x <= 0.0 ? 1.0 : exp(-fmin(x, 60.0));   // stage-2 probability
+                xo = -beta * s_dhat * L.nfit;
             } else if (L.etab) {
                 double d = 0.0;
                 for (int w = 0; w < (int)(blockDim.x / 32); ++w) d += s_de[w];
-                x += L.energy_beta * d;
+                xo = L.energy_beta * d;
             }
+            double x = beta * (c2 - L.chi2[c]) * L.nfit + xo;
+            s_xo = xo;
             if (feat && log_on) {
                 const long long li = (long long)(((s_step - 1) * (uint64_t)L.nrep + (uint64_t)c) %
                                                  (uint64_t)L.log_cap);
@@ -1083,8 +1271,77 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 u = u01(splitmix64(h));
             }
             int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
-            if (feat && da_on && acc) s_dast[2] += 1.0;
+            // a near tie: the FP32 transform of the change may move x by up to
+            // tau = beta * 2 eps sqrt(chi^2_tot * sum s^2 |change|^2 / sigma^2)
+            // (Cauchy-Schwarz on the first-order term); if x - tau and x + tau
+            // decide differently, the test is redone in FP64 below
+            // plus the FP32 terms' share: an error e(k) of the change moves x by
+            // at most beta * 2 (||r|| + ||change||) s tie_gain ||e||
+            s_tie = 0;
+            if (use_xr && L.tie_eps > 0.0) {
+                const double rn = sqrt(fmax(c2, 0.0) * L.nfit), dn = sqrt(fmax(s_d2, 0.0));
+                double tau = beta * 2.0 * L.tie_eps * rn * dn;
+                if (tie_terms) {
+                    double e2 = 0.0, smax = 0.0;
+                    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) e2 += s_e2w[w];
+                    for (int q = 0; q < NSP; ++q) smax = fmax(smax, fabs(s_scale[q]));
+                    tau += beta * 2.0 * (rn + dn) * smax * L.tie_gain * sqrt(e2);
+                }
+                const double xl = x - tau, xh = x + tau;
+                const int al = (xl <= 0.0) || (u < exp(-fmin(xl, 60.0)));
+                const int ah = (xh <= 0.0) || (u < exp(-fmin(xh, 60.0)));
+                if (al != ah) {
+                    s_tie = 1;
+                    s_uu = u;
+                }
+            }
             s_acc = acc;
+            s_xd = x;
+        }
+        __syncthreads();
+        if (PREC != CHX_FP64 && s_tie) {
+            // the R-factor comparison in FP64: first the move's change again
+            // with FP64 terms (the direct records' FP64 term, the FP64 (shell,
+            // type) and MS rows), replacing the FP32 one; then chi^2 of the
+            // current and the trial chi(k) through FP64 transforms, in the span
+            // of the resampled rows / transform / direct records
+            tie_delta64<NSP>(L, s_dir, s_list, 2 * maxaff, ndn, s_msb, s_ndir, s_ndn, s_dchi);
+            typedef typename Real<CHX_FP64>::T2 d2t;
+            double *u64 = (double *)(smem + so.u);
+            d2t *x64 = (d2t *)(smem + so.u + al16<double>((size_t)(L.nchan + (L.nchan & 1)) *
+                                                          L.ncoef));
+            for (int pass = 0; pass < 2; ++pass) {
+                for (int q = tid; q < NSP * nk; q += blockDim.x) {
+                    double v = (s_chi[q] + (pass ? s_dchi[q] : 0.0)) / fmax(CNT[q / nk], 1.0);
+                    if (L.chi_extra) v += L.chi_extra[q];
+                    s_tr[q] = v;
+                }
+                __syncthreads();
+                ft_chi2<NSP, CHX_FP64>(L, s_tr, u64, x64, s_num, s_den, s_sq, s_scale,
+                                       pass ? &s_c2t : &s_c2c, nullptr, nullptr, 1);
+            }
+            if (tid == 0) {
+                const int rung = s_rung;
+                const double x = L.beta_rung[rung] * (s_c2t - s_c2c) * L.nfit + s_xo;
+                const double u = s_uu;
+                const int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
+                if (L.tie_stat) {
+                    L.tie_stat[2 * (long)c] += 1.0;
+                    if (acc != s_acc) L.tie_stat[2 * (long)c + 1] += 1.0;
+                }
+                s_acc = acc;
+                s_xd = x;
+                s_c2 = s_c2t;        // an accepted state keeps its FP64 chi^2
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            const int acc = s_acc, rung = s_rung;
+            if (feat && da_on) {
+                const double x = s_xd;
+                s_dast[3] += x <= 0.0 ? 1.0 : exp(-fmin(x, 60.0));   // stage-2 probability
+                if (acc) s_dast[2] += 1.0;
+            }
             L.acc_rung[rung] = (uint8_t)acc;
             if (L.acc_log) L.acc_log[(long)st * L.nrep + rung] = (uint8_t)acc;
         }
@@ -1099,6 +1356,21 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         // ---- 7. commit
         if (s_acc) {
             for (int q = tid; q < NSP * nk; q += blockDim.x) s_chi[q] += s_dchi[q];
+            if (use_xr) {
+                const int nx = L.nchan * L.nwin;
+                if (s_tie) {        // the FP64 trial chi(R) of the near-tie test
+                    const double *x64 =
+                        (const double *)(smem + so.u +
+                                         al16<double>((size_t)(L.nchan + (L.nchan & 1)) * L.ncoef));
+                    for (int q = tid; q < 2 * nx; q += blockDim.x) XR[q] = x64[q];
+                } else {
+                    for (int q = tid; q < nx; q += blockDim.x) {
+                        const real2 d = s_x[q];
+                        XR[2 * q] += (double)d.x;
+                        XR[2 * q + 1] += (double)d.y;
+                    }
+                }
+            }
             if (nent && swp) {
                 int *C = L.ms_C + (long)c * nent;
                 for (int q = tid; q < nms; q += blockDim.x) C[l_ms[q].x] += l_ms[q].y;
@@ -1178,7 +1450,7 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
     typedef typename Real<PREC>::T2 real2;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ chx_ladder_t L;
-    __shared__ double s_num[32], s_den[32], s_sq[40], s_scale[8], s_c2;
+    __shared__ double s_num[32], s_den[32], s_sq[48], s_scale[8], s_c2;
     const int tid = threadIdx.x, slot = blockIdx.x;
     if (mask && !mask[slot]) return;
     {
@@ -1199,7 +1471,26 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
         s_tr[q] = v;
     }
     __syncthreads();
-    ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
+    if (PREC != CHX_FP64 && L.xr) {
+        // FP32C with the kept chi(R): the transform in FP64 (one bin split,
+        // in the span the step reserves for it), and for the slot's own chi
+        // its FP64 chi(R) stored for the step
+        const int nx = L.nchan * L.nwin;
+        double *u64 = (double *)(smem + so.u);
+        double2 *x64 =
+            (double2 *)(smem + so.u + al16<double>((size_t)(L.nchan + (L.nchan & 1)) * L.ncoef));
+        ft_chi2<NSP, CHX_FP64>(L, s_tr, u64, x64, s_num, s_den, s_sq, s_scale, &s_c2, nullptr,
+                               nullptr, 1);
+        if (!chi_in) {
+            double *X = L.xr + (long)c * nx * 2;
+            for (int q = tid; q < nx; q += blockDim.x) {
+                X[2 * q] = x64[q].x;
+                X[2 * q + 1] = x64[q].y;
+            }
+        }
+    } else {
+        ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
+    }
     if (tid == 0) {
         if (out) out[slot] = s_c2;
         else L.chi2[c] = s_c2;      // masked refresh: the slot's own chi^2
@@ -1678,22 +1969,29 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
                     "sampler: ladder %d has an incomplete surrogate feature set or swap log", i);
         StepSmem s = step_smem(L, precision);
         // field sizes of this ladder, then the running maximum of each
-        size_t f[13] = {s.x - s.u, s.tr - s.x, s.dchi - s.tr, s.dir - s.dchi, s.dirv - s.dir,
-                        s.hist - s.dirv, s.dn - s.hist, s.list - s.dn, s.sp - s.list,
+        size_t f[13] = {s.x - s.u, s.dir - s.x, s.dirv - s.dir, s.tr - s.dirv, s.dchi - s.tr,
+                        s.hist - s.dchi, s.dn - s.hist, s.list - s.dn, s.sp - s.list,
                         s.nb - s.sp, s.cd - s.nb, s.chi - s.cd, s.total - s.chi};
-        size_t *g[13] = {&mx.u, &mx.x, &mx.tr, &mx.dchi, &mx.dir, &mx.dirv, &mx.hist, &mx.dn,
+        size_t *g[13] = {&mx.u, &mx.x, &mx.dir, &mx.dirv, &mx.tr, &mx.dchi, &mx.hist, &mx.dn,
                          &mx.list, &mx.sp, &mx.nb, &mx.cd, &mx.chi};
         for (int q = 0; q < 13; ++q) *g[q] = std::max(*g[q], f[q]);
+        mx.tie = std::max(mx.tie, s.tie);
+    }
+    // the near-tie span u .. dirv must hold the largest FP64 buffers
+    {
+        const size_t span = mx.u + mx.x + mx.dir + mx.dirv;
+        if (span < mx.tie) mx.dirv += (mx.tie - span + 15) / 16 * 16;
     }
     // mx holds field sizes; turn them into offsets
     StepSmem o;
     size_t at = 0;
+    o.tie = mx.tie;
     o.u = at; at += mx.u;
     o.x = at; at += mx.x;
-    o.tr = at; at += mx.tr;
-    o.dchi = at; at += mx.dchi;
     o.dir = at; at += mx.dir;
     o.dirv = at; at += mx.dirv;
+    o.tr = at; at += mx.tr;
+    o.dchi = at; at += mx.dchi;
     o.hist = at; at += mx.hist;
     o.dn = at; at += mx.dn;
     o.list = at; at += mx.list;
@@ -1870,6 +2168,36 @@ static int reanchor_launch(const chx_ladder_t *d_ladders, const chx_ladder_t *ho
 int64_t chx_reanchor_scratch_bytes(const chx_ladder_t *host_ladders, int nladders, int max_due) {
     if (!host_ladders || nladders <= 0 || max_due <= 0) return -1;
     return ra_bytes(host_ladders, nladders, std::min(max_due, kRaWindow));
+}
+
+int chx_refresh_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                     int nladders, const int *slot_ladder, int nslots, int precision,
+                     const uint8_t *mask, void *stream) {
+    CHX_REQUIRE(d_ladders && host_ladders && slot_ladder && nladders > 0 && nslots > 0,
+                "refresh_chi2: bad arguments");
+    StepSmem so;
+    size_t smem = 0;
+    int rc = plan_ladders(host_ladders, nladders, precision, &so, &smem);
+    if (rc != CHX_OK) return rc;
+    cudaStream_t st = as_stream(stream);
+    int nsp = host_ladders[0].nsp;
+#define CHX_EV(N, PR) launch_eval<N, PR>(d_ladders, slot_ladder, nslots, so, smem, nullptr, nullptr, nullptr, mask, st)
+    if (precision == CHX_FP64) {
+        switch (nsp) {
+            case 2: return CHX_EV(2, CHX_FP64);
+            case 3: return CHX_EV(3, CHX_FP64);
+            case 4: return CHX_EV(4, CHX_FP64);
+        }
+    } else {
+        switch (nsp) {
+            case 2: return CHX_EV(2, CHX_FP32C);
+            case 3: return CHX_EV(3, CHX_FP32C);
+            case 4: return CHX_EV(4, CHX_FP32C);
+        }
+    }
+#undef CHX_EV
+    set_error("refresh_chi2: nsp %d not built", nsp);
+    return CHX_ERR_UNSUPPORTED;
 }
 
 int chx_reanchor(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders, int nladders,

@@ -56,6 +56,35 @@ def _fp32_rows(t):
     return out
 
 
+def _window_gain(f, win, sm, nsp, nk):
+    """sqrt of the largest eigenvalue, over the edges, of B^H W B: B the map
+    from an edge's normalised chi(k) (nk) to its channels' chi(R) on the fit
+    bins (resample, window x k^w, transform: the set-up f of _ft_setup), W
+    the weights 1 / sigma^2 (sm, (nchan, nwin)). ||B x||_W <= gain ||x||."""
+    nchan, nkw = f["nchan"], f["nkw"]
+    n = f["n0"][0] + np.arange(f["ncoef"])
+    win = np.asarray(win, np.int64)
+    z = np.exp(-2j * np.pi * ((np.outer(n, win) % f["nfft"]) / f["nfft"])) * f["norm"]
+    best = 0.0
+    for e in range(nsp):
+        G = np.zeros((nk, nk), complex)
+        for c in range(e * nkw, (e + 1) * nkw):
+            B = np.zeros((nk, win.size), complex)
+            wt = f["w"][c][:, None] * z
+            np.add.at(B, f["idx"][c], (1.0 - f["frac"][c])[:, None] * wt)
+            np.add.at(B, np.minimum(f["idx"][c] + 1, nk - 1), f["frac"][c][:, None] * wt)
+            Bw = B * (1.0 / np.asarray(sm[c], float))[None, :]
+            G += Bw @ Bw.conj().T
+        best = max(best, float(np.linalg.eigvalsh(G).max()))
+    return float(np.sqrt(max(best, 0.0)))
+
+
+def torch_cat_host(ts):
+    """Concatenate device tensors along dim 0 and bring them to the host."""
+    import torch
+    return torch.cat([t.reshape(t.shape[0], -1) for t in ts]).cpu().numpy()
+
+
 def _on_device(x, dtype):
     """x as a contiguous CUDA tensor of dtype (one host->device copy, none
     for a device tensor of that type)."""
@@ -122,6 +151,12 @@ class LadderSpec:
 
 class Ladders:
     """Device state and descriptors of a batch of ladders (see module doc)."""
+
+    # FP32C: keep each slot's FP64 chi(R) and transform only a move's change
+    # (xr of chx_ladder_t); tie_eps: relative bound of the FP32 transform's
+    # rounding used by the near-tie FP64 re-check (0: off)
+    delta_transform = True
+    tie_eps = 3e-5
 
     def __init__(self, specs, precision=FP64, use_table=True, threads=256, min_blocks=3):
         import torch
@@ -329,6 +364,32 @@ class Ladders:
         L.acc_log = N.dptr(b["acc_log"])
         L.exch_att, L.exch_acc = N.dptr(b["exch_att"]), N.dptr(b["exch_acc"])
         L.best_stale = N.dptr(b["best_stale"])
+        # FP32C: the slots' FP64 chi(R) on the fit window (the step transforms
+        # a move's change alone) and the near-tie FP64 re-check
+        if self.precision != FP64 and self.delta_transform:
+            b["xr"] = torch.zeros((nrep, f["nchan"], int(win.size), 2), dtype=torch.float64,
+                                  device="cuda")
+            b["tie_stat"] = torch.zeros((nrep, 2), dtype=torch.float64, device="cuda")
+            self.keep += [b["xr"], b["tie_stat"]]
+            L.xr, L.tie_stat, L.tie_eps = N.dptr(b["xr"]), N.dptr(b["tie_stat"]), self.tie_eps
+            # the FP32 terms' share of the near-tie bound: row maxima of the
+            # tables the step rounds to FP32, and the transform's gain
+            if "sstab" in b:
+                b["sstab_max"] = b["sstab"].abs().amax(dim=1).float().contiguous()
+                L.sstab_max = N.dptr(b["sstab_max"])
+                self.keep.append(b["sstab_max"])
+            else:
+                L.sstab_max = 0
+            if ms is not None:
+                b["ms_T_max"] = ms.T.abs().amax(dim=1).float().contiguous()
+                L.ms_T_max = N.dptr(b["ms_T_max"])
+                self.keep.append(b["ms_T_max"])
+            else:
+                L.ms_T_max = 0
+            L.tie_gain = _window_gain(f, win, sm, nsp, nk)
+        else:
+            L.xr, L.tie_stat, L.tie_eps = 0, 0, 0.0
+            L.sstab_max, L.ms_T_max, L.tie_gain = 0, 0, 0.0
         b["beta_host"] = beta
         b["cplx"] = cplx
         return b
@@ -425,7 +486,12 @@ class Ladders:
             N.call("chx_reanchor", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
                    N.ptr(self.slot_ladder), self.nslots, N.ptr(m) if m is not None else None,
                    N.ptr(scr), need, N.ptr(self.err), N.stream())
+            # chi^2 (and the FP32C chi(R)) of the re-anchored slots only
+            N.call("chx_refresh_chi2", N.ptr(self.d_ladders), C.byref(self.host), self.nladders,
+                   N.ptr(self.slot_ladder), self.nslots, self.precision,
+                   N.ptr(m) if m is not None else None, N.stream())
             self._reanchor_keep = (m, scr)      # alive until the launches have run
+            return
         else:
             for s, b in zip(self.specs, self.bufs):
                 chi = s.fm.chi_full(b["pos"], b["species"], precision=FP64)
@@ -547,6 +613,18 @@ class Ladders:
 
     def screening_on(self):
         return [bool(int(b["da_on"].item())) if "da_on" in b else False for b in self.bufs]
+
+    def tie_stats(self, reset=False):
+        """(nladders, 2) summed over each ladder's slots: Metropolis tests
+        re-decided with FP64 transforms (near ties), and decisions they
+        changed (FP32C with the kept chi(R))."""
+        out = np.zeros((self.nladders, 2))
+        for li, b in enumerate(self.bufs):
+            if "tie_stat" in b:
+                out[li] = _host(b["tie_stat"]).sum(0)
+                if reset:
+                    b["tie_stat"].zero_()
+        return out
 
     def da_stats(self, reset=False):
         """(nladders, 4) summed over each ladder's slots: moves screened,
@@ -1015,6 +1093,9 @@ class BatchedSampler:
             self.graph.replay()
             self.blocks += 1
             self.steps += self.exchange_every
+            if (self.collect_from is not None and self.blocks >= self.collect_from
+                    and self.blocks % self.collect_every_blocks == 0):
+                self.collect()
             if self.blocks % self.check_every == 0:
                 if self.reanchor_every and not self.device_reanchor:
                     for lad in self.groups:
@@ -1091,6 +1172,73 @@ class BatchedSampler:
                 if self.groups[g] is lad:
                     out[gi] = st[q]
         self.last_screen = out
+
+    # ------------------------------------------------- posterior samples
+    collect_from = None      # first exchange period (count) at which samples are taken
+
+    def enable_collect(self, from_block, every_blocks=2, collect_beta=0.5, n_collect=4):
+        """Posterior samples the way the reference's fit loop takes them
+        (fitrun.py:307-333 with method_a_rmc.py:404-431, 458-491): from
+        exchange period `from_block` on, every `every_blocks` periods (the
+        reference's 50 steps are 2 periods of 25), the configurations of the
+        n_collect rungs whose beta is nearest collect_beta in log spacing are
+        reduced on the device to their first-shell pair-type counts
+        (chx_pair_counts); `posterior_wc` turns them into Warren-Cowley
+        parameters."""
+        self.collect_from, self.collect_every_blocks = int(from_block), int(every_blocks)
+        self.collect_beta, self.n_collect = float(collect_beta), int(n_collect)
+        self._samples = [[] for _ in range(self.nladders)]
+        self._shell_pairs = {}
+
+    def _first_shell(self, fm):
+        key = id(fm)
+        if key not in self._shell_pairs:
+            sel = np.asarray(fm.shell) == 0
+            self._shell_pairs[key] = (N.to_dev(np.ascontiguousarray(fm.i_idx[sel], np.int32)),
+                                      N.to_dev(np.ascontiguousarray(fm.j_idx[sel], np.int32)),
+                                      int(sel.sum()))
+        return self._shell_pairs[key]
+
+    def collect(self):
+        """Take one posterior sample set now (device work, no host sync)."""
+        torch = self.torch
+        for li in range(self.nladders):
+            lad, q = self.ladder(li)
+            b, spec = lad.bufs[q], lad.specs[q]
+            beta = b["beta_host"]
+            k = min(self.n_collect, spec.nrep)
+            rungs = np.argsort(np.abs(np.log(beta) - np.log(self.collect_beta)))[:k]
+            if "_collect_rungs" not in b:
+                b["_collect_rungs"] = N.to_dev(np.ascontiguousarray(rungs, np.int64))
+            rt = b["_collect_rungs"]
+            sp = b["species"].index_select(0, b["slot_of"].index_select(0, rt).long()).contiguous()
+            pi, pj, npair = self._first_shell(spec.fm)
+            cnt = torch.empty((k, lad.nsp * lad.nsp), dtype=torch.int32, device="cuda")
+            N.call("chx_pair_counts", N.ptr(sp), k, spec.fm.natoms, N.ptr(pi), N.ptr(pj), npair,
+                   lad.nsp, N.ptr(cnt), N.ptr(lad.err), N.stream())
+            self._samples[li].append((self.blocks, cnt))
+
+    def posterior_wc(self, li, composition=None, from_block=None):
+        """(mean, sd, n) of ladder li's first-shell Warren-Cowley vector (the
+        upper triangle, lattice.wc_vector order) over its collected samples
+        (method_a_rmc.py:477-491), those taken at or after exchange period
+        from_block if given. composition: the species fractions (default the
+        ladder's own, constant under swaps)."""
+        lad, q = self.ladder(li)
+        nsp = lad.nsp
+        sel = [c for blk, c in self._samples[li] if from_block is None or blk >= from_block]
+        if not sel:
+            raise RuntimeError("no posterior samples: enable_collect before running")
+        n = torch_cat_host(sel).reshape(-1, nsp, nsp).astype(np.float64)
+        if composition is None:
+            composition = _host(lad.bufs[q]["count"][0]) / lad.specs[q].fm.natoms
+        c = np.asarray(composition, np.float64)
+        tot = n.sum(2, keepdims=True)
+        alpha = 1.0 - np.divide(n, np.maximum(tot, 1.0)) / c[None, None, :]
+        alpha[np.broadcast_to(tot == 0, alpha.shape)] = 0.0
+        iu = np.triu_indices(nsp)
+        v = alpha[:, iu[0], iu[1]]
+        return v.mean(0), v.std(0), v.shape[0]
 
     def best(self, li):
         lad, q = self.ladder(li)

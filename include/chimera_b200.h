@@ -192,6 +192,17 @@ CHX_API int chx_ms_delta(const int *species, int nrep, int natoms, const int *in
 CHX_API int chx_ms_chi_of(const int *counts, const double *T, int nconf, int nsp, int nblk,
                   int nk, double *chi, void *stream);
 
+/* Pair-type counts over a subset of pairs (e.g. the first shell), one row per
+ * configuration: counts (nconf, nsp*nsp), counts[c][a*nsp+b] = number of
+ * pairs q with species[c][pi[q]] = a and species[c][pj[q]] = b. The
+ * Warren-Cowley parameters of exafs_gpu/lattice.py:167-185 follow as
+ * alpha_AB = 1 - (n_AB / n_A) / c_B; the posterior samples of
+ * method_a_rmc.py:477-491 (posterior_wc) are taken from them on the device.
+ * Out-of-range indices or species set CHX_DEVERR_INDEX in *d_err. */
+CHX_API int chx_pair_counts(const int *species, int nconf, int natoms, const int *pi,
+                            const int *pj, int npair, int nsp, int *counts, int *d_err,
+                            void *stream);
+
 /* ------------------------------------------------------------------------
  * 4. The fused PT-RMC step (A3-A7) and replica exchange (A8) of
  *    methods/method_a_rmc.py:RMCSampler, for a batch of independent ladders.
@@ -352,6 +363,28 @@ typedef struct {
     /* (nrep) 1 where pos may differ from best_pos (a displacement since
        best_pos was written), 0 where they are equal; NULL: always copy */
     uint8_t *best_stale;
+    /* CHX_FP32C, optional: each slot's chi(R) on the fit window in FP64,
+       (nrep, nchan, nwin) complex as (re, im) pairs, written in FP64 by
+       chx_eval_chi2 (and so by re-anchoring) and kept by the step: a move's
+       change alone goes through the FP32 transform and is added to it, so the
+       transform's rounding scales with the change, not with chi. NULL: the
+       step transforms the whole trial chi in FP32. */
+    double *xr;
+    /* near ties (with xr): when |x + ln u| of a Metropolis test is within
+       tie_eps times a bound of the FP32 transform's effect on x, the trial
+       and current chi^2 are recomputed with FP64 transforms of their FP64
+       chi(k) and the test is decided on those (tie_eps 0: never);
+       tie_stat (nrep, 2): FP64 re-evaluations, decisions they changed. */
+    double tie_eps;
+    double *tie_stat;
+    /* the FP32 terms' share of the near-tie bound (optional, NULL: left out):
+       the largest |value| of each (shell, type) and MS table row (FP64 rows
+       rounded to FP32 in the step), and tie_gain = sqrt of the largest
+       eigenvalue of B^H W B per edge (B the window transform of a normalised
+       chi(k) onto the fit bins, W = 1 / sigma^2), which turns a bound on a
+       k-space error into one on its weighted chi(R) norm */
+    const float *sstab_max, *ms_T_max;
+    double tie_gain;
 } chx_ladder_t;
 
 /* Bytes of dynamic shared memory the step kernel needs for these ladders. */
@@ -396,6 +429,13 @@ CHX_API int chx_eval_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *hos
  * (deterministic); scratch (caller-owned) is sized by
  * chx_reanchor_scratch_bytes(host_ladders, nladders, max_due) with
  * max_due = nslots for chx_reanchor. */
+/* chi^2 of each slot with mask[slot] != 0 (mask NULL: every slot) from its own
+ * chi, written to the slot's chi2 (and, in CHX_FP32C with xr, its FP64
+ * chi(R)): the refresh after a re-anchoring of those slots
+ * (method_a_rmc.py:180 evaluates the start state the same way). */
+CHX_API int chx_refresh_chi2(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,
+                             int nladders, const int *slot_ladder, int nslots, int precision,
+                             const uint8_t *mask, void *stream);
 CHX_API int64_t chx_reanchor_scratch_bytes(const chx_ladder_t *host_ladders, int nladders,
                                            int max_due);
 CHX_API int chx_reanchor(const chx_ladder_t *d_ladders, const chx_ladder_t *host_ladders,

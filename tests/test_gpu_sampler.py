@@ -326,3 +326,77 @@ def test_device_reanchoring_equals_host_reanchoring(cuda):
     for k in a:
         assert np.array_equal(a[k], b[k]), k
     assert bs_dev.reanchors > 0 and bs_host.host_reanchors > 0
+
+
+def test_posterior_warren_cowley_matches_lattice_definition(cuda):
+    """Posterior samples reduced on the device (chx_pair_counts over the first
+    shell) give the Warren-Cowley vector of lattice.warren_cowley (the
+    reference's definition, exafs_gpu/lattice.py:167-185) for the sampled
+    rungs' configurations."""
+    from chimera_b200 import configs
+    from chimera_b200 import lattice as L
+    from chimera_b200.sampler import BatchedSampler, LadderSpec
+    prob = configs.Problem(elements=("Fe", "Ni", "Cr"), composition=(0.4, 0.4, 0.2),
+                           ncell=(4, 4, 4), ms=False)
+    pos = prob.position(0)
+    spec = LadderSpec(prob.fm, prob.ft, pos.target, pos.mask, pos.sigma_R, nrep=8, tmin=1e-3,
+                      tmax=1e-1, seed=3, swap_frac=1.0)
+    bs = BatchedSampler([spec], precision=1, exchange_every=25, reanchor_every=0)
+    bs.init_state([prob.random_config(5)], prob.cell.ideal)
+    bs.enable_collect(from_block=10 ** 9)            # manual collection only
+    want = []
+    for blocks in (0, 3, 4):
+        bs.run_blocks(blocks) if blocks else None
+        bs.collect()
+        b = bs.lad.bufs[0]
+        rungs = b["_collect_rungs"].cpu().numpy()
+        slots = b["slot_of"].cpu().numpy()[rungs]
+        for sp in b["species"].cpu().numpy()[slots]:
+            a = L.warren_cowley(sp, prob.top.i, prob.top.j, prob.top.shift, prob.cell,
+                                float(prob.top.r_shell[0]), nsp=3)
+            want.append(a[np.triu_indices(3)])
+    want = np.array(want)
+    mean, sd, n = bs.posterior_wc(0)
+    assert n == len(want) == 12
+    np.testing.assert_allclose(mean, want.mean(0), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(sd, want.std(0), rtol=0, atol=1e-12)
+    assert bs.lad.device_error() == 0
+
+
+@pytest.mark.parametrize("name", ["rmc_trace.npz", "rmc_trace_disp.npz", "rmc_trace_ms.npz"])
+def test_fp32c_decisions_shadow_fp64_over_1000_steps(cuda, name):
+    """Decision agreement of FP32C with FP64 on the same states: an FP64
+    chain runs 1,000 steps on the reference's streams; before each of its
+    steps an FP32C sampler takes its exact state (species, positions, FP64
+    chi and chi^2, MS counts, rung maps; its FP64 chi(R) from a refresh) and
+    step counter, and makes the same proposal. Every (step, rung) decision
+    is compared. FP32C evaluates a move with FP32 terms and an FP32
+    transform of the change, re-deciding near ties with FP64 transforms;
+    the measured disagreement stays below one decision in 1,000."""
+    torch = cuda
+    d = trace_inputs(name)
+    s64, fm = device_objects(d, precision=0, reproduce=True)
+    s32, _ = device_objects(d, precision=1, reproduce=True)
+    s64.init_state(d["species0"], d["ideal"])
+    s32.init_state(d["species0"], d["ideal"])
+    keys = ("species", "pos", "moved", "chi", "chi2", "ms_C", "rung_of", "slot_of", "count")
+    diff, total = [], 0
+    for it in range(1000):
+        for k in keys:
+            s32.b[k].copy_(s64.b[k])
+        s32.lad.refresh_chi2()                  # chi^2 and chi(R) of that state in FP64
+        assert torch.allclose(s32.b["chi2"], s64.b["chi2"], rtol=1e-12, atol=0)
+        s32.lad.stepc.copy_(s64.lad.stepc)
+        s32._stepc = s64._stepc
+        a32 = s32.step().cpu().numpy()
+        a64 = s64.step().cpu().numpy()
+        total += a64.size
+        diff += [(it, r) for r in np.nonzero(a32 != a64)[0]]
+        if (it + 1) % 25 == 0:
+            s64.replica_exchange()
+    assert s64.lad.device_error() == 0 and s32.lad.device_error() == 0
+    ties = s32.lad.tie_stats().sum(0)
+    rate = len(diff) / total
+    print(f"{name}: {len(diff)} of {total} decisions differ ({rate:.2e}); "
+          f"{ties[0]:.0f} near-tie FP64 re-checks, {ties[1]:.0f} decisions changed by them")
+    assert rate <= 1e-3, (diff[:5], ties)
