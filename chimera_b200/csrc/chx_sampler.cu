@@ -31,6 +31,7 @@
 //      (kernels.py:328-346, 490-511; method_a_rmc.py:298-307).
 // The last CTA to finish advances the step counter, so a sequence of blocks
 // is a sequence of identical launches (CUDA-graph capturable).
+#include <cuda_bf16.h>
 #include "chx_device.cuh"
 #include "chx_mlp.cuh"
 
@@ -71,6 +72,13 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     // resampled rows, channel stride padded to even (channel pairs of the DFT)
     const size_t nchp = (size_t)L.nchan + (L.nchan & 1);
     s.u = o; o += f64 ? al16<double>(nchp * L.ncoef) : al16<float>(nchp * L.ncoef);
+    if (!f64 && L.xr && L.ft_frag) {
+        // the change's BF16 hi/lo operands of the tensor-core transform,
+        // channel-major with a padded row stride (tc_row_stride)
+        const size_t need = al16<uint16_t>((size_t)2 * ((L.nchan + 7) / 8 * 8) *
+                                           (L.ft_kt * 16 + 8));
+        if (o - s.u < need) o = s.u + need;
+    }
     size_t xs = f64 ? al16<double2>((size_t)kMaxSplit * L.nchan * L.nwin)
                     : al16<float2>((size_t)kMaxSplit * L.nchan * L.nwin);
     // the surrogate's scratch (partial sums of every warp + one activation
@@ -464,6 +472,180 @@ __device__ void chi2_profiled(const chx_ladder_t &L, GetM getm, const R2 *dx, do
     __syncthreads();
 }
 
+// The same chi^2 in one pass, anchored at the scale s0 of the slot's
+// current state: with r0 = s0 m - t, |s m - t|^2 = |r0|^2 + 2 (s - s0)
+// Re(m r0*) + (s - s0)^2 |m|^2, so per channel R = sum |r0|^2 / sigma^2,
+// Q = sum Re(m r0*) / sigma^2 and P = sum |m|^2 / sigma^2 are summed with
+// num and den in one sweep; R carries the size of chi^2 and the other terms
+// are small, so nothing cancels. For a state whose scale is s0, R is summed
+// exactly as chi2_profiled's second pass: a move that changes nothing
+// reproduces the current chi^2 bit for bit. *s_d2 as in chi2_profiled.
+template <int NSP, typename GetM, typename R2>
+__device__ void chi2_anchored(const chx_ladder_t &L, GetM getm, const R2 *dx, const double *s0,
+                              double *s_num, double *s_den, double *s_sq, double *s_scale,
+                              double *s_c2, double *s_d2) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nchan = L.nchan, nwin = L.nwin, nkw = L.nkw;
+    for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
+        const double sa = s0[ch / nkw];
+        double nu = 0.0, dn = 0.0, R = 0.0, Q = 0.0, Pp = 0.0, D = 0.0;
+        for (int q = lane; q < nwin; q += 32) {
+            const long g = (long)ch * nwin + q;
+            const double2 m = getm(g);
+            const double tr = L.tm_re[g], sg = L.sm[g];
+            if (L.cplx) {
+                const double ti = L.tm_im[g];
+                nu += m.x * tr + m.y * ti;
+                dn += m.x * m.x + m.y * m.y;
+                const double dr = (m.x * sa - tr) / sg;
+                const double di = (m.y * sa - ti) / sg;
+                R += dr * dr + di * di;
+                Q += (m.x * dr + m.y * di) / sg;
+                Pp += (m.x * m.x + m.y * m.y) / (sg * sg);
+            } else {
+                const double mag = sqrt(m.x * m.x + m.y * m.y);
+                nu += mag * tr;
+                dn += mag * mag;
+                const double dr = (mag * sa - tr) / sg;
+                R += dr * dr;
+                Q += mag * dr / sg;
+                Pp += mag * mag / (sg * sg);
+            }
+            const double a = dx[g].x, b = dx[g].y;
+            D += (a * a + b * b) * L.w2[g];
+        }
+        nu = warp_sum(nu);
+        dn = warp_sum(dn);
+        R = warp_sum(R);
+        Q = warp_sum(Q);
+        Pp = warp_sum(Pp);
+        D = warp_sum(D);
+        if (lane == 0) {
+            s_num[ch] = nu;
+            s_den[ch] = dn;
+            s_sq[ch] = R;
+            s_sq[12 + ch] = Q;
+            s_sq[24 + ch] = Pp;
+            s_sq[36 + ch] = D;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double tot = 0.0, d2 = 0.0;
+        for (int e = 0; e < NSP; ++e) {
+            double sc = 1.0;
+            if (L.profile) {
+                double nu = 0.0, dn = 0.0;
+                for (int q = 0; q < nkw; ++q) {
+                    nu += s_num[e * nkw + q];
+                    dn += s_den[e * nkw + q];
+                }
+                sc = nu / fmax(dn, 1e-30);
+            }
+            s_scale[e] = sc;
+        }
+        for (int ch = 0; ch < nchan; ++ch) {
+            const double sc = s_scale[ch / nkw], ds = sc - s0[ch / nkw];
+            tot += s_sq[ch];
+            if (ds != 0.0) tot += ds * (2.0 * s_sq[12 + ch] + ds * s_sq[24 + ch]);
+            d2 += sc * sc * s_sq[36 + ch];
+        }
+        *s_c2 = tot / L.nfit;
+        if (s_d2) *s_d2 = d2;
+    }
+    __syncthreads();
+}
+
+// The change's window transform on the tensor cores, FP32C with the kept
+// chi(R): the normalised change s_tr (nsp, nk) is resampled, windowed and
+// weighted by k^w as in ft_window, rounded to BF16 hi + lo (lo = the rest),
+// and X = W^T U is formed by mma m16n8k16 with the split-BF16 products
+// hi.hi + hi.lo + lo.hi accumulated in FP32 (W^T and its split prepared on
+// the host in A-fragment order, ft_frag). U sits in shared memory
+// channel-major with a row stride of KP + 8 taps, so the eight rows a B
+// fragment reads fall in different banks. Each warp owns m tiles (16 rows:
+// re/im of 8 window bins) and all n tiles (8 channels each); s_x receives
+// the change's chi(R) (channel-major, as ft_window writes it).
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint4 &a, uint32_t b0,
+                                         uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
+}
+
+template <int NSP>
+__device__ __noinline__ void ft_window_tc(const chx_ladder_t &L, const double *s_tr,
+                                          uint16_t *s_ub, float2 *s_x) {
+    constexpr int MAXNT = (3 * NSP + 7) / 8;        // n tiles of 8 channels
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    const int nk = L.nk, nchan = L.nchan, ncoef = L.ncoef, nkw = L.nkw, nwin = L.nwin;
+    const int mtn = L.ft_mt, ktn = L.ft_kt;
+    const int KS = ktn * 16 + 8;                    // row stride (taps) of U
+    const int nnt = (nchan + 7) >> 3, NP = nnt * 8;
+    uint16_t *uh = s_ub, *ul = s_ub + (long)NP * KS;
+    for (int q = tid; q < NP * KS; q += blockDim.x) {
+        const int ch = q / KS, j = q - ch * KS;
+        float u = 0.f;
+        if (ch < nchan && j < ncoef) {
+            const int e = ch / nkw;
+            const long g = (long)ch * ncoef + j;
+            const int id = L.ft_idx[g];
+            const double va = s_tr[e * nk + id], vb = s_tr[e * nk + id + 1];
+            u = (float)((va + (vb - va) * L.ft_frac[g]) * L.ft_w[g]);
+        }
+        const __nv_bfloat16 h = __float2bfloat16_rn(u);
+        const __nv_bfloat16 l = __float2bfloat16_rn(u - __bfloat162float(h));
+        uh[q] = __bfloat16_as_ushort(h);
+        ul[q] = __bfloat16_as_ushort(l);
+    }
+    __syncthreads();
+    const int gid = lane >> 2, tig = lane & 3;
+    const uint4 *Ah = (const uint4 *)L.ft_frag;
+    const uint4 *Al = Ah + (long)mtn * ktn * 32;
+    for (int mt = warp; mt < mtn; mt += nwarp) {
+        float acc[MAXNT][4];
+#pragma unroll
+        for (int t = 0; t < MAXNT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
+        const uint4 *ah_p = Ah + (long)mt * ktn * 32 + lane;
+        const uint4 *al_p = Al + (long)mt * ktn * 32 + lane;
+#pragma unroll 4
+        for (int kt = 0; kt < ktn; ++kt) {
+            const uint4 ah = __ldg(ah_p + kt * 32), al = __ldg(al_p + kt * 32);
+            const int k0 = kt * 16 + tig * 2;
+#pragma unroll
+            for (int t = 0; t < MAXNT; ++t) {
+                if (t < nnt) {
+                    const int rowo = (t * 8 + gid) * KS + k0;
+                    const uint32_t bh0 = *(const uint32_t *)&uh[rowo];
+                    const uint32_t bh1 = *(const uint32_t *)&uh[rowo + 8];
+                    const uint32_t bl0 = *(const uint32_t *)&ul[rowo];
+                    const uint32_t bl1 = *(const uint32_t *)&ul[rowo + 8];
+                    mma_bf16(acc[t], ah, bh0, bh1);
+                    mma_bf16(acc[t], ah, bl0, bl1);
+                    mma_bf16(acc[t], al, bh0, bh1);
+                }
+            }
+        }
+        // D: c0, c1 at row gid, columns tig*2, tig*2+1; c2, c3 at row gid + 8
+#pragma unroll
+        for (int t = 0; t < MAXNT; ++t) {
+            if (t >= nnt) continue;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int row = mt * 16 + gid + 8 * (r >> 1), col = t * 8 + tig * 2 + (r & 1);
+                const int q = row >> 1;
+                if (q < nwin && col < nchan) {
+                    float *o = (float *)&s_x[col * nwin + q];
+                    o[row & 1] = acc[t][r];
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
 // Steps 4-5 (and the whole of k_eval_chi2): trial chi(R) on the window bins
 // (ft_window), then the profiled chi^2 into *s_c2. In FP32C with xr_base
 // (the slot's FP64 chi(R) on the window) s_tr holds a move's change alone:
@@ -475,12 +657,19 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real
                         typename Real<PREC>::T2 *s_x, double *s_num, double *s_den,
                         double *s_sq, double *s_scale, double *s_c2,
                         const double *xr_base = nullptr, double *s_d2 = nullptr,
-                        int max_split = kMaxSplit) {
+                        int max_split = kMaxSplit, const double *xs_base = nullptr) {
     typedef typename Real<PREC>::T real;
     typedef typename Real<PREC>::T2 real2;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nchan = L.nchan, nwin = L.nwin, nkw = L.nkw;
-    ft_window<NSP, PREC>(L, s_tr, s_u, s_x, max_split);
+    if constexpr (PREC != CHX_FP64) {
+        if (xr_base && L.ft_frag)
+            ft_window_tc<NSP>(L, s_tr, (uint16_t *)s_u, (float2 *)s_x);
+        else
+            ft_window<NSP, PREC>(L, s_tr, s_u, s_x, max_split);
+    } else {
+        ft_window<NSP, PREC>(L, s_tr, s_u, s_x, max_split);
+    }
 
     if constexpr (PREC != CHX_FP64) {
         if (xr_base) {
@@ -490,7 +679,7 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real
                 const real2 d = s_x[g];
                 return make_double2((double)d.x + xr_base[2 * g], (double)d.y + xr_base[2 * g + 1]);
             };
-            chi2_profiled<NSP>(L, getm, s_x, s_num, s_den, s_sq, s_scale, s_c2, s_d2);
+            chi2_anchored<NSP>(L, getm, s_x, xs_base, s_num, s_den, s_sq, s_scale, s_c2, s_d2);
             return;
         }
         // one pass: per channel num = Re<m,t>, den = <m,m> (the profiled scale)
@@ -813,6 +1002,11 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     const bool use_xr = (PREC != CHX_FP64) && L.xr != nullptr;
     const bool tie_terms = use_xr && L.tie_eps > 0.0 && L.tie_gain > 0.0;
     double *XR = use_xr ? L.xr + (long)c * L.nchan * L.nwin * 2 : nullptr;
+    double *XS = use_xr ? L.xs + (long)c * NSP : nullptr;
+    if (use_xr && !L.xs) {      // the anchored chi^2 needs the state's scales
+        if (threadIdx.x == 0) atomicOr(err, CHX_DEVERR_INDEX);
+        return;
+    }
     const float *msT32 = L.ms_T32;
     const bool da_on = DA && s_daon != 0;
     const bool log_on = DA && L.log_cap > 0 && L.log_codes != nullptr && L.log_y != nullptr;
@@ -1232,7 +1426,8 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         __syncthreads();
 
         // ---- 4-5. trial chi(R) on the window and its profiled chi^2
-        ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2, XR, &s_d2);
+        ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2, XR, &s_d2,
+                           kMaxSplit, XS);
 
         // ---- 6. Metropolis
         if (tid == 0) {
@@ -1358,6 +1553,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             for (int q = tid; q < NSP * nk; q += blockDim.x) s_chi[q] += s_dchi[q];
             if (use_xr) {
                 const int nx = L.nchan * L.nwin;
+                if (tid < NSP) XS[tid] = s_scale[tid];
                 if (s_tie) {        // the FP64 trial chi(R) of the near-tie test
                     const double *x64 =
                         (const double *)(smem + so.u +
@@ -1487,6 +1683,7 @@ __global__ void __launch_bounds__(kStepThreads) k_eval_chi2(const chx_ladder_t *
                 X[2 * q] = x64[q].x;
                 X[2 * q + 1] = x64[q].y;
             }
+            if (tid < NSP && L.xs) L.xs[(long)c * NSP + tid] = s_scale[tid];
         }
     } else {
         ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2);
@@ -1959,6 +2156,9 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
                         L.nkw <= 3 && L.nchan == L.nsp * L.nkw && (L.nfft & (L.nfft - 1)) == 0 &&
                         L.natoms < (1 << 20) && L.nwin > 0,
                     "sampler: ladder %d outside the built limits", i);
+        CHX_REQUIRE(!L.ft_frag || (L.xr && L.ft_mt * 16 >= 2 * L.nwin && L.ft_kt * 16 >= L.ncoef &&
+                                   L.ft_mt > 0 && L.ft_kt > 0),
+                    "sampler: ladder %d has transform fragments that do not cover its window", i);
         CHX_REQUIRE(L.nrep >= 1 && L.nrep <= kMaxExchRungs,
                     "sampler: ladder %d has %d rungs (1..%d)", i, L.nrep, kMaxExchRungs);
         CHX_REQUIRE(!L.mlp || (L.da_on && L.da_stat),

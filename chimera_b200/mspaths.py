@@ -508,6 +508,16 @@ class SupercellPaths:
         return self._dev
 
 
+def _host_array(x):
+    """NumPy copy of a host or device array (a torch tensor, or an object
+    with a `get()` or `cpu()` method)."""
+    if hasattr(x, "detach"):
+        return x.detach().cpu().numpy()
+    if hasattr(x, "get"):
+        return np.asarray(x.get())
+    return np.asarray(x)
+
+
 class SupercellMS:
     """Per-replica entry counts on the device (chimera/mslibrary.py:341-492).
 
@@ -516,21 +526,75 @@ class SupercellMS:
     chx_ms_delta. The sampler itself applies the deltas inside its fused step.
     """
 
-    def __init__(self, paths: SupercellPaths, table):
+    def __init__(self, paths, table=None):
+        """SupercellMS(SupercellPaths, table), or the reference's own call
+        SupercellMS(lib, S) (chimera/mslibrary.py:351-404): lib a path library
+        (its classes, species count and `table`), S the spectrum whose
+        reference supercell (a0_ref, ideal0, H0) the paths are laid on; the
+        table then comes from set_params, as in the reference."""
         import torch
+        self.lib = None
+        if not isinstance(paths, SupercellPaths):
+            lib, S = paths, table
+            paths = SupercellPaths(list(lib.classes), S.ideal0, S.H0, float(S.a0_ref),
+                                   int(lib.nsp))
+            self.lib, table = lib, None
         self.paths = paths
         self.nsp, self.nblk, self.nent = paths.nsp, paths.nblk, paths.nent
         self.natoms, self.npath, self.M = paths.natoms, paths.npath, paths.M
-        T = np.ascontiguousarray(table, np.float64)
-        assert T.shape[0] == self.nent, f"table has {T.shape[0]} rows, need {self.nent}"
-        self.T = N.to_dev(T)
-        self.nk = T.shape[1]
+        self.T, self.nk = None, None
+        if table is not None:
+            self.set_table(table)
         self.C = None
+        self._dC = None
         self._torch = torch
 
+    @classmethod
+    def adopt(cls, ms, cell):
+        """This class for an MS object built elsewhere: the reference's own
+        SupercellMS (it carries its library `lib` and device table `T` but no
+        paths of this package), laid on `cell` (ideal, H, a0: the forward
+        model's supercell); objects of this class are returned as they are."""
+        if ms is None or isinstance(ms, cls):
+            return ms
+        lib = getattr(ms, "lib", None)
+        if lib is None or getattr(ms, "T", None) is None:
+            raise TypeError("an MS library needs its path library (lib) and table (T)")
+        paths = SupercellPaths(list(lib.classes), np.asarray(cell.ideal), np.asarray(cell.H),
+                               float(cell.a0), int(lib.nsp))
+        out = cls(paths, _host_array(ms.T))
+        out.lib = lib
+        return out
+
     def set_table(self, table):
-        self.T = N.to_dev(np.ascontiguousarray(table, np.float64))
+        T = np.ascontiguousarray(table, np.float64)
+        if T.shape[0] != self.nent:
+            raise ValueError(f"table has {T.shape[0]} rows, need {self.nent}")
+        self.T = N.to_dev(T)
+        self.nk = T.shape[1]
         return self
+
+    def set_params(self, sigma2_nn, r_nn, c_ms=1.3, amp=1.0, s02=1.0, a_scale=1.0):
+        """The library's table at these parameters (mslibrary.py:406-408)."""
+        if self.lib is None:
+            raise ValueError("set_params needs the path library (SupercellMS(lib, S))")
+        return self.set_table(_host_array(self.lib.table(sigma2_nn, r_nn, c_ms, amp, s02,
+                                                         a_scale)))
+
+    def expected_chi(self, composition=None):
+        """Random-alloy chi_MS per absorbing atom (nsp, nk), NumPy
+        (mslibrary.py:410-413)."""
+        return self.lib.chi_counts(self.lib.expected_counts(composition), _host_array(self.T))
+
+    def commit(self, acc):
+        """Apply the last delta where accepted (mslibrary.py:488-489)."""
+        torch = self._torch
+        a = torch.as_tensor(acc).to("cuda").to(self.C.dtype)
+        self.C = self.C + self._dC * a[:, None]
+
+    def permute(self, ix):
+        """Follow a replica exchange (mslibrary.py:491-492)."""
+        self.C = self.C[self._torch.as_tensor(ix).to("cuda").long()]
 
     def counts(self, species):
         torch = self._torch

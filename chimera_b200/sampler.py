@@ -56,6 +56,46 @@ def _fp32_rows(t):
     return out
 
 
+def _bf16_bits(x):
+    """Round float32 values to BF16 (nearest, ties to even): the bit patterns
+    (uint16) and the rounded values (float32)."""
+    b = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16).astype(np.uint32)
+    return r.astype(np.uint16), (r << 16).view(np.float32)
+
+
+def transform_fragments(f, win):
+    """The fit-window transform W^T as split-BF16 A operands of mma m16n8k16
+    (row-major A, the fragment layout of the PTX ISA): rows 2q (re) and
+    2q + 1 (im) of window bin q, columns the ncoef taps of the shared tap run,
+    entries norm * (cos, -sin)(2 pi n m_q / nfft), n = n0 + tap; hi = BF16(W),
+    lo = BF16(W - hi). Returns (uint32 array [2][mt][kt][32][4], mt, kt)."""
+    ncoef, nfft = int(f["ncoef"]), int(f["nfft"])
+    win = np.asarray(win, np.int64)
+    n = int(f["n0"][0]) + np.arange(ncoef)
+    ph = (np.outer(win, n) % nfft).astype(np.float64) * (2.0 * np.pi / nfft)
+    Wt = np.zeros((2 * win.size, ncoef))
+    Wt[0::2] = np.cos(ph) * f["norm"]
+    Wt[1::2] = -np.sin(ph) * f["norm"]
+    mt, kt = -(-Wt.shape[0] // 16), -(-ncoef // 16)
+    Wp = np.zeros((mt * 16, kt * 16), np.float32)
+    Wp[:Wt.shape[0], :ncoef] = Wt
+    hi_bits, hi = _bf16_bits(Wp)
+    lo_bits, _ = _bf16_bits(Wp - hi)
+    lane = np.arange(32)
+    gid, tig = lane >> 2, lane & 3
+    out = np.zeros((2, mt, kt, 32, 4), np.uint32)
+    for part, bits in enumerate((hi_bits, lo_bits)):
+        B = bits.astype(np.uint32).reshape(mt, 16, kt, 16).transpose(0, 2, 1, 3)  # [mt][kt][r][c]
+        for r in range(4):
+            row = gid + 8 * (r & 1)
+            col = tig * 2 + 8 * (r >> 1)
+            e0 = B[:, :, row, col]          # (mt, kt, 32)
+            e1 = B[:, :, row, col + 1]
+            out[part, :, :, :, r] = e0 | (e1 << 16)
+    return out, mt, kt
+
+
 def _window_gain(f, win, sm, nsp, nk):
     """sqrt of the largest eigenvalue, over the edges, of B^H W B: B the map
     from an edge's normalised chi(k) (nk) to its channels' chi(R) on the fit
@@ -146,7 +186,10 @@ class LadderSpec:
         self.swap_frac, self.disp_sigma, self.max_disp = swap_frac, disp_sigma, max_disp
         self.profile_scale = bool(profile_scale)
         self.energy_prior = energy_prior
-        self.ms = ms_library
+        # the package's MS object, or the reference's own SupercellMS adopted
+        # onto the forward model's supercell
+        from .mspaths import SupercellMS
+        self.ms = SupercellMS.adopt(ms_library, fm.cell) if ms_library is not None else None
 
 
 class Ladders:
@@ -157,6 +200,9 @@ class Ladders:
     # rounding used by the near-tie FP64 re-check (0: off)
     delta_transform = True
     tie_eps = 3e-5
+    # FP32C with the kept chi(R): the change's window transform as split-BF16
+    # tensor-core products (ft_frag of chx_ladder_t) instead of the FP32 DFT
+    tc_transform = True
 
     def __init__(self, specs, precision=FP64, use_table=True, threads=256, min_blocks=3):
         import torch
@@ -370,7 +416,9 @@ class Ladders:
             b["xr"] = torch.zeros((nrep, f["nchan"], int(win.size), 2), dtype=torch.float64,
                                   device="cuda")
             b["tie_stat"] = torch.zeros((nrep, 2), dtype=torch.float64, device="cuda")
-            self.keep += [b["xr"], b["tie_stat"]]
+            b["xs"] = torch.ones((nrep, nsp), dtype=torch.float64, device="cuda")
+            self.keep += [b["xr"], b["tie_stat"], b["xs"]]
+            L.xs = N.dptr(b["xs"])
             L.xr, L.tie_stat, L.tie_eps = N.dptr(b["xr"]), N.dptr(b["tie_stat"]), self.tie_eps
             # the FP32 terms' share of the near-tie bound: row maxima of the
             # tables the step rounds to FP32, and the transform's gain
@@ -387,9 +435,21 @@ class Ladders:
             else:
                 L.ms_T_max = 0
             L.tie_gain = _window_gain(f, win, sm, nsp, nk)
+            # the change's transform on the tensor cores (split BF16)
+            if self.tc_transform:
+                key = tuple(win.tolist())
+                fc = fcache.setdefault(("ft_frag", id(s.ft)), {})
+                if key not in fc:
+                    frag, mt, kt = transform_fragments(f, win)
+                    fc[key] = (self._t(frag.reshape(-1).view(np.int32)), mt, kt)
+                b["ft_frag"], L.ft_mt, L.ft_kt = fc[key]
+                L.ft_frag = N.dptr(b["ft_frag"])
+            else:
+                L.ft_frag, L.ft_mt, L.ft_kt = 0, 0, 0
         else:
             L.xr, L.tie_stat, L.tie_eps = 0, 0, 0.0
-            L.sstab_max, L.ms_T_max, L.tie_gain = 0, 0, 0.0
+            L.sstab_max, L.ms_T_max, L.tie_gain, L.xs = 0, 0, 0.0, 0
+            L.ft_frag, L.ft_mt, L.ft_kt = 0, 0, 0
         b["beta_host"] = beta
         b["cplx"] = cplx
         return b
@@ -704,7 +764,7 @@ class RMCSampler:
                                seed=seed, swap_frac=swap_frac, disp_sigma=disp_sigma,
                                max_disp=max_disp, profile_scale=profile_scale,
                                energy_prior=energy_prior, ms_library=ms_library)
-        self.ms = ms_library
+        self.ms = self.spec.ms
         self.lad = Ladders([self.spec], precision=precision, use_table=use_table)
         self.b = self.lad.bufs[0]
         self.complex = self.b["cplx"]

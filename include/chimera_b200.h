@@ -385,6 +385,19 @@ typedef struct {
        k-space error into one on its weighted chi(R) norm */
     const float *sstab_max, *ms_T_max;
     double tie_gain;
+    /* with xr: (nrep, nsp) the profiled scale of each slot's current state,
+       the anchor of the step's one-pass chi^2 (written with xr) */
+    double *xs;
+    /* with xr, optional: the window transform as split-BF16 tensor-core
+       operands, so the step transforms a move's change with three BF16
+       products (hi.hi + hi.lo + lo.hi, FP32 accumulation; mma m16n8k16) in
+       place of the FP32 DFT. W^T (2 nwin rows: re, im of each window bin;
+       ncoef tap columns; the transform norm folded in) in A-fragment order:
+       [part hi/lo][m tile (16 rows)][k tile (16 taps)][lane][4 x uint32],
+       ft_mt = ceil(2 nwin / 16) m tiles, ft_kt = ceil(ncoef / 16) k tiles,
+       zero padded. NULL: the FP32 DFT. */
+    const uint32_t *ft_frag;
+    int ft_mt, ft_kt;
 } chx_ladder_t;
 
 /* Bytes of dynamic shared memory the step kernel needs for these ladders. */

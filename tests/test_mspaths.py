@@ -239,3 +239,34 @@ def test_templates_cover_incident_paths_on_bcc_and_hcp(lattice, a0, nc):
                     sp.cls_off, nsp, sp.nblk, np.array([a], np.int32), np.array([b], np.int32),
                     np.array([species[b]], np.int32), np.array([species[a]], np.int32))[0]
     assert np.array_equal(C1 - C0, dC)
+
+
+@pytest.mark.parametrize("nsp", [2, 3])
+def test_reference_construction_lays_the_same_paths(classes, nsp):
+    """SupercellMS(lib, S), the call chimera/model.py:335 makes with its path
+    library and spectrum, lays the reference's path arrays (the golden digest
+    of SupercellMS.__init__, mslibrary.py:351-404) on the spectrum's reference
+    supercell; set_params then takes the library's table, as the reference."""
+    import types
+    g = golden("ms.npz")
+    cell = L.CrystalSupercell("fcc", (5, 5, 5), 3.59)
+    calls = []
+
+    class Lib:                  # the parts of PathLibrary the construction reads
+        def __init__(self):
+            self.classes, self.nsp = classes, nsp
+
+        def table(self, *args):
+            calls.append(args)
+            return np.zeros((nsp * sum(nsp ** c.nslot for c in classes), 4))
+
+    S = types.SimpleNamespace(a0_ref=3.59, ideal0=cell.ideal, H0=cell.H)
+    ms = MP.SupercellMS(Lib(), S)
+    sp = ms.paths
+    key = f"sc{nsp}_"
+    assert sp.npath == int(g[key + "npath"]) and sp.M == int(g[key + "M"])
+    P_abs = np.r_[sp.p_abs, 0].astype(np.int32)
+    P_cls = np.r_[sp.p_cls, 0].astype(np.int32)
+    P_slot = np.vstack([sp.p_slot, -np.ones((1, 3), np.int32)]).astype(np.int32)
+    assert digest(P_abs, P_cls, P_slot, sp.inc) == str(g[key + "digest"])
+    assert ms.T is None and ms.lib is not None
