@@ -67,8 +67,7 @@ class Ladder(C.Structure):
         ("exch_att", c_p), ("exch_acc", c_p),
         ("mlp", c_p), ("feat_nbr", c_p), ("feat_D", c_i), ("da_on", c_p), ("da_stat", c_p),
         ("log_codes", c_p), ("log_y", c_p), ("log_cap", c_i64), ("best_stale", c_p),
-        ("xr", c_p), ("tie_eps", c_d), ("tie_stat", c_p), ("sstab_max", c_p), ("ms_T_max", c_p),
-        ("tie_gain", c_d), ("xs", c_p), ("ft_frag", c_p), ("ft_mt", c_i), ("ft_kt", c_i)]
+        ("xr", c_p), ("tie_eps", c_d), ("tie_stat", c_p), ("tie_gdiag", c_p), ("xs", c_p), ("ft_frag", c_p), ("ft_mt", c_i), ("ft_kt", c_i)]
 
 
 class Mlp(C.Structure):

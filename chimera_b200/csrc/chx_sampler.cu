@@ -42,11 +42,15 @@ constexpr int kMaxCoord = 256;
 constexpr int kReseed = 32;      // taps between exact twiddles in the transform
 constexpr int kMaxSplit = 2;     // threads sharing one bin's taps
 constexpr int kUndo = 32;        // accepted moves kept after a slot's best point
-// relative error bounds of the FP32 parts of a move's change, for the near-tie
-// test: a direct record's term (FP32 exp, sin of an FP64-reduced phase and
-// amplitude products), and a table row rounded from FP64 to FP32 (2^-24)
-constexpr double kEpsRec = 1e-6;
-constexpr double kEpsTab = 6.0e-8;
+// The near-tie test's model of the FP32 parts of a move's change: each is an
+// independent relative rounding of RMS at most eps (a direct record's term:
+// FP32 exp, sin of an FP64-reduced phase, amplitude products; an MS row rounded
+// from FP64 to FP32: 2^-24 / sqrt(3)), summed in quadrature, and the bound
+// taken at kTieSigma standard deviations; the (shell, type) rows and every
+// accumulation of the change are FP64 and add nothing
+constexpr double kEpsRec = 2e-7;
+constexpr double kEpsTab = 3.5e-8;
+constexpr double kTieSigma = 6.0;
 
 // Shared-memory carve-up of one step CTA (all offsets 16-byte aligned).
 // The near-tie FP64 transforms reuse the span u .. dirv (the resampled rows,
@@ -798,6 +802,34 @@ __device__ __noinline__ void tie_delta64(const chx_ladder_t &L, const PairRec *s
     __syncthreads();
 }
 
+// The near-tie re-check's arithmetic (out of line, off the hot path): the
+// change in FP64 (tie_delta64), its FP64 window transform in the span the
+// step reserves for it, and the trial chi^2 from the slot's FP64 chi(R) plus
+// that transform (chi2_anchored, as the step's own chi^2) into *s_c2t.
+template <int NSP>
+__device__ __noinline__ void tie_recheck(const chx_ladder_t &L, const StepSmem &so,
+                                         unsigned char *smem, const PairRec *s_dir,
+                                         const int *s_list, int ndirmax, int ndn,
+                                         const int *s_msb, int ndir, int ndnz, double *s_dchi,
+                                         double *s_tr, const double *CNT, const double *XR,
+                                         const double *XS, double *s_num, double *s_den,
+                                         double *s_sq, double *s_scale, double *s_c2t) {
+    const int nk = L.nk;
+    tie_delta64<NSP>(L, s_dir, s_list, ndirmax, ndn, s_msb, ndir, ndnz, s_dchi);
+    double *u64 = (double *)(smem + so.u);
+    double2 *x64 =
+        (double2 *)(smem + so.u + al16<double>((size_t)(L.nchan + (L.nchan & 1)) * L.ncoef));
+    for (int q = threadIdx.x; q < NSP * nk; q += blockDim.x)
+        s_tr[q] = s_dchi[q] / fmax(CNT[q / nk], 1.0);
+    __syncthreads();
+    ft_window<NSP, CHX_FP64>(L, s_tr, u64, x64, 1);
+    auto getm = [&](long g) {
+        const double2 d = x64[g];
+        return make_double2(d.x + XR[2 * g], d.y + XR[2 * g + 1]);
+    };
+    chi2_anchored<NSP>(L, getm, x64, XS, s_num, s_den, s_sq, s_scale, s_c2t, nullptr);
+}
+
 // Stage 1 of delayed acceptance for a swap of a and b (species differ),
 // run by every thread of the step CTA: the surrogate's input (sites lo < hi,
 // their neighbourhoods in the feature order, code NSP for lo and hi
@@ -901,11 +933,11 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     __shared__ int s_msb[NSP + 1];
     __shared__ chx_mlp_t s_mlp;
     __shared__ double s_dhat, s_dast[4];
-    __shared__ double s_d2, s_xo, s_xd, s_uu, s_c2t, s_c2c;   // near-tie re-check
+    __shared__ double s_d2, s_xo, s_xd, s_uu, s_c2t;   // near-tie re-check
     __shared__ int s_tie;
-    // near-tie bound of the FP32 terms: per warp, sum |count| x row max of the
-    // table / MS rows by absorber, and the squared k-space error bound
-    __shared__ double s_mtab[NT / 32][NSP], s_e2w[NT / 32];
+    // near-tie bound of the FP32 terms: per warp, the expected squared
+    // weighted chi(R) norm of the change's rounding
+    __shared__ double s_e2w[NT / 32];
     __shared__ float s_sigma;
     __shared__ int s_daon, s_skip;
     __shared__ long long s_logi;
@@ -1000,7 +1032,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     __syncthreads();
     const bool use_tab = (PREC != CHX_FP64) && L.sstab32 != nullptr;
     const bool use_xr = (PREC != CHX_FP64) && L.xr != nullptr;
-    const bool tie_terms = use_xr && L.tie_eps > 0.0 && L.tie_gain > 0.0;
+    const bool tie_terms = use_xr && L.tie_eps > 0.0 && L.tie_gdiag != nullptr;
     double *XR = use_xr ? L.xr + (long)c * L.nchan * L.nwin * 2 : nullptr;
     double *XS = use_xr ? L.xs + (long)c * NSP : nullptr;
     if (use_xr && !L.xs) {      // the anchored chi^2 needs the state's scales
@@ -1021,11 +1053,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         }
         for (int e = tid; e < nent; e += blockDim.x) s_hist[e] = 0;
         for (int e = tid; e < ndn; e += blockDim.x) s_dn[e] = 0;
-        if (tid < NT / 32) {
-            s_e2w[tid] = 0.0;
-#pragma unroll
-            for (int q = 0; q < NSP; ++q) s_mtab[tid][q] = 0.0;
-        }
+        if (tid < NT / 32) s_e2w[tid] = 0.0;
         __syncthreads();
         const int a = prop.a, b = prop.b, nsa = prop.nsa, nsb = prop.nsb, swp = prop.swap;
 
@@ -1201,17 +1229,11 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         {
             int off = 0;
             for (int w = 0; w < warp; ++w) off += s_wcnt[w];
-            double mt[NSP];
-#pragma unroll
-            for (int q = 0; q < NSP; ++q) mt[q] = 0.0;
             for (int i0 = ms0; i0 < ms1; i0 += 32) {
                 const int i = i0 + lane;
                 const int v = i < ms1 ? s_hist[i] : 0;
                 const unsigned m = __ballot_sync(0xffffffffu, v != 0);
                 if (v != 0) l_ms[off + __popc(m & ((1u << lane) - 1))] = make_int2(i, v);
-                if (tie_terms && v != 0 && L.ms_T_max)
-                    add_by_species<NSP>(mt, i / L.ms_nblk,
-                                        fabs((double)v) * (double)L.ms_T_max[i]);
                 // list position of each absorber block's first entry, by the
                 // warp whose run holds the block's first index
                 if (lane < NSP) {
@@ -1220,13 +1242,6 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                         s_msb[lane] = off + __popc(m & ((1u << d) - 1));
                 }
                 off += __popc(m);
-            }
-            if (tie_terms) {
-#pragma unroll
-                for (int q = 0; q < NSP; ++q) {
-                    const double t = warp_sum(mt[q]);
-                    if (lane == 0) s_mtab[warp][q] += t;
-                }
             }
             if (warp == nwarp - 1) {
                 if (lane == 0) s_nhist = off;
@@ -1240,22 +1255,6 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         } else if (warp == 1) {
             int n = warp_compact_pairs(ndn, s_dn, l_dn);
             if (lane == 0) s_ndn = n;
-            if (tie_terms && L.sstab_max) {
-                __syncwarp();
-                double mt[NSP];
-#pragma unroll
-                for (int q = 0; q < NSP; ++q) mt[q] = 0.0;
-                for (int q = lane; q < n; q += 32) {
-                    const int2 jc = l_dn[q];
-                    add_by_species<NSP>(mt, (jc.x % nn) / NSP,
-                                        fabs((double)jc.y) * (double)L.sstab_max[jc.x]);
-                }
-#pragma unroll
-                for (int q = 0; q < NSP; ++q) {
-                    const double t = warp_sum(mt[q]);
-                    if (lane == 0) s_mtab[1][q] += t;    // after this warp's MS share
-                }
-            }
         }
         __syncthreads();
 
@@ -1298,12 +1297,12 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                         d.t &= 0xFFFF;
                         const double v = rec_term<NSP, PREC>(d, kc);
                         add_by_species<NSP>(acc, d.t / NSP, neg ? -v : v);
-                        if (tie_terms) add_by_species<NSP>(gab, d.t / NSP, fabs(v));
+                        if (tie_terms) add_by_species<NSP>(gab, d.t / NSP, v * v);
                     }
 #pragma unroll
                     for (int s = 0; s < NSP; ++s) {
                         s_dchi[s * nk + ik] = acc[s];
-                        // the records' sum of |term|, read back by the item
+                        // the records' sum of term^2, read back by the item
                         // of (s, ik) below before it writes the trial there
                         if (tie_terms) s_tr[s * nk + ik] = gab[s];
                     }
@@ -1322,15 +1321,57 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                     if (k1ok) acc1 = s_dchi[sa_ * nk + k0 + 1];
                 }
                 if (use_tab) {
-                    for (int q = 0; q < ndnz; ++q) {
-                        const int2 jc = l_dn[q];
-                        if ((jc.x % nn) / NSP != sa_) continue;
-                        const float2 t = __ldg((const float2 *)&L.sstab32[(long)jc.x * nk2 + k0]);
-                        acc0 += (double)((float)jc.y * t.x);
-                        acc1 += (double)((float)jc.y * t.y);
+                    if (use_xr) {
+                        // FP64 (shell, type) rows: few rows, no rounding
+                        for (int q = 0; q < ndnz; ++q) {
+                            const int2 jc = l_dn[q];
+                            if ((jc.x % nn) / NSP != sa_) continue;
+                            const double *t = L.sstab + (long)jc.x * nk + k0;
+                            acc0 = fma((double)jc.y, __ldg(t), acc0);
+                            if (k1ok) acc1 = fma((double)jc.y, __ldg(t + 1), acc1);
+                        }
+                    } else {
+                        for (int q = 0; q < ndnz; ++q) {
+                            const int2 jc = l_dn[q];
+                            if ((jc.x % nn) / NSP != sa_) continue;
+                            const float2 t =
+                                __ldg((const float2 *)&L.sstab32[(long)jc.x * nk2 + k0]);
+                            acc0 += (double)((float)jc.y * t.x);
+                            acc1 += (double)((float)jc.y * t.y);
+                        }
                     }
                 }
-                {
+                double v0 = 0.0, v1 = 0.0;   // sum (count x row)^2 of the MS rows
+                if (use_xr) {
+                    // FP32 MS rows, FP64 accumulation
+                    const int q0 = s_msb[sa_], q1 = s_msb[sa_ + 1];
+                    double m0 = 0.0, m1 = 0.0;
+                    if (tie_terms) {
+#pragma unroll 16
+                        for (int q = q0; q < q1; ++q) {
+                            const int2 ec = l_ms[q];
+                            const float2 t =
+                                __ldg((const float2 *)&msT32[(long)ec.x * nk2 + k0]);
+                            const double p0 = (double)ec.y * (double)t.x;
+                            const double p1 = (double)ec.y * (double)t.y;
+                            m0 += p0;
+                            m1 += p1;
+                            v0 = fma(p0, p0, v0);
+                            v1 = fma(p1, p1, v1);
+                        }
+                    } else {
+#pragma unroll 16
+                        for (int q = q0; q < q1; ++q) {
+                            const int2 ec = l_ms[q];
+                            const float2 t =
+                                __ldg((const float2 *)&msT32[(long)ec.x * nk2 + k0]);
+                            m0 = fma((double)ec.y, (double)t.x, m0);
+                            m1 = fma((double)ec.y, (double)t.y, m1);
+                        }
+                    }
+                    acc0 += m0;
+                    acc1 += m1;
+                } else {
                     const int q0 = s_msb[sa_], q1 = s_msb[sa_ + 1];
                     float2 sm = make_float2(0.f, 0.f);
 #pragma unroll 16
@@ -1346,17 +1387,20 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 const double inv = fmax(CNT[sa_], 1.0);
                 const int o = sa_ * nk + k0;
                 if (tie_terms) {
-                    // |FP32 error| of the change at (sa_, k) <= eps_rec sum |record
-                    // terms| + eps_tab sum |count| x row max
-                    double mt = 0.0;
-                    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mt += s_mtab[w][sa_];
+                    // the change's rounding at (sa_, k): variance eps_rec^2 sum
+                    // term^2 + eps_tab^2 sum (count x row)^2 + eps_tr^2 change^2
+                    // (the transform's rounding, of relative RMS eps_tr = tie_eps,
+                    // acts as an independent error on each input), weighted by
+                    // the transform's gain at k
+                    const double *gd = L.tie_gdiag + (long)sa_ * nk;
+                    const double et2 = L.tie_eps * L.tie_eps;
                     const double g0 = ndir ? s_tr[o] : 0.0;
-                    const double e0 = (kEpsRec * g0 + kEpsTab * mt) / inv;
-                    e2acc += e0 * e0;
+                    e2acc += (kEpsRec * kEpsRec * g0 + kEpsTab * kEpsTab * v0 + et2 * acc0 * acc0) *
+                             gd[k0] / (inv * inv);
                     if (k1ok) {
                         const double g1 = ndir ? s_tr[o + 1] : 0.0;
-                        const double e1 = (kEpsRec * g1 + kEpsTab * mt) / inv;
-                        e2acc += e1 * e1;
+                        e2acc += (kEpsRec * kEpsRec * g1 + kEpsTab * kEpsTab * v1 +
+                                  et2 * acc1 * acc1) * gd[k0 + 1] / (inv * inv);
                     }
                 }
                 s_dchi[o] = acc0;
@@ -1466,22 +1510,19 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 u = u01(splitmix64(h));
             }
             int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
-            // a near tie: the FP32 transform of the change may move x by up to
-            // tau = beta * 2 eps sqrt(chi^2_tot * sum s^2 |change|^2 / sigma^2)
-            // (Cauchy-Schwarz on the first-order term); if x - tau and x + tau
-            // decide differently, the test is redone in FP64 below
-            // plus the FP32 terms' share: an error e(k) of the change moves x by
-            // at most beta * 2 (||r|| + ||change||) s tie_gain ||e||
+            // a near tie: a rounding e(k) of the change (FP32 terms and rows,
+            // the transform) moves x by at most beta * 2 (||r|| + ||change||)
+            // s ||B e||_W (Cauchy-Schwarz on the chi^2 change; B the window
+            // transform, W = 1 / sigma^2), ||B e||_W taken at kTieSigma
+            // standard deviations of the rounding model; if x - tau and
+            // x + tau decide differently, the test is redone in FP64 below
             s_tie = 0;
-            if (use_xr && L.tie_eps > 0.0) {
+            if (tie_terms) {
                 const double rn = sqrt(fmax(c2, 0.0) * L.nfit), dn = sqrt(fmax(s_d2, 0.0));
-                double tau = beta * 2.0 * L.tie_eps * rn * dn;
-                if (tie_terms) {
-                    double e2 = 0.0, smax = 0.0;
-                    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) e2 += s_e2w[w];
-                    for (int q = 0; q < NSP; ++q) smax = fmax(smax, fabs(s_scale[q]));
-                    tau += beta * 2.0 * (rn + dn) * smax * L.tie_gain * sqrt(e2);
-                }
+                double e2 = 0.0, smax = 0.0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w) e2 += s_e2w[w];
+                for (int q = 0; q < NSP; ++q) smax = fmax(smax, fabs(s_scale[q]));
+                const double tau = beta * 2.0 * (rn + dn) * smax * kTieSigma * sqrt(e2);
                 const double xl = x - tau, xh = x + tau;
                 const int al = (xl <= 0.0) || (u < exp(-fmin(xl, 60.0)));
                 const int ah = (xh <= 0.0) || (u < exp(-fmin(xh, 60.0)));
@@ -1495,29 +1536,17 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         }
         __syncthreads();
         if (PREC != CHX_FP64 && s_tie) {
-            // the R-factor comparison in FP64: first the move's change again
-            // with FP64 terms (the direct records' FP64 term, the FP64 (shell,
-            // type) and MS rows), replacing the FP32 one; then chi^2 of the
-            // current and the trial chi(k) through FP64 transforms, in the span
-            // of the resampled rows / transform / direct records
-            tie_delta64<NSP>(L, s_dir, s_list, 2 * maxaff, ndn, s_msb, s_ndir, s_ndn, s_dchi);
-            typedef typename Real<CHX_FP64>::T2 d2t;
-            double *u64 = (double *)(smem + so.u);
-            d2t *x64 = (d2t *)(smem + so.u + al16<double>((size_t)(L.nchan + (L.nchan & 1)) *
-                                                          L.ncoef));
-            for (int pass = 0; pass < 2; ++pass) {
-                for (int q = tid; q < NSP * nk; q += blockDim.x) {
-                    double v = (s_chi[q] + (pass ? s_dchi[q] : 0.0)) / fmax(CNT[q / nk], 1.0);
-                    if (L.chi_extra) v += L.chi_extra[q];
-                    s_tr[q] = v;
-                }
-                __syncthreads();
-                ft_chi2<NSP, CHX_FP64>(L, s_tr, u64, x64, s_num, s_den, s_sq, s_scale,
-                                       pass ? &s_c2t : &s_c2c, nullptr, nullptr, 1);
-            }
+            // the R-factor comparison in FP64: the move's change again with
+            // FP64 terms (the direct records' FP64 term, the FP64 (shell, type)
+            // and MS rows) replacing the FP32 one, its FP64 window transform
+            // (in the span of the resampled rows / transform / direct
+            // records), and the trial chi^2 from the slot's FP64 chi(R) plus
+            // that, against the current chi^2 the same sums gave
+            tie_recheck<NSP>(L, so, smem, s_dir, s_list, 2 * maxaff, ndn, s_msb, s_ndir, s_ndn,
+                             s_dchi, s_tr, CNT, XR, XS, s_num, s_den, s_sq, s_scale, &s_c2t);
             if (tid == 0) {
                 const int rung = s_rung;
-                const double x = L.beta_rung[rung] * (s_c2t - s_c2c) * L.nfit + s_xo;
+                const double x = L.beta_rung[rung] * (s_c2t - L.chi2[c]) * L.nfit + s_xo;
                 const double u = s_uu;
                 const int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
                 if (L.tie_stat) {
@@ -1526,7 +1555,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 }
                 s_acc = acc;
                 s_xd = x;
-                s_c2 = s_c2t;        // an accepted state keeps its FP64 chi^2
+                s_c2 = s_c2t;
             }
             __syncthreads();
         }
@@ -1554,11 +1583,11 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             if (use_xr) {
                 const int nx = L.nchan * L.nwin;
                 if (tid < NSP) XS[tid] = s_scale[tid];
-                if (s_tie) {        // the FP64 trial chi(R) of the near-tie test
+                if (s_tie) {        // the FP64 transform of the near-tie test's change
                     const double *x64 =
                         (const double *)(smem + so.u +
                                          al16<double>((size_t)(L.nchan + (L.nchan & 1)) * L.ncoef));
-                    for (int q = tid; q < 2 * nx; q += blockDim.x) XR[q] = x64[q];
+                    for (int q = tid; q < 2 * nx; q += blockDim.x) XR[q] += x64[q];
                 } else {
                     for (int q = tid; q < nx; q += blockDim.x) {
                         const real2 d = s_x[q];

@@ -96,27 +96,25 @@ def transform_fragments(f, win):
     return out, mt, kt
 
 
-def _window_gain(f, win, sm, nsp, nk):
-    """sqrt of the largest eigenvalue, over the edges, of B^H W B: B the map
-    from an edge's normalised chi(k) (nk) to its channels' chi(R) on the fit
-    bins (resample, window x k^w, transform: the set-up f of _ft_setup), W
-    the weights 1 / sigma^2 (sm, (nchan, nwin)). ||B x||_W <= gain ||x||."""
-    nchan, nkw = f["nchan"], f["nkw"]
+def _window_gain_diag(f, win, sm, nsp, nk):
+    """(nsp, nk): per edge e the diagonal of G_e = B_e W B_e^H, B_e the map
+    from the edge's normalised chi(k) (nk) to its channels' chi(R) on the fit
+    bins (resample, window x k^w, transform: the set-up f of _ft_setup) and W
+    the weights 1 / sigma^2 (sm, (nchan, nwin)); G_kk is the weighted chi(R)
+    norm^2 that a unit change at k alone produces."""
+    nkw = f["nkw"]
     n = f["n0"][0] + np.arange(f["ncoef"])
     win = np.asarray(win, np.int64)
     z = np.exp(-2j * np.pi * ((np.outer(n, win) % f["nfft"]) / f["nfft"])) * f["norm"]
-    best = 0.0
+    out = np.zeros((nsp, nk))
     for e in range(nsp):
-        G = np.zeros((nk, nk), complex)
         for c in range(e * nkw, (e + 1) * nkw):
             B = np.zeros((nk, win.size), complex)
             wt = f["w"][c][:, None] * z
             np.add.at(B, f["idx"][c], (1.0 - f["frac"][c])[:, None] * wt)
             np.add.at(B, np.minimum(f["idx"][c] + 1, nk - 1), f["frac"][c][:, None] * wt)
-            Bw = B * (1.0 / np.asarray(sm[c], float))[None, :]
-            G += Bw @ Bw.conj().T
-        best = max(best, float(np.linalg.eigvalsh(G).max()))
-    return float(np.sqrt(max(best, 0.0)))
+            out[e] += (np.abs(B) ** 2 / np.asarray(sm[c], float)[None, :] ** 2).sum(1)
+    return np.ascontiguousarray(out)
 
 
 def torch_cat_host(ts):
@@ -196,10 +194,11 @@ class Ladders:
     """Device state and descriptors of a batch of ladders (see module doc)."""
 
     # FP32C: keep each slot's FP64 chi(R) and transform only a move's change
-    # (xr of chx_ladder_t); tie_eps: relative bound of the FP32 transform's
-    # rounding used by the near-tie FP64 re-check (0: off)
+    # (xr of chx_ladder_t), with the near-tie FP64 re-check
     delta_transform = True
-    tie_eps = 3e-5
+    # the near-tie test's relative RMS rounding of the change's transform
+    # (split BF16, three products: ~3e-6 per element); 0 turns the test off
+    tie_eps = 5e-6
     # FP32C with the kept chi(R): the change's window transform as split-BF16
     # tensor-core products (ft_frag of chx_ladder_t) instead of the FP32 DFT
     tc_transform = True
@@ -420,21 +419,13 @@ class Ladders:
             self.keep += [b["xr"], b["tie_stat"], b["xs"]]
             L.xs = N.dptr(b["xs"])
             L.xr, L.tie_stat, L.tie_eps = N.dptr(b["xr"]), N.dptr(b["tie_stat"]), self.tie_eps
-            # the FP32 terms' share of the near-tie bound: row maxima of the
-            # tables the step rounds to FP32, and the transform's gain
-            if "sstab" in b:
-                b["sstab_max"] = b["sstab"].abs().amax(dim=1).float().contiguous()
-                L.sstab_max = N.dptr(b["sstab_max"])
-                self.keep.append(b["sstab_max"])
+            # the FP32 terms' share of the near-tie bound: the transform's
+            # per-k gain (diagonal of B W B^H per edge)
+            if self.tie_eps > 0:
+                b["tie_gdiag"] = self._t(_window_gain_diag(f, win, sm, nsp, nk))
+                L.tie_gdiag = N.dptr(b["tie_gdiag"])
             else:
-                L.sstab_max = 0
-            if ms is not None:
-                b["ms_T_max"] = ms.T.abs().amax(dim=1).float().contiguous()
-                L.ms_T_max = N.dptr(b["ms_T_max"])
-                self.keep.append(b["ms_T_max"])
-            else:
-                L.ms_T_max = 0
-            L.tie_gain = _window_gain(f, win, sm, nsp, nk)
+                L.tie_gdiag = 0
             # the change's transform on the tensor cores (split BF16)
             if self.tc_transform:
                 key = tuple(win.tolist())
@@ -448,7 +439,7 @@ class Ladders:
                 L.ft_frag, L.ft_mt, L.ft_kt = 0, 0, 0
         else:
             L.xr, L.tie_stat, L.tie_eps = 0, 0, 0.0
-            L.sstab_max, L.ms_T_max, L.tie_gain, L.xs = 0, 0, 0.0, 0
+            L.tie_gdiag, L.xs = 0, 0
             L.ft_frag, L.ft_mt, L.ft_kt = 0, 0, 0
         b["beta_host"] = beta
         b["cplx"] = cplx

@@ -370,21 +370,21 @@ typedef struct {
        transform's rounding scales with the change, not with chi. NULL: the
        step transforms the whole trial chi in FP32. */
     double *xr;
-    /* near ties (with xr): when |x + ln u| of a Metropolis test is within
-       tie_eps times a bound of the FP32 transform's effect on x, the trial
-       and current chi^2 are recomputed with FP64 transforms of their FP64
-       chi(k) and the test is decided on those (tie_eps 0: never);
+    /* near ties (with xr and tie_gdiag): x of a Metropolis test is bounded
+       against the rounding of the move's change (FP32 terms and MS rows,
+       the transform with relative RMS tie_eps per input) at six standard
+       deviations; when x - tau and x + tau decide differently, the change is
+       recomputed with FP64 terms and rows and both chi^2 with FP64
+       transforms, and the test is decided on those;
        tie_stat (nrep, 2): FP64 re-evaluations, decisions they changed. */
     double tie_eps;
     double *tie_stat;
     /* the FP32 terms' share of the near-tie bound (optional, NULL: left out):
-       the largest |value| of each (shell, type) and MS table row (FP64 rows
-       rounded to FP32 in the step), and tie_gain = sqrt of the largest
-       eigenvalue of B^H W B per edge (B the window transform of a normalised
-       chi(k) onto the fit bins, W = 1 / sigma^2), which turns a bound on a
-       k-space error into one on its weighted chi(R) norm */
-    const float *sstab_max, *ms_T_max;
-    double tie_gain;
+       (nsp, nk) the diagonal of G = B W B^H per edge, B the window transform
+       of a normalised chi(k) onto the fit bins (all the edge's channels) and
+       W = 1 / sigma^2: an independent rounding e(k) of the change adds
+       sum_k e(k)^2 G_kk to the expected squared weighted chi(R) norm */
+    const double *tie_gdiag;
     /* with xr: (nrep, nsp) the profiled scale of each slot's current state,
        the anchor of the step's one-pass chi^2 (written with xr) */
     double *xs;
