@@ -44,10 +44,11 @@ constexpr int kMaxSplit = 2;     // threads sharing one bin's taps
 constexpr int kUndo = 32;        // accepted moves kept after a slot's best point
 // The near-tie test's model of the FP32 parts of a move's change: each is an
 // independent relative rounding of RMS at most eps (a direct record's term:
-// FP32 exp, sin of an FP64-reduced phase, amplitude products; an MS row rounded
-// from FP64 to FP32: 2^-24 / sqrt(3)), summed in quadrature, and the bound
-// taken at kTieSigma standard deviations; the (shell, type) rows and every
-// accumulation of the change are FP64 and add nothing
+// FP32 exp, sin of an FP64-reduced phase, amplitude products; an MS row
+// rounded from FP64 to FP32, and each FP32 accumulation step of the MS rows:
+// 2^-24 / sqrt(3)), summed in quadrature, and the bound taken at kTieSigma
+// standard deviations; the (shell, type) rows and the other accumulations of
+// the change are FP64 and add nothing
 constexpr double kEpsRec = 2e-7;
 constexpr double kEpsTab = 3.5e-8;
 constexpr double kTieSigma = 6.0;
@@ -1341,36 +1342,29 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                         }
                     }
                 }
-                double v0 = 0.0, v1 = 0.0;   // sum (count x row)^2 of the MS rows
-                if (use_xr) {
-                    // FP32 MS rows, FP64 accumulation
+                // near-tie model of the MS rows: sum of (count x row)^2 (the
+                // rows' FP64 -> FP32 rounding) and of the running sum^2 (the
+                // FP32 accumulation's rounding)
+                double v0 = 0.0, v1 = 0.0;
+                if (tie_terms) {
                     const int q0 = s_msb[sa_], q1 = s_msb[sa_ + 1];
-                    double m0 = 0.0, m1 = 0.0;
-                    if (tie_terms) {
-#pragma unroll 16
-                        for (int q = q0; q < q1; ++q) {
-                            const int2 ec = l_ms[q];
-                            const float2 t =
-                                __ldg((const float2 *)&msT32[(long)ec.x * nk2 + k0]);
-                            const double p0 = (double)ec.y * (double)t.x;
-                            const double p1 = (double)ec.y * (double)t.y;
-                            m0 += p0;
-                            m1 += p1;
-                            v0 = fma(p0, p0, v0);
-                            v1 = fma(p1, p1, v1);
-                        }
-                    } else {
-#pragma unroll 16
-                        for (int q = q0; q < q1; ++q) {
-                            const int2 ec = l_ms[q];
-                            const float2 t =
-                                __ldg((const float2 *)&msT32[(long)ec.x * nk2 + k0]);
-                            m0 = fma((double)ec.y, (double)t.x, m0);
-                            m1 = fma((double)ec.y, (double)t.y, m1);
-                        }
+                    const float2 z2 = make_float2(0.f, 0.f), o2 = make_float2(1.f, 1.f);
+                    float2 sm = z2, vq = z2;
+#pragma unroll 8
+                    for (int q = q0; q < q1; ++q) {
+                        const int2 ec = l_ms[q];
+                        const float w = (float)ec.y;
+                        const float2 p = ffma2(make_float2(w, w),
+                                               __ldg((const float2 *)&msT32[(long)ec.x * nk2 + k0]),
+                                               z2);
+                        sm = ffma2(p, o2, sm);
+                        vq = ffma2(p, p, vq);
+                        vq = ffma2(sm, sm, vq);
                     }
-                    acc0 += m0;
-                    acc1 += m1;
+                    acc0 += (double)sm.x;
+                    acc1 += (double)sm.y;
+                    v0 = (double)vq.x;
+                    v1 = (double)vq.y;
                 } else {
                     const int q0 = s_msb[sa_], q1 = s_msb[sa_ + 1];
                     float2 sm = make_float2(0.f, 0.f);

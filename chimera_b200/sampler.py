@@ -434,6 +434,7 @@ class Ladders:
                     frag, mt, kt = transform_fragments(f, win)
                     fc[key] = (self._t(frag.reshape(-1).view(np.int32)), mt, kt)
                 b["ft_frag"], L.ft_mt, L.ft_kt = fc[key]
+                b["ft_tiles"] = (L.ft_mt, L.ft_kt)
                 L.ft_frag = N.dptr(b["ft_frag"])
             else:
                 L.ft_frag, L.ft_mt, L.ft_kt = 0, 0, 0
@@ -456,6 +457,26 @@ class Ladders:
         else:
             self.d_ladders.copy_(src)
         return self.d_ladders
+
+    def has_tc_transform(self):
+        """Whether the ladders carry the tensor-core operands of the change's
+        window transform (FP32C with the kept chi(R))."""
+        return any("ft_frag" in b for b in self.bufs)
+
+    def set_transform(self, tensor_cores):
+        """Transform a move's change with the split-BF16 tensor-core products
+        (True) or the FP32 rotation DFT (False); FP32C with the kept chi(R).
+        Takes effect for launches made (or graphs captured) after the call."""
+        for li, b in enumerate(self.bufs):
+            if "ft_frag" not in b:
+                continue
+            L = self.host[li]
+            if tensor_cores:
+                L.ft_frag = N.dptr(b["ft_frag"])
+                L.ft_mt, L.ft_kt = b["ft_tiles"]
+            else:
+                L.ft_frag, L.ft_mt, L.ft_kt = 0, 0, 0
+        self._upload()
 
     def set_field(self, li, name, value):
         setattr(self.host[li], name, value)
