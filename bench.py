@@ -331,6 +331,49 @@ def bench_ft(args):
             "rms_err_re": float(dz[..., 0].pow(2).mean().sqrt()) / scale,
             "rms_err_im": float(dz[..., 1].pow(2).mean().sqrt()) / scale,
             "rfactor_max": float(rf.max()), "rfactor_mean": float(rf.mean())}
+    # the fused form (chx_ft_window_sums): the same contraction, its epilogue
+    # summing each spectrum against a target over the fit window (1.4-5.0 A)
+    # instead of writing chi(R); the three weights are the channels of one
+    # edge, so the sums over all 600 bins are the edge's sums; anchored at
+    # s0 = 1 (the targets are near scale 1)
+    from chimera_b200.fourier import WindowSums, FourierTransform as _FT
+    z64 = ref.transpose(0, 1).reshape(nspec, nR, 2)
+    zc = torch.complex(z64[..., 0], z64[..., 1])                      # FP64 chi(R)
+    Rg = _FT(k, 3.0, 13.0, 1).R[bins]
+    win = np.tile((Rg >= 1.4) & (Rg <= 5.0), 3)
+    tgt = zc[0].cpu().numpy() * 1.05 + rng.normal(0, 1e-3, nR) * (1 + 1j)
+    wgt = np.where(win, 1.0 / 2e-3 ** 2, 0.0)
+    tg = torch.from_numpy(tgt).cuda()
+    wg = torch.from_numpy(wgt).cuda()
+    wn = torch.from_numpy(win).cuda()
+    T0 = float((tg.abs() ** 2 * wn).sum())
+    sc64 = (zc * tg.conj()).real.mul(wn).sum(1) / (zc.abs() ** 2 * wn).sum(1)
+    c64 = ((sc64[:, None] * zc - tg).abs() ** 2 * wg).sum(1)
+    r64 = ((sc64[:, None] * zc - tg).abs() ** 2 * wn).sum(1) / T0
+    for prec in (2, 3):
+        ws = WindowSums(Bc, tgt, wgt, nspec, prec, s0=1.0, Bd=basis)
+        for _ in range(max(3, args.warmup)):
+            ws(x)
+        ts = []
+        for _ in range(max(5, min(args.steps, 30))):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            o5 = ws(x)
+            b.record(s)
+            b.synchronize()
+            ts.append(a.elapsed_time(b) * 1e-3)
+        assert ws.device_error() == 0, "device error word set"
+        sc, c, rn = WindowSums.chi2(o5, 1.0)
+        r = rn / T0              # the R-factor from the same sums (model.py:535-540)
+        t = float(np.median(ts))
+        byts = (nspec * nk + nk * 2 * nR + nspec * 7) * 8
+        res[f"fused_{prec}"] = {
+            "us": t * 1e6, "GB_per_s": byts / t / 1e9,
+            "useful_TFLOP_per_s": 2.0 * nspec * nk * 2 * nR / t / 1e12,
+            "chi2_rel_err_max": float(((c - c64).abs() / c64.abs()).max()),
+            "rfactor_rel_err_max": float(((r - r64).abs() / r64.abs()).max()),
+            "bytes_out_per_spectrum": 56}
     hbm, src = peaks()
     tc = res["2"]
     line = {"metric": "windowed FT contraction chi(k) -> chi(R)", "kernel": "chx_ft_batch",
@@ -338,7 +381,9 @@ def bench_ft(args):
                                    "Kaiser dk 1, k 3-13",
                        "spectra": nspec, "nk": nk, "nR": nR, "l2": "flushed before each call"},
             "precisions": {"0": "FP64 SIMT", "1": "FP32 SIMT", "2": "split-BF16 tcgen05",
-                           "3": "TF32 tcgen05"},
+                           "3": "TF32 tcgen05",
+                           "fused_2": "split-BF16 tcgen05, window-sums epilogue "
+                                      "(chx_ft_window_sums)", "fused_3": "TF32, fused"},
             "results": res,
             "roofline": {"bound": "hbm", "achieved": tc["GB_per_s"], "peak": hbm,
                          "unit": "GB/s", "frac": tc["GB_per_s"] / hbm, "peak_source": src,

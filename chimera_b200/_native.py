@@ -124,6 +124,9 @@ _SIGS = {
     "chx_sampler_smem_bytes": ([c_p, c_i, c_i], c_i),
     "chx_shell_table": ([c_p, c_p, c_p, c_p, c_p], c_i),
     "chx_sampler_step": ([c_p, c_p, c_i, c_p, c_i, c_i, c_i, c_i, c_i, c_p, c_p, c_p, c_p], c_i),
+    "chx_ft_window_sums_scratch_bytes": ([c_i, c_i, c_i, c_i], C.c_int64),
+    "chx_ft_window_sums": ([c_p, c_i, c_i, c_p, c_i, c_p, c_p, c_d, c_i, c_p, c_p, C.c_int64,
+                            c_p], c_i),
     "chx_pair_counts": ([c_p, c_i, c_i, c_p, c_p, c_i, c_i, c_p, c_p, c_p], c_i),
     "chx_refresh_chi2": ([c_p, c_p, c_i, c_p, c_i, c_i, c_p, c_p], c_i),
     "chx_reanchor_scratch_bytes": ([c_p, c_i, c_i], C.c_int64),

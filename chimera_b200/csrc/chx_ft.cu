@@ -18,6 +18,10 @@ namespace chx {
 int ft_batch_tc(const double *chi, int rows, int nk, const double *basis, int nR, double *out,
                 void *scratch, int64_t scratch_bytes, cudaStream_t st, bool tf32);
 int64_t ft_batch_tc_scratch(int rows, int nk, int nR, bool tf32);
+int ft_sums_tc(const double *chi, int rows, int nk, const double *basis, int nR,
+               const double *target, const double *weight, double s0, double *out4,
+               void *scratch, int64_t scratch_bytes, cudaStream_t st, bool tf32);
+int64_t ft_sums_tc_scratch(int rows, int nk, int nR, bool tf32);
 
 // 64 x 64 output tile per CTA, 256 threads, 4 x 4 outputs per thread
 template <typename T>
@@ -97,6 +101,22 @@ int chx_ft_batch(const double *chi, int rows, int nk, const double *basis, int n
     }
     CHX_CHECK_LAUNCH("ft_batch");
     return CHX_OK;
+}
+
+int64_t chx_ft_window_sums_scratch_bytes(int rows, int nk, int nR, int precision) {
+    if (rows <= 0 || nk <= 0 || nR <= 0 || (precision != 2 && precision != 3)) return -1;
+    return ft_sums_tc_scratch(rows, nk, nR, precision == 3);
+}
+
+int chx_ft_window_sums(const double *chi, int rows, int nk, const double *basis, int nR,
+                       const double *target, const double *weight, double s0, int precision,
+                       double *sums, void *scratch, int64_t scratch_bytes, void *stream) {
+    CHX_REQUIRE(chi && basis && target && weight && sums && rows > 0 && nk > 0 && nR > 0,
+                "ft_window_sums: bad arguments");
+    CHX_REQUIRE(precision == 2 || precision == 3,
+                "ft_window_sums: precision %d (the fused form is 2 or 3)", precision);
+    return ft_sums_tc(chi, rows, nk, basis, nR, target, weight, s0, sums, scratch,
+                      scratch_bytes, as_stream(stream), precision == 3);
 }
 
 }  // extern "C"

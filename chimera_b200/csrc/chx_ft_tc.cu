@@ -30,6 +30,7 @@
 // word in the first 4 bytes of scratch (CHX_DEVERR_INDEX), waits (bounded)
 // for the copies and MMAs it started, frees its tensor memory and returns.
 #include <cuda.h>
+#include <cstring>
 #include <cuda_bf16.h>
 #include "chx_common.cuh"
 
@@ -273,7 +274,35 @@ __device__ __forceinline__ bool tc_tile(int i, int ntn, int mtiles, int &mt, int
     return t < ntn * mtiles;
 }
 
-template <bool TF32, bool RES>
+// The window sums of the fused form (SUMS): instead of chi(R), each row's
+// sums against the target t and weights w over the tile's bins (w is 0
+// outside the fit window, so they run over it), anchored at a scale s0:
+// Re<m,t>, <m,m>, R = sum w |s0 m - t|^2, Q = sum w Re(m (s0 m - t)*),
+// P = sum w |m|^2, and the unweighted Ru = sum |s0 m - t|^2 and
+// Qu = sum Re(m (s0 m - t)*), into part[(row * ntn + nt) * kSums]; then
+// sum w |s m - t|^2 = R + 2 (s - s0) Q + (s - s0)^2 P for any scale s (and
+// the R-factor's numerator Ru + 2 (s - s0) Qu + (s - s0)^2 <m,m>), the
+// residual at s0 carrying its size without cancelling.
+constexpr int kSums = 7;
+struct TcSums {
+    const double *tgt;   // (nR, 2) target chi(R), re/im
+    const double *wgt;   // (nR) 1 / sigma^2 on the fit window, 0 elsewhere
+    double *part;        // (rows, ntn, kSums)
+    int nR;
+    double s0;
+    const float2 *tgt32; // FP32 copies of tgt and wgt (in the scratch)
+    const float *wgt32;
+};
+
+__global__ void k_tc_sums_prep(const double *__restrict__ tgt, const double *__restrict__ wgt,
+                               int nR, float2 *__restrict__ t32, float *__restrict__ w32) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nR) return;
+    t32[b] = make_float2((float)tgt[2 * b], (float)tgt[2 * b + 1]);
+    w32[b] = (float)wgt[b];
+}
+
+template <bool TF32, bool RES, bool SUMS>
 __global__ void __launch_bounds__(kTcThreads, 1) k_ft_tc(const uint8_t *__restrict__ Ahi,
                                                          const uint8_t *__restrict__ Alo,
                                                          int rows,
@@ -281,7 +310,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_ft_tc(const uint8_t *__restri
                                                          const uint8_t *__restrict__ Blo,
                                                          int nkt, int ncol, int ntn, int mtiles,
                                                          const __grid_constant__ CUtensorMap tm_out,
-                                                         int *__restrict__ err) {
+                                                         TcSums sums, int *__restrict__ err) {
     extern __shared__ uint8_t tc_raw[];
     __shared__ __align__(8) uint64_t full[kTcStages], freed[kTcStages], acc_full[kTcAcc],
         acc_empty[kTcAcc], done;
@@ -457,6 +486,46 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_ft_tc(const uint8_t *__restri
                                  tc_smem(&acc_empty[b]))
                              : "memory");
             const int y = mt * kTcM + warp * 32;
+            if constexpr (SUMS) {
+                // this lane's row: 64 complex bins of the tile against the
+                // channel's target, FP64 sums
+                // FP32 products and sums over the tile's 64 bins (the
+                // accumulator itself is FP32), FP64 across tiles
+                float nu = 0.f, dn = 0.f, R = 0.f, Q = 0.f, P = 0.f, Ru = 0.f, Qu = 0.f;
+                const float s0 = (float)sums.s0;
+                const int b0 = (nt * kTcN) >> 1;
+#pragma unroll
+                for (int j = 0; j < 64; ++j) {
+                    const int bin = b0 + j;
+                    const float w = bin < sums.nR ? sums.wgt32[bin] : 0.f;
+                    if (w != 0.f) {
+                        const float mr = __uint_as_float(v[j >> 4][(j & 15) * 2]);
+                        const float mi = __uint_as_float(v[j >> 4][(j & 15) * 2 + 1]);
+                        const float2 t = sums.tgt32[bin];
+                        const float rr = fmaf(s0, mr, -t.x), ri = fmaf(s0, mi, -t.y);
+                        const float mm = fmaf(mr, mr, mi * mi);
+                        const float r2 = fmaf(rr, rr, ri * ri), q2 = fmaf(mr, rr, mi * ri);
+                        nu = fmaf(mr, t.x, fmaf(mi, t.y, nu));
+                        dn += mm;
+                        R = fmaf(w, r2, R);
+                        Q = fmaf(w, q2, Q);
+                        P = fmaf(w, mm, P);
+                        Ru += r2;
+                        Qu += q2;
+                    }
+                }
+                const int row = y + lane;
+                if (row < rows) {
+                    double *o = sums.part + ((long)row * ntn + nt) * kSums;
+                    o[0] = nu;
+                    o[1] = dn;
+                    o[2] = R;
+                    o[3] = Q;
+                    o[4] = P;
+                    o[5] = Ru;
+                    o[6] = Qu;
+                }
+            } else {
 #pragma unroll
             for (int g = 0; g < kTcN / 16; ++g) {
                 const int x = nt * kTcN + g * 16;             // even: 16-byte aligned
@@ -485,6 +554,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_ft_tc(const uint8_t *__restri
                     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                 }
             }
+            }   // chi(R) boxes
         }
         // the stores are complete before the CTA leaves
         if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
@@ -542,12 +612,12 @@ static TcEncodeFn tc_encode_fn() {
 // the contraction as a programmatic dependent of the split: its prologue
 // (barriers, tensor memory) overlaps the split's tail, its loads wait for the
 // split's end
-template <bool TF32, bool RES>
+template <bool TF32, bool RES, bool SUMS>
 static cudaError_t tc_launch(int grid, size_t smem, cudaStream_t st, const uint8_t *ahi,
                              const uint8_t *al, int rows, const uint8_t *bhi, const uint8_t *bl,
                              int nkt, int ncol, int ntn, int mtiles, const CUtensorMap &tm,
-                             int *err) {
-    cudaError_t e = cudaFuncSetAttribute(k_ft_tc<TF32, RES>,
+                             const TcSums &sums, int *err) {
+    cudaError_t e = cudaFuncSetAttribute(k_ft_tc<TF32, RES, SUMS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
@@ -560,33 +630,62 @@ static cudaError_t tc_launch(int grid, size_t smem, cudaStream_t st, const uint8
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_ft_tc<TF32, RES>, ahi, al, rows, bhi, bl, nkt, ncol, ntn,
-                              mtiles, tm, err);
+    return cudaLaunchKernelEx(&cfg, k_ft_tc<TF32, RES, SUMS>, ahi, al, rows, bhi, bl, nkt, ncol,
+                              ntn, mtiles, tm, sums, err);
 }
 
+// rows x ntn partial window sums after the operand scratch (the fused form)
+static size_t tc_sums_bytes(int rows, int nR) {
+    const int ntn = (2 * nR + kTcN - 1) / kTcN;
+    return ((size_t)rows * ntn * kSums * sizeof(double) + 255) / 256 * 256 +
+           ((size_t)nR * 12 + 255) / 256 * 256;
+}
+
+// row r of out = the sum over column tiles (in order) of its partials
+__global__ void k_tc_sums_reduce(const double *__restrict__ part, int rows, int ntn,
+                                 double *__restrict__ out) {
+    const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    double a[kSums] = {};
+    for (int t = 0; t < ntn; ++t)
+#pragma unroll
+        for (int q = 0; q < kSums; ++q) a[q] += part[(r * ntn + t) * kSums + q];
+#pragma unroll
+    for (int q = 0; q < kSums; ++q) out[r * kSums + q] = a[q];
+}
+
+// out: chi(R) (sums NULL), or with sums the (rows, 4) window sums
 template <bool TF32>
 static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *basis, int nR,
-                            double *out, void *scratch, int64_t scratch_bytes, cudaStream_t st) {
+                            double *out, void *scratch, int64_t scratch_bytes, cudaStream_t st,
+                            const TcSums *sums = nullptr) {
     typedef TcMode<TF32> Md;
     const TcPlan p = tc_plan(rows, nk, nR, TF32);
-    CHX_REQUIRE(scratch && scratch_bytes >= (int64_t)p.total,
-                "ft_batch: the tensor-core path needs %zu bytes of scratch", p.total);
+    const size_t need = p.total + (sums ? tc_sums_bytes(rows, nR) : 0);
+    CHX_REQUIRE(scratch && scratch_bytes >= (int64_t)need,
+                "ft_batch: the tensor-core path needs %zu bytes of scratch", need);
     CHX_REQUIRE(((uintptr_t)scratch & 255) == 0, "ft_batch: scratch must be 256-byte aligned");
     CHX_REQUIRE(((uintptr_t)out & 15) == 0,
                 "ft_batch: precisions 2 and 3 need out 16-byte aligned");
     const int ncol = 2 * nR;
     // chi(R) (rows x ncol FP64, rows ncol * 8 bytes apart) as the TMA store
-    // target, in boxes of 32 rows x 16 columns, 128-byte swizzle
-    const TcEncodeFn enc = tc_encode_fn();
-    CHX_REQUIRE(enc != nullptr, "ft_batch: cuTensorMapEncodeTiled is not available");
+    // target, in boxes of 32 rows x 16 columns, 128-byte swizzle (not used by
+    // the fused form, which writes sums)
     CUtensorMap tm;
-    const cuuint64_t gdim[2] = {(cuuint64_t)ncol, (cuuint64_t)rows};
-    const cuuint64_t gstride[1] = {(cuuint64_t)ncol * sizeof(double)};
-    const cuuint32_t box[2] = {16, 32}, estr[2] = {1, 1};
-    const CUresult cr = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)out, gdim, gstride,
-                            box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                            CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    CHX_REQUIRE(cr == CUDA_SUCCESS, "ft_batch: chi(R) tensor map refused (CUresult %d)", (int)cr);
+    memset(&tm, 0, sizeof(tm));
+    if (!sums) {
+        const TcEncodeFn enc = tc_encode_fn();
+        CHX_REQUIRE(enc != nullptr, "ft_batch: cuTensorMapEncodeTiled is not available");
+        const cuuint64_t gdim[2] = {(cuuint64_t)ncol, (cuuint64_t)rows};
+        const cuuint64_t gstride[1] = {(cuuint64_t)ncol * sizeof(double)};
+        const cuuint32_t box[2] = {16, 32}, estr[2] = {1, 1};
+        const CUresult cr = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void *)out, gdim,
+                                gstride, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        CHX_REQUIRE(cr == CUDA_SUCCESS, "ft_batch: chi(R) tensor map refused (CUresult %d)",
+                    (int)cr);
+    }
     int dev = 0, nsm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -613,13 +712,50 @@ static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *b
     const int grid = std::min(ntn * mtiles, nsm);
     const bool res = p.Kp <= kTcResKp && ntn <= grid;
     const size_t smem = Md::smem(res, nkt);
-    e = res ? tc_launch<TF32, true>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol, ntn,
-                                    mtiles, tm, err)
-            : tc_launch<TF32, false>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol, ntn,
-                                     mtiles, tm, err);
+    if (sums) {
+        TcSums sm = *sums;
+        sm.part = (double *)(base + p.total);
+        const int ntn_ = (2 * nR + kTcN - 1) / kTcN;
+        uint8_t *f32 = base + p.total +
+                       ((size_t)rows * ntn_ * kSums * sizeof(double) + 255) / 256 * 256;
+        sm.tgt32 = (const float2 *)f32;
+        sm.wgt32 = (const float *)(f32 + (size_t)nR * 8);
+        k_tc_sums_prep<<<(nR + 255) / 256, 256, 0, st>>>(sums->tgt, sums->wgt, nR,
+                                                          (float2 *)f32,
+                                                          (float *)(f32 + (size_t)nR * 8));
+        CHX_CHECK_LAUNCH("ft_sums prep");
+        e = res ? tc_launch<TF32, true, true>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol,
+                                              ntn, mtiles, tm, sm, err)
+                : tc_launch<TF32, false, true>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol,
+                                               ntn, mtiles, tm, sm, err);
+        if (e != cudaSuccess) return cuda_fail(e, "ft_sums tc launch");
+        CHX_CHECK_LAUNCH("ft_sums tc");
+        k_tc_sums_reduce<<<(rows + 255) / 256, 256, 0, st>>>(sm.part, rows, ntn, out);
+        CHX_CHECK_LAUNCH("ft_sums reduce");
+        return CHX_OK;
+    }
+    const TcSums none = {nullptr, nullptr, nullptr, 0, 1.0, nullptr, nullptr};
+    e = res ? tc_launch<TF32, true, false>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol, ntn,
+                                           mtiles, tm, none, err)
+            : tc_launch<TF32, false, false>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol,
+                                            ntn, mtiles, tm, none, err);
     if (e != cudaSuccess) return cuda_fail(e, "ft_batch tc launch");
     CHX_CHECK_LAUNCH("ft_batch tc");
     return CHX_OK;
+}
+
+int64_t ft_sums_tc_scratch(int rows, int nk, int nR, bool tf32) {
+    return (int64_t)(tc_plan(rows, nk, nR, tf32).total + tc_sums_bytes(rows, nR));
+}
+
+int ft_sums_tc(const double *chi, int rows, int nk, const double *basis, int nR,
+               const double *target, const double *weight, double s0, double *out4,
+               void *scratch, int64_t scratch_bytes, cudaStream_t st, bool tf32) {
+    const TcSums sums = {target, weight, nullptr, nR, s0, nullptr, nullptr};
+    return tf32 ? ft_batch_tc_mode<true>(chi, rows, nk, basis, nR, out4, scratch, scratch_bytes,
+                                         st, &sums)
+                : ft_batch_tc_mode<false>(chi, rows, nk, basis, nR, out4, scratch, scratch_bytes,
+                                          st, &sums);
 }
 
 int ft_batch_tc(const double *chi, int rows, int nk, const double *basis, int nR, double *out,

@@ -255,3 +255,67 @@ class EdgeTransforms:
         kmin = min(f.kmin for f in self.fts)
         kmax = max(f.kmax for f in self.fts)
         return 2 * (kmax - kmin) * (rmax - rmin) / np.pi + 2
+
+
+class WindowSums:
+    """The fused form of the transform (chx_ft_window_sums) for a fixed basis
+    B (nk, nbins), target (nbins, complex) and weights (nbins; 1 / sigma^2 on
+    the fit window, 0 elsewhere): for each row of chi (rows, nk), with m its
+    chi(R), the sums (rows, 7) = (Re<m,t>, <m,m>, sum w |s0 m - t|^2,
+    sum w Re(m (s0 m - t)*), sum w |m|^2, sum |s0 m - t|^2,
+    sum Re(m (s0 m - t)*)) over the window, chi(R) itself never written; precision 2 (split BF16) or 3 (TF32) on the tensor cores. The
+    device copies of basis, target and weights and the scratch are made once,
+    so `__call__` is one launch pair on the current stream."""
+
+    def __init__(self, B, target, weight, rows, precision=2, s0=1.0, Bd=None):
+        import torch
+        N.require_cuda()
+        self.nk, self.nb = B.shape
+        self.rows, self.precision, self.s0 = int(rows), int(precision), float(s0)
+        self.Bd = basis_to_device(B) if Bd is None else Bd
+        t = np.asarray(target)
+        self.td = torch.from_numpy(np.ascontiguousarray(
+            np.stack([t.real, t.imag], -1).reshape(-1), np.float64)).to("cuda")
+        self.wd = torch.from_numpy(np.ascontiguousarray(weight, np.float64)).to("cuda")
+        self.nsc = int(N.lib().chx_ft_window_sums_scratch_bytes(self.rows, self.nk, self.nb,
+                                                                self.precision))
+        self.scr = torch.empty(max(self.nsc, 1), dtype=torch.uint8, device="cuda")
+        self.out = torch.empty((self.rows, 7), dtype=torch.float64, device="cuda")
+
+    def __call__(self, x):
+        """x: (rows, nk) FP64 CUDA tensor -> (rows, 7) CUDA tensor (reused)."""
+        N.call("chx_ft_window_sums", N.ptr(x), self.rows, self.nk, N.ptr(self.Bd), self.nb,
+               N.ptr(self.td), N.ptr(self.wd), self.s0, self.precision, N.ptr(self.out),
+               N.ptr(self.scr), self.nsc, N.stream())
+        return self.out
+
+    def device_error(self):
+        """The scratch's error word (non-zero: a bounded wait ran out)."""
+        import torch
+        return int(self.scr[:4].view(torch.int32).item())
+
+    @staticmethod
+    def chi2(sums, s0=1.0, profile=True):
+        """Per row: the profiled scale s (Re<m,t> / <m,m>, or 1),
+        sum w |s m - t|^2 and sum |s m - t|^2 (the R-factor's numerator) from
+        the anchored sums."""
+        nu, dn, R, Q, P, Ru, Qu = (sums[..., q] for q in range(7))
+        s = nu / dn if profile else 1.0 + 0.0 * nu
+        ds = s - s0
+        return s, R + 2.0 * ds * Q + ds * ds * P, Ru + 2.0 * ds * Qu + ds * ds * dn
+
+
+def window_sums(chi, B, target, weight, precision=2, s0=1.0, Bd=None):
+    """One-off chx_ft_window_sums (WindowSums) on chi (..., nk), host or
+    device; returns (..., 7) of the same kind."""
+    import torch
+    host = not (isinstance(chi, torch.Tensor) and chi.is_cuda)
+    x = torch.as_tensor(np.asarray(chi) if host else chi).to("cuda", torch.float64).contiguous()
+    lead = tuple(x.shape[:-1])
+    rows = int(np.prod(lead)) if lead else 1
+    ws = WindowSums(B, target, weight, rows, precision, s0, Bd=Bd)
+    out = ws(x.reshape(rows, -1)).clone()
+    if ws.device_error():
+        raise N.ChxError("chx_ft_window_sums: the tensor-core contraction gave up a bounded wait")
+    out = out.reshape(lead + (7,))
+    return out.cpu().numpy() if host else out

@@ -494,6 +494,27 @@ CHX_API int chx_apply_exchange(const chx_ladder_t *d_ladders, int ladder, const 
 CHX_API int chx_ft_batch(const double *chi, int rows, int nk, const double *basis, int nR,
                  int precision, double *out, void *scratch, int64_t scratch_bytes,
                  void *stream);
+
+/* The fused form of the windowed FT for a profiled chi^2 (config 2's form):
+ * the same tensor-core contraction (precision 2 split-BF16, 3 TF32) of chi
+ * (rows, nk) with basis (nk, 2 nR) as chx_ft_batch, but instead of chi(R) its
+ * epilogue writes each row's sums against a target and weights over the bins
+ * with w != 0 (the fit window), anchored at a scale s0: sums (rows, 7) =
+ * {Re<m,t>, <m,m>, R = sum w |s0 m - t|^2, Q = sum w Re(m (s0 m - t)*),
+ * P = sum w |m|^2, Ru = sum |s0 m - t|^2, Qu = sum Re(m (s0 m - t)*)},
+ * 56 bytes per row in place of 16 nR. The profiled scale
+ * s = sum Re<m,t> / sum <m,m> (over an edge's channels),
+ * sum w |s m - t|^2 = R + 2 (s - s0) Q + (s - s0)^2 P and the R-factor
+ * numerator Ru + 2 (s - s0) Qu + (s - s0)^2 <m,m> follow on the host
+ * (method_a_rmc.py:190-227, model.py:497-540); with s0 near s nothing
+ * cancels. Products and the sums within one 128-column tile are FP32 (the
+ * accumulator's precision), the sums across tiles FP64. target (nR, 2) re/im, weight (nR) = 1 / sigma^2 in the window, 0
+ * outside. Scratch: chx_ft_window_sums_scratch_bytes (256-byte aligned). */
+CHX_API int64_t chx_ft_window_sums_scratch_bytes(int rows, int nk, int nR, int precision);
+CHX_API int chx_ft_window_sums(const double *chi, int rows, int nk, const double *basis, int nR,
+                               const double *target, const double *weight, double s0,
+                               int precision, double *sums, void *scratch,
+                               int64_t scratch_bytes, void *stream);
 CHX_API int64_t chx_ft_batch_scratch_bytes(int rows, int nk, int nR, int precision);
 
 /* ------------------------------------------------------------------------

@@ -108,3 +108,48 @@ def test_tensor_core_edge_shapes(cuda, precision):
         z = apply_basis(x, B, precision).cpu().numpy()
         assert z.shape == (rows, nb)
         assert np.abs(z - z0).max() <= TOL[precision] * np.abs(z0).max(), (rows, nk, nb)
+
+
+@pytest.mark.parametrize("precision,tol", [(2, 1e-4), (3, 3e-3)])
+def test_fused_window_sums_match_fp64_transform(cuda, precision, tol):
+    """The fused form (chx_ft_window_sums: the tensor-core contraction whose
+    epilogue sums each row against the target instead of writing chi(R))
+    against sums of the FP64 transform, on the series configuration's shape
+    (k^2 Kaiser window, 241 k, 200 R points at 0.03 A) with a fit window
+    inside the R range; rows not a multiple of the 128-row tile. The sums
+    give the profiled scale and chi^2 of the reference (method_a_rmc.py:
+    190-227) at any scale from the anchor s0; each sum's error is stated
+    relative to its own scale, and the chi^2 relative to itself."""
+    from chimera_b200.fourier import FourierTransform, WindowSums, apply_basis, window_sums
+    from chimera_b200.tables import uniform_k
+    k = uniform_k()
+    f = FourierTransform(k, 3.0, 13.0, 2, window="kaiser")
+    Rb = np.arange(46, 246)
+    B = f.basis(Rb)
+    rng = np.random.default_rng(7)
+    rows = 1000
+    chi = rng.normal(0, 0.05, (rows, k.size)) * np.exp(-0.01 * k ** 2) * np.sin(5.0 * k)
+    chi[1::2] = chi[0] * (1.0 + rng.normal(0, 0.01, (rows // 2, 1)))   # near the target
+    m64 = apply_basis(chi, B, 0)
+    t = m64[0] * 1.1 + rng.normal(0, 1e-3, Rb.size) * (1 + 1j)
+    w = np.where((f.R[Rb] >= 1.4) & (f.R[Rb] <= 5.0), 1.0 / 2e-3 ** 2, 0.0)
+    inw = w != 0
+    s0 = 1.1
+    r0 = s0 * m64 - t
+    want = np.stack([(m64 * t.conj()).real[:, inw].sum(1), (np.abs(m64) ** 2)[:, inw].sum(1),
+                     (np.abs(r0) ** 2 * w).sum(1), ((m64 * r0.conj()).real * w).sum(1),
+                     (np.abs(m64) ** 2 * w).sum(1), (np.abs(r0) ** 2)[:, inw].sum(1),
+                     (m64 * r0.conj()).real[:, inw].sum(1)], -1)
+    got = window_sums(chi, B, t, w, precision, s0=s0)
+    assert got.shape == (rows, 7)
+    scale = np.abs(want).max(0)
+    assert (np.abs(got - want) / scale).max() <= tol
+    # the profiled chi^2 from the anchored sums against FP64's own
+    s64 = want[:, 0] / want[:, 1]
+    c64 = (np.abs(s64[:, None] * m64 - t) ** 2 * w).sum(1)
+    r64 = (np.abs(s64[:, None] * m64 - t) ** 2)[:, inw].sum(1)
+    _, c, r = WindowSums.chi2(got, s0)
+    near = slice(1, None, 2)                  # the rows near the target (chi^2 small)
+    assert (np.abs(c - c64) / c64).max() <= 10 * tol
+    assert (np.abs(c[near] - c64[near]) / c64[near]).max() <= 10 * tol
+    assert (np.abs(r - r64) / r64).max() <= 10 * tol
