@@ -11,34 +11,61 @@ struct Proposal {
     double np[3];
 };
 
-// S(i) returns the species of site i (an array or a shared-memory accessor).
-template <typename SpeciesOf>
-__device__ __forceinline__ Proposal propose_one(SpeciesOf S, const double *P, const double *Id,
-                                                int natoms, uint64_t seed, uint64_t stepc, int c,
-                                                double swap_frac, double disp_sigma,
-                                                double max_disp) {
-    Proposal pr;
+// The draws of one proposal that do not depend on the state: the move kind,
+// site a and the eight candidate partners, keyed (seed, step, replica c).
+// They can be drawn ahead of the step that uses them.
+struct ProposalDraws {
+    uint64_t h0;   // hash state after the draw of a (a displacement without swap)
+    uint64_t h8;   // after the eight candidate draws (the failed swap's displacement)
+    int sw, a;
+    int cand[8];
+};
+
+__device__ __forceinline__ void propose_draws(ProposalDraws &d, uint64_t seed, uint64_t stepc,
+                                              int c, int natoms, double swap_frac) {
     uint64_t h = splitmix64(seed ^ (stepc * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)c << 32));
     h = splitmix64(h);
-    int sw = (u01(h) < swap_frac) ? 1 : 0;
+    d.sw = (u01(h) < swap_frac) ? 1 : 0;
     h = splitmix64(h);
     int a = (int)(u01(h) * natoms);
     if (a >= natoms) a = natoms - 1;
+    d.a = a;
+    d.h0 = h;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        h = splitmix64(h);
+        int cand = (int)(u01(h) * natoms);
+        if (cand >= natoms) cand = natoms - 1;
+        d.cand[t] = cand;
+    }
+    d.h8 = h;
+}
+
+// The proposal from its draws and the current species S(i) (an array or a
+// shared-memory accessor): the first candidate of another species than a's
+// is the swap partner; with none (or no swap drawn), a Gaussian displacement
+// of a, Box-Muller on the draws that follow. keep_pos: also report a's
+// position as np for a swap (the reference's proposal record); the fused
+// step leaves it out, it reads np for displacements only.
+template <typename SpeciesOf>
+__device__ __forceinline__ Proposal propose_finish(const ProposalDraws &d, SpeciesOf S,
+                                                   const double *P, const double *Id,
+                                                   double disp_sigma, double max_disp,
+                                                   bool keep_pos = true) {
+    Proposal pr;
+    const int a = d.a;
     int sa = S(a), b = a, sb = sa;
-    if (sw) {
+    if (d.sw) {
         for (int t = 0; t < 8; ++t) {
-            h = splitmix64(h);
-            int cand = (int)(u01(h) * natoms);
-            if (cand >= natoms) cand = natoms - 1;
-            int sc = S(cand);
+            int sc = S(d.cand[t]);
             if (sc != sa) {
-                b = cand;
+                b = d.cand[t];
                 sb = sc;
                 break;
             }
         }
     }
-    int real_swap = (sw && b != a) ? 1 : 0;
+    int real_swap = (d.sw && b != a) ? 1 : 0;
     pr.swap = real_swap;
     pr.a = a;
     pr.b = b;
@@ -47,10 +74,16 @@ __device__ __forceinline__ Proposal propose_one(SpeciesOf S, const double *P, co
     const double *Pa = P + (long)a * 3;
     const double *Ia = Id + (long)a * 3;
     if (real_swap) {
-        pr.np[0] = Pa[0];
-        pr.np[1] = Pa[1];
-        pr.np[2] = Pa[2];
+        if (keep_pos) {
+            pr.np[0] = Pa[0];
+            pr.np[1] = Pa[1];
+            pr.np[2] = Pa[2];
+        } else {
+            pr.np[0] = pr.np[1] = pr.np[2] = 0.0;
+        }
     } else {
+        // a swap drawn but no partner found consumed all eight candidate draws
+        uint64_t h = d.sw ? d.h8 : d.h0;
         // Box-Muller on two pairs of draws, clamped to max_disp from the site
         double g[3];
         for (int t = 0; t < 3; t += 2) {
@@ -73,6 +106,21 @@ __device__ __forceinline__ Proposal propose_one(SpeciesOf S, const double *P, co
         pr.np[2] = Ia[2] + oz * sc;
     }
     return pr;
+}
+
+// Proposal of one replica: draws exactly the reference's splitmix64 sequence
+// (exafs_gpu/kernels.py:376-421) keyed (seed, step, replica index c). The
+// reference draws the candidates one at a time and stops at the first of
+// another species; drawing all eight ahead reads the same stream, since a
+// candidate draw after the partner is found is never used.
+template <typename SpeciesOf>
+__device__ __forceinline__ Proposal propose_one(SpeciesOf S, const double *P, const double *Id,
+                                                int natoms, uint64_t seed, uint64_t stepc, int c,
+                                                double swap_frac, double disp_sigma,
+                                                double max_disp) {
+    ProposalDraws d;
+    propose_draws(d, seed, stepc, c, natoms, swap_frac);
+    return propose_finish(d, S, P, Id, disp_sigma, max_disp);
 }
 
 

@@ -482,42 +482,44 @@ __device__ void chi2_profiled(const chx_ladder_t &L, GetM getm, const R2 *dx, do
 // Re(m r0*) + (s - s0)^2 |m|^2, so per channel R = sum |r0|^2 / sigma^2,
 // Q = sum Re(m r0*) / sigma^2 and P = sum |m|^2 / sigma^2 are summed with
 // num and den in one sweep; R carries the size of chi^2 and the other terms
-// are small, so nothing cancels. For a state whose scale is s0, R is summed
-// exactly as chi2_profiled's second pass: a move that changes nothing
-// reproduces the current chi^2 bit for bit. *s_d2 as in chi2_profiled.
+// are small, so nothing cancels. The weights are the stored 1 / sigma^2
+// (w2), so no bin divides; against chi2_profiled's (r / sigma)^2 a state's
+// own chi^2 differs by rounding only (a few ulps of chi^2). The channel
+// terms are combined by one warp (the absorbers' scales, then one lane per
+// channel and a warp sum). *s_d2 as in chi2_profiled.
 template <int NSP, typename GetM, typename R2>
 __device__ void chi2_anchored(const chx_ladder_t &L, GetM getm, const R2 *dx, const double *s0,
                               double *s_num, double *s_den, double *s_sq, double *s_scale,
                               double *s_c2, double *s_d2) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nchan = L.nchan, nwin = L.nwin, nkw = L.nkw;
+    const bool cplx = L.cplx;
     for (int ch = warp; ch < nchan; ch += blockDim.x / 32) {
         const double sa = s0[ch / nkw];
         double nu = 0.0, dn = 0.0, R = 0.0, Q = 0.0, Pp = 0.0, D = 0.0;
         for (int q = lane; q < nwin; q += 32) {
             const long g = (long)ch * nwin + q;
             const double2 m = getm(g);
-            const double tr = L.tm_re[g], sg = L.sm[g];
-            if (L.cplx) {
+            const double tr = L.tm_re[g], w = L.w2[g];
+            const double mm = m.x * m.x + m.y * m.y;
+            if (cplx) {
                 const double ti = L.tm_im[g];
                 nu += m.x * tr + m.y * ti;
-                dn += m.x * m.x + m.y * m.y;
-                const double dr = (m.x * sa - tr) / sg;
-                const double di = (m.y * sa - ti) / sg;
-                R += dr * dr + di * di;
-                Q += (m.x * dr + m.y * di) / sg;
-                Pp += (m.x * m.x + m.y * m.y) / (sg * sg);
+                dn += mm;
+                const double rr = m.x * sa - tr, ri = m.y * sa - ti;
+                R += (rr * rr + ri * ri) * w;
+                Q += (m.x * rr + m.y * ri) * w;
             } else {
-                const double mag = sqrt(m.x * m.x + m.y * m.y);
+                const double mag = sqrt(mm);
                 nu += mag * tr;
-                dn += mag * mag;
-                const double dr = (mag * sa - tr) / sg;
-                R += dr * dr;
-                Q += mag * dr / sg;
-                Pp += mag * mag / (sg * sg);
+                dn += mm;
+                const double rr = mag * sa - tr;
+                R += rr * rr * w;
+                Q += mag * rr * w;
             }
+            Pp += mm * w;
             const double a = dx[g].x, b = dx[g].y;
-            D += (a * a + b * b) * L.w2[g];
+            D += (a * a + b * b) * w;
         }
         nu = warp_sum(nu);
         dn = warp_sum(dn);
@@ -535,28 +537,32 @@ __device__ void chi2_anchored(const chx_ladder_t &L, GetM getm, const R2 *dx, co
         }
     }
     __syncthreads();
-    if (tid == 0) {
-        double tot = 0.0, d2 = 0.0;
-        for (int e = 0; e < NSP; ++e) {
-            double sc = 1.0;
-            if (L.profile) {
-                double nu = 0.0, dn = 0.0;
-                for (int q = 0; q < nkw; ++q) {
-                    nu += s_num[e * nkw + q];
-                    dn += s_den[e * nkw + q];
-                }
-                sc = nu / fmax(dn, 1e-30);
+    if (warp == 0) {
+        double sc_l = 1.0;      // lane e < NSP: absorber e's profiled scale
+        if (lane < NSP && L.profile) {
+            double nu = 0.0, dn = 0.0;
+            for (int q = 0; q < nkw; ++q) {
+                nu += s_num[lane * nkw + q];
+                dn += s_den[lane * nkw + q];
             }
-            s_scale[e] = sc;
+            sc_l = nu / fmax(dn, 1e-30);
         }
-        for (int ch = 0; ch < nchan; ++ch) {
-            const double sc = s_scale[ch / nkw], ds = sc - s0[ch / nkw];
-            tot += s_sq[ch];
-            if (ds != 0.0) tot += ds * (2.0 * s_sq[12 + ch] + ds * s_sq[24 + ch]);
-            d2 += sc * sc * s_sq[36 + ch];
+        if (lane < NSP) s_scale[lane] = sc_l;
+        const int e = min(lane / nkw, NSP - 1);
+        const double sc = __shfl_sync(0xffffffffu, sc_l, e);
+        double t = 0.0, d2 = 0.0;
+        if (lane < nchan) {     // lane ch: channel ch's terms
+            const double ds = sc - s0[e];
+            t = s_sq[lane];
+            if (ds != 0.0) t += ds * (2.0 * s_sq[12 + lane] + ds * s_sq[24 + lane]);
+            d2 = sc * sc * s_sq[36 + lane];
         }
-        *s_c2 = tot / L.nfit;
-        if (s_d2) *s_d2 = d2;
+        t = warp_sum(t);
+        d2 = warp_sum(d2);
+        if (lane == 0) {
+            *s_c2 = t / L.nfit;
+            if (s_d2) *s_d2 = d2;
+        }
     }
     __syncthreads();
 }
@@ -590,34 +596,44 @@ __device__ __noinline__ void ft_window_tc(const chx_ladder_t &L, const double *s
     const int KS = ktn * 16 + 8;                    // row stride (taps) of U
     const int nnt = (nchan + 7) >> 3, NP = nnt * 8;
     uint16_t *uh = s_ub, *ul = s_ub + (long)NP * KS;
-    for (int q = tid; q < NP * KS; q += blockDim.x) {
-        const int ch = q / KS, j = q - ch * KS;
-        float u = 0.f;
-        if (ch < nchan && j < ncoef) {
-            const int e = ch / nkw;
-            const long g = (long)ch * ncoef + j;
-            const int id = L.ft_idx[g];
-            const double va = s_tr[e * nk + id], vb = s_tr[e * nk + id + 1];
-            u = (float)((va + (vb - va) * L.ft_frac[g]) * L.ft_w[g]);
+    // the resample, one tap column per thread across the channel rows: the
+    // row's absorber (ch / nkw, nkw <= 3, by multiply and shift) and offsets
+    // are uniform over the warp, so no index divides
+    for (int j = tid; j < KS; j += blockDim.x) {
+        const bool tap = j < ncoef;
+#pragma unroll 4
+        for (int ch = 0; ch < NP; ++ch) {
+            float u = 0.f;
+            if (tap && ch < nchan) {
+                const int e = nkw == 1 ? ch : (nkw == 2 ? ch >> 1 : (ch * 11) >> 5);
+                const long g = (long)ch * ncoef + j;
+                const int id = __ldg(&L.ft_idx[g]);
+                const double va = s_tr[e * nk + id], vb = s_tr[e * nk + id + 1];
+                u = (float)((va + (vb - va) * __ldg(&L.ft_frac[g])) * __ldg(&L.ft_w[g]));
+            }
+            const __nv_bfloat16 h = __float2bfloat16_rn(u);
+            const __nv_bfloat16 l = __float2bfloat16_rn(u - __bfloat162float(h));
+            uh[ch * KS + j] = __bfloat16_as_ushort(h);
+            ul[ch * KS + j] = __bfloat16_as_ushort(l);
         }
-        const __nv_bfloat16 h = __float2bfloat16_rn(u);
-        const __nv_bfloat16 l = __float2bfloat16_rn(u - __bfloat162float(h));
-        uh[q] = __bfloat16_as_ushort(h);
-        ul[q] = __bfloat16_as_ushort(l);
     }
     __syncthreads();
     const int gid = lane >> 2, tig = lane & 3;
     const uint4 *Ah = (const uint4 *)L.ft_frag;
     const uint4 *Al = Ah + (long)mtn * ktn * 32;
     for (int mt = warp; mt < mtn; mt += nwarp) {
-        float acc[MAXNT][4];
+        // hi.hi in acc, the two correction products in acc2: two shorter
+        // dependent chains of MMAs, added at the end
+        float acc[MAXNT][4], acc2[MAXNT][4];
 #pragma unroll
-        for (int t = 0; t < MAXNT; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.f;
+        for (int t = 0; t < MAXNT; ++t)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[t][r] = acc2[t][r] = 0.f;
         const uint4 *ah_p = Ah + (long)mt * ktn * 32 + lane;
         const uint4 *al_p = Al + (long)mt * ktn * 32 + lane;
 #pragma unroll 4
         for (int kt = 0; kt < ktn; ++kt) {
-            const uint4 ah = __ldg(ah_p + kt * 32), al = __ldg(al_p + kt * 32);
+            const uint4 ah = __ldcg(ah_p + kt * 32), al = __ldcg(al_p + kt * 32);
             const int k0 = kt * 16 + tig * 2;
 #pragma unroll
             for (int t = 0; t < MAXNT; ++t) {
@@ -628,11 +644,15 @@ __device__ __noinline__ void ft_window_tc(const chx_ladder_t &L, const double *s
                     const uint32_t bl0 = *(const uint32_t *)&ul[rowo];
                     const uint32_t bl1 = *(const uint32_t *)&ul[rowo + 8];
                     mma_bf16(acc[t], ah, bh0, bh1);
-                    mma_bf16(acc[t], ah, bl0, bl1);
-                    mma_bf16(acc[t], al, bh0, bh1);
+                    mma_bf16(acc2[t], ah, bl0, bl1);
+                    mma_bf16(acc2[t], al, bh0, bh1);
                 }
             }
         }
+#pragma unroll
+        for (int t = 0; t < MAXNT; ++t)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[t][r] += acc2[t][r];
         // D: c0, c1 at row gid, columns tig*2, tig*2+1; c2, c3 at row gid + 8
 #pragma unroll
         for (int t = 0; t < MAXNT; ++t) {
@@ -682,7 +702,8 @@ __device__ void ft_chi2(const chx_ladder_t &L, const double *s_tr, typename Real
             // of the change (added in the order the commit adds it)
             auto getm = [&](long g) {
                 const real2 d = s_x[g];
-                return make_double2((double)d.x + xr_base[2 * g], (double)d.y + xr_base[2 * g + 1]);
+                const double2 b = ((const double2 *)xr_base)[g];
+                return make_double2((double)d.x + b.x, (double)d.y + b.y);
             };
             chi2_anchored<NSP>(L, getm, s_x, xs_base, s_num, s_den, s_sq, s_scale, s_c2, s_d2);
             return;
@@ -915,6 +936,13 @@ __device__ __noinline__ int da_stage1(const chx_ladder_t &L, const chx_mlp_t &M,
 
 // DA: built with the delayed-acceptance screen and the swap log (a ladder of
 // the launch has a surrogate or a log); without it those paths compile away.
+// The Metropolis uniform of (step, rung) when no stream of uniforms is given.
+__device__ __forceinline__ double metropolis_u(uint64_t seed, uint64_t stepc, int rung) {
+    uint64_t h = splitmix64(splitmix64(seed ^ 0xD1B54A32D192ED03ULL) ^
+                            (stepc * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)rung << 32));
+    return u01(splitmix64(h));
+}
+
 template <int NSP, int PREC, int NT, int MINB, bool DA>
 __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restrict__ Ls,
                                                          const int *__restrict__ slot_ladder,
@@ -951,6 +979,17 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     __shared__ uint8_t u_sa[kUndo], u_sb[kUndo], u_sw[kUndo];
     __shared__ double u_p[kUndo][3];
     __shared__ int s_wcnt[NT / 32];          // non-zero MS entries per warp segment
+    // the next step's proposal draws and Metropolis uniform, drawn ahead by
+    // the last thread while the others work on the current step (they do
+    // not depend on the state); double-buffered by step parity
+    __shared__ ProposalDraws s_drw[2];
+    __shared__ double s_umet[2];
+    // the slot's current chi^2 and its rung's inverse temperature (only this
+    // CTA writes the one, the other is fixed for the launch)
+    __shared__ double s_c2cur, s_beta;
+    // the slot's anchored scales (its FP64 chi(R)'s profiled scale per
+    // absorber), kept here beside their global copy
+    __shared__ double s_xs[NSP];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int slot = blockIdx.x;
@@ -1024,6 +1063,10 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         s_bc2 = L.best_chi2[c];
         s_bimp = s_nu = s_flush = s_dsp = s_posd = 0;
         s_gst = L.best_stale ? L.best_stale[c] : 1;
+        s_c2cur = L.chi2[c];
+        s_beta = L.beta_rung[s_rung];
+        propose_draws(s_drw[0], L.seed, s_base + 1, s_rung, natoms, L.swap_frac);
+        s_umet[0] = metropolis_u(L.seed, s_base + 1, s_rung);
     }
     if (tid <= NSP) s_msb[tid] = 0;
     for (int i = tid; i < natoms; i += blockDim.x)
@@ -1040,6 +1083,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         if (threadIdx.x == 0) atomicOr(err, CHX_DEVERR_INDEX);
         return;
     }
+    if (use_xr && tid < NSP) s_xs[tid] = XS[tid];   // read after the step's first barrier
     const float *msT32 = L.ms_T32;
     const bool da_on = DA && s_daon != 0;
     const bool log_on = DA && L.log_cap > 0 && L.log_codes != nullptr && L.log_y != nullptr;
@@ -1049,14 +1093,18 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         // ---- 1. proposal (one thread)
         if (tid == 0) {
             s_step = s_base + st + 1;
-            prop = propose_one(spc, P, L.ideal, natoms, L.seed, s_step, s_rung, L.swap_frac,
-                               L.disp_sigma, L.max_disp);
+            prop = propose_finish(s_drw[st & 1], spc, P, L.ideal, L.disp_sigma, L.max_disp,
+                                  false);
         }
         for (int e = tid; e < nent; e += blockDim.x) s_hist[e] = 0;
         for (int e = tid; e < ndn; e += blockDim.x) s_dn[e] = 0;
         if (tid < NT / 32) s_e2w[tid] = 0.0;
         __syncthreads();
         const int a = prop.a, b = prop.b, nsa = prop.nsa, nsb = prop.nsb, swp = prop.swap;
+        if (tid == NT - 1 && st + 1 < nsteps) {
+            propose_draws(s_drw[(st + 1) & 1], L.seed, s_step + 1, s_rung, natoms, L.swap_frac);
+            s_umet[(st + 1) & 1] = metropolis_u(L.seed, s_step + 1, s_rung);
+        }
 
         // ---- 1b. delayed acceptance, stage 1 (features, prediction, screen)
         const bool feat = swp && (da_on || log_on) && spc(a) != spc(b);
@@ -1174,10 +1222,20 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             const int M = L.ms_M, D = L.ms_D, nblk = L.ms_nblk;
             const uint2 *tpl = (const uint2 *)L.ms_tpl;
             // each template once, resolved at site a (half 0) and site b
-            // (half 1): one load feeds two independent lookup chains
+            // (half 1): one load feeds two independent lookup chains; a
+            // thread loads kTg of its templates before resolving any of them
+            constexpr int kTg = 8;
+            for (int m0 = tid; m0 < M; m0 += kTg * blockDim.x) {
+                uint2 tg[kTg];
+#pragma unroll
+                for (int r = 0; r < kTg; ++r) {
+                    const int m = m0 + r * blockDim.x;
+                    tg[r] = m < M ? __ldg(&tpl[m]) : make_uint2(0u, 0u);
+                }
 #pragma unroll 2
-            for (int m = tid; m < M; m += blockDim.x) {
-                const uint2 t = __ldg(&tpl[m]);
+            for (int r = 0; r < kTg; ++r) {
+                if (m0 + r * blockDim.x >= M) break;
+                const uint2 t = tg[r];
                 int eo[2], en[2], hasa[2];
 #pragma unroll
                 for (int half = 0; half < 2; ++half) {
@@ -1204,6 +1262,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                     atomicAdd(&s_hist[en[1]], 1);
                     atomicSub(&s_hist[eo[1]], 1);
                 }
+            }
             }
         }
         __syncthreads();
@@ -1323,13 +1382,31 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 }
                 if (use_tab) {
                     if (use_xr) {
-                        // FP64 (shell, type) rows: few rows, no rounding
-                        for (int q = 0; q < ndnz; ++q) {
-                            const int2 jc = l_dn[q];
-                            if ((jc.x % nn) / NSP != sa_) continue;
-                            const double *t = L.sstab + (long)jc.x * nk + k0;
-                            acc0 = fma((double)jc.y, __ldg(t), acc0);
-                            if (k1ok) acc1 = fma((double)jc.y, __ldg(t + 1), acc1);
+                        // FP64 (shell, type) rows: few rows, no rounding; four
+                        // rows' loads issued before they are summed in order
+                        for (int q0 = 0; q0 < ndnz; q0 += 4) {
+                            int w4[4];
+                            double2 t4[4];
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                w4[r] = 0;
+                                t4[r] = make_double2(0.0, 0.0);
+                                if (q0 + r < ndnz) {
+                                    const int2 jc = l_dn[q0 + r];
+                                    if ((jc.x % nn) / NSP == sa_) {
+                                        const double *t = L.sstab + (long)jc.x * nk + k0;
+                                        w4[r] = jc.y;
+                                        t4[r].x = __ldg(t);
+                                        if (k1ok) t4[r].y = __ldg(t + 1);
+                                    }
+                                }
+                            }
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) {
+                                if (w4[r] == 0) continue;       // another absorber's row
+                                acc0 = fma((double)w4[r], t4[r].x, acc0);
+                                if (k1ok) acc1 = fma((double)w4[r], t4[r].y, acc1);
+                            }
                         }
                     } else {
                         for (int q = 0; q < ndnz; ++q) {
@@ -1355,7 +1432,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                         const int2 ec = l_ms[q];
                         const float w = (float)ec.y;
                         const float2 p = ffma2(make_float2(w, w),
-                                               __ldg((const float2 *)&msT32[(long)ec.x * nk2 + k0]),
+                                               __ldcg((const float2 *)&msT32[(long)ec.x * nk2 + k0]),
                                                z2);
                         sm = ffma2(p, o2, sm);
                         vq = ffma2(p, p, vq);
@@ -1373,7 +1450,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                         const int2 ec = l_ms[q];
                         const float w = (float)ec.y;
                         sm = ffma2(make_float2(w, w),
-                                   __ldg((const float2 *)&msT32[(long)ec.x * nk2 + k0]), sm);
+                                   __ldcg((const float2 *)&msT32[(long)ec.x * nk2 + k0]), sm);
                     }
                     acc0 += (double)sm.x;
                     acc1 += (double)sm.y;
@@ -1465,13 +1542,13 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
 
         // ---- 4-5. trial chi(R) on the window and its profiled chi^2
         ft_chi2<NSP, PREC>(L, s_tr, s_u, s_x, s_num, s_den, s_sq, s_scale, &s_c2, XR, &s_d2,
-                           kMaxSplit, XS);
+                           kMaxSplit, s_xs);
 
         // ---- 6. Metropolis
         if (tid == 0) {
             double c2 = s_c2;
             int rung = s_rung;
-            const double beta = L.beta_rung[rung];
+            const double beta = s_beta;
             double xo = 0.0;      // the exact terms of x beside the chi^2 change
             if (feat && da_on) {
                 // stage 2 of delayed acceptance: the surrogate's error alone
@@ -1482,12 +1559,12 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 for (int w = 0; w < (int)(blockDim.x / 32); ++w) d += s_de[w];
                 xo = L.energy_beta * d;
             }
-            double x = beta * (c2 - L.chi2[c]) * L.nfit + xo;
+            double x = beta * (c2 - s_c2cur) * L.nfit + xo;
             s_xo = xo;
             if (feat && log_on) {
                 const long long li = (long long)(((s_step - 1) * (uint64_t)L.nrep + (uint64_t)c) %
                                                  (uint64_t)L.log_cap);
-                L.log_y[4 * li] = s_sigma * (float)(c2 - L.chi2[c]);
+                L.log_y[4 * li] = s_sigma * (float)(c2 - s_c2cur);
                 L.log_y[4 * li + 1] = lnb;
                 L.log_y[4 * li + 2] = (float)(L.slot0 + rung);    // chain: ladder and rung
                 L.log_y[4 * li + 3] = (float)s_step;
@@ -1499,9 +1576,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 u = L.u_stream[ui * L.nrep + rung];
             } else {
                 if (L.u_stream) atomicOr(err, CHX_DEVERR_INDEX);
-                uint64_t h = splitmix64(splitmix64(L.seed ^ 0xD1B54A32D192ED03ULL) ^
-                                        (s_step * 0x9E3779B97F4A7C15ULL) ^ ((uint64_t)rung << 32));
-                u = u01(splitmix64(h));
+                u = s_umet[st & 1];
             }
             int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
             // a near tie: a rounding e(k) of the change (FP32 terms and rows,
@@ -1537,10 +1612,9 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             // records), and the trial chi^2 from the slot's FP64 chi(R) plus
             // that, against the current chi^2 the same sums gave
             tie_recheck<NSP>(L, so, smem, s_dir, s_list, 2 * maxaff, ndn, s_msb, s_ndir, s_ndn,
-                             s_dchi, s_tr, CNT, XR, XS, s_num, s_den, s_sq, s_scale, &s_c2t);
+                             s_dchi, s_tr, CNT, XR, s_xs, s_num, s_den, s_sq, s_scale, &s_c2t);
             if (tid == 0) {
-                const int rung = s_rung;
-                const double x = L.beta_rung[rung] * (s_c2t - L.chi2[c]) * L.nfit + s_xo;
+                const double x = s_beta * (s_c2t - s_c2cur) * L.nfit + s_xo;
                 const double u = s_uu;
                 const int acc = (x <= 0.0) || (u < exp(-fmin(x, 60.0)));
                 if (L.tie_stat) {
@@ -1576,7 +1650,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             for (int q = tid; q < NSP * nk; q += blockDim.x) s_chi[q] += s_dchi[q];
             if (use_xr) {
                 const int nx = L.nchan * L.nwin;
-                if (tid < NSP) XS[tid] = s_scale[tid];
+                if (tid < NSP) XS[tid] = s_xs[tid] = s_scale[tid];
                 if (s_tie) {        // the FP64 transform of the near-tie test's change
                     const double *x64 =
                         (const double *)(smem + so.u +
@@ -1619,6 +1693,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                     s_dsp = 1;
                 }
                 L.chi2[c] = s_c2;
+                s_c2cur = s_c2;
                 L.n_acc[c] += 1;
                 if (s_c2 < s_bc2) {          // a new best: the current state
                     s_bc2 = s_c2;

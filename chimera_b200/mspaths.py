@@ -504,8 +504,23 @@ class SupercellPaths:
             self._dev = {}
         for k in what:
             if k not in self._dev:
-                self._dev[k] = N.to_dev(getattr(self, k))
+                a = getattr(self, k)
+                if k == "tpl":
+                    a = a[self.tpl_order()]
+                self._dev[k] = N.to_dev(np.ascontiguousarray(a))
         return self._dev
+
+    def tpl_order(self):
+        """Device order of the templates: the classes interleaved (the i-th
+        template of every class, then the (i+1)-th ...), so that the lanes of
+        a warp, which take consecutive templates, resolve them to different
+        MS entries and their shared-memory count updates rarely collide. The
+        counts are integer sums, so the order does not change them."""
+        off = self.tpl[:, 0].astype(np.int64)
+        first = np.r_[True, off[1:] != off[:-1]]
+        start = np.maximum.accumulate(np.where(first, np.arange(len(off)), 0))
+        rank = np.arange(len(off)) - start
+        return np.lexsort((off, rank))
 
 
 def _host_array(x):
