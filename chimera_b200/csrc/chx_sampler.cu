@@ -42,6 +42,9 @@ constexpr int kMaxCoord = 256;
 constexpr int kReseed = 32;      // taps between exact twiddles in the transform
 constexpr int kMaxSplit = 2;     // threads sharing one bin's taps
 constexpr int kUndo = 32;        // accepted moves kept after a slot's best point
+// MS entry counts below this are resolved from packed words (old entry in
+// bits 0-13, new entry in bits 14-27, occurrences of site a in 28-31)
+constexpr int kMsPackMax = 1 << 14;
 // The near-tie test's model of the FP32 parts of a move's change: each is an
 // independent relative rounding of RMS at most eps (a direct record's term:
 // FP32 exp, sin of an FP64-reduced phase, amplitude products; an MS row
@@ -57,7 +60,7 @@ constexpr double kTieSigma = 6.0;
 // The near-tie FP64 transforms reuse the span u .. dirv (the resampled rows,
 // the transform's output and the direct records, all rebuilt every step).
 struct StepSmem {
-    size_t u, x, dir, dirv, tr, dchi, hist, dn, list, sp, nb, cd, chi, total;
+    size_t u, x, dir, dirv, tr, dchi, hist, dn, list, sp, nb, nbm, cd, chi, total;
     size_t tie;      // bytes the FP64 near-tie buffers need (0: none)
 };
 
@@ -104,6 +107,9 @@ static StepSmem step_smem(const chx_ladder_t &L, int precision) {
     s.list = o; o += al16<int>((size_t)(2 * maxaff + 2 * ndn + 2 * nent + 64));
     s.sp = o; o += al16<uint8_t>((size_t)L.natoms);
     s.nb = o; o += al16<uint16_t>((size_t)2 * (std::max(L.ms_D, 1) + 2));
+    // the neighbourhood words of both sites premultiplied per template
+    // position (kMsPackMax), 4 x (D + 2) each
+    s.nbm = o; o += al16<uint32_t>((size_t)8 * (std::max(L.ms_D, 1) + 2));
     s.cd = o; o += al16<uint8_t>((size_t)((L.mlp || L.log_cap > 0) ? 2 * L.feat_D + 1 : 1));
     s.chi = o; o += al16<double>((size_t)L.nsp * L.nk);
     s.total = o;
@@ -1019,6 +1025,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
     int *s_list = (int *)(smem + so.list);
     uint8_t *s_sp = (uint8_t *)(smem + so.sp);
     uint16_t *s_nb = (uint16_t *)(smem + so.nb);
+    uint32_t *s_nbm = (uint32_t *)(smem + so.nbm);
     double *s_chi = (double *)(smem + so.chi);
     uint8_t *s_codes = (uint8_t *)(smem + so.cd);
     float *s_mpart = (float *)(smem + so.x);       // surrogate scratch, shares the
@@ -1201,7 +1208,33 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
         // template position adds nothing), so that the template loop below
         // reads every position the same way, without branches
         const bool do_ms = nent && swp;
-        if (do_ms) {
+        const bool ms_pack = nent < kMsPackMax;
+        if (do_ms && ms_pack) {
+            // word of neighbourhood slot d of site a (half 0) or b (half 1) at
+            // template position pp: (old species | new species << 14) times
+            // the position's entry multiplier, plus 1 << 28 for site a; slot
+            // D is the site itself, D + 1 an unused position (zero)
+            const int D = L.ms_D, nblk = L.ms_nblk;
+            for (int it = tid; it < 2 * (D + 2); it += blockDim.x) {
+                const int half = it >= D + 2, d = it - half * (D + 2);
+                uint32_t so = 0, sn = 0, fa = 0;
+                if (d < D) {
+                    const int site = __ldg(&L.ms_nbr[(long)(half ? b : a) * D + d]);
+                    so = s_sp[site] & 0x7F;
+                    sn = site == a ? nsa : (site == b ? nsb : so);
+                    fa = site == a;
+                } else if (d == D) {
+                    so = half ? sb_old : sa_old;
+                    sn = half ? nsb : nsa;
+                }
+                const uint32_t w = so | (sn << 14);
+                uint32_t *o = s_nbm + half * 4 * (D + 2) + d;
+                o[0] = w * (uint32_t)nblk + (fa << 28);
+                o[D + 2] = w + (fa << 28);
+                o[2 * (D + 2)] = w * (uint32_t)NSP + (fa << 28);
+                o[3 * (D + 2)] = w * (uint32_t)(NSP * NSP) + (fa << 28);
+            }
+        } else if (do_ms) {
             const int D = L.ms_D;
             for (int d = tid; d < 2 * D; d += blockDim.x) {
                 int half = d >= D;
@@ -1237,6 +1270,22 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 if (m0 + r * blockDim.x >= M) break;
                 const uint2 t = tg[r];
                 int eo[2], en[2], hasa[2];
+                if (ms_pack) {
+                    // one shared load and one add per position (the device
+                    // templates index slot D for the site itself, D + 1 for
+                    // an unused position)
+#pragma unroll
+                    for (int half = 0; half < 2; ++half) {
+                        const uint32_t *nbm = s_nbm + half * 4 * (D + 2);
+                        uint32_t acc = t.x | (t.x << 14);
+#pragma unroll
+                        for (int pp = 0; pp < 4; ++pp)
+                            acc += nbm[pp * (D + 2) + ((t.y >> (8 * pp)) & 0xFF)];
+                        eo[half] = (int)(acc & 0x3FFF);
+                        en[half] = (int)((acc >> 14) & 0x3FFF);
+                        hasa[half] = (int)(acc >> 28);
+                    }
+                } else {
 #pragma unroll
                 for (int half = 0; half < 2; ++half) {
                     const uint16_t *nb = s_nb + half * (D + 2);
@@ -1252,6 +1301,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                         en[half] += ((w >> 8) & 0x7F) * mul;
                         hasa[half] |= w & 0x8000;
                     }
+                }
                 }
                 // a path through both sites counts once (in the half of site a)
                 if (eo[0] != en[0]) {
@@ -1333,13 +1383,8 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
             return v;
         };
         if (PREC != CHX_FP64 && (nent == 0 || msT32 != nullptr)) {
-            // FP32 tables: one item per (absorber species, pair of k points),
-            // each summing only its absorber's direct records, table rows and
-            // MS rows (two float2 loads' worth of k per row), in the same
-            // order as a sum per k over all rows, so the result is the same
-            // to the bit; the FP32 tables' row stride is nk rounded up to even.
-            // The k pairs of one absorber fill whole warps (npw, a multiple
-            // of 32), so no warp runs two absorbers' row loops in turn.
+            // FP32 tables: items per (absorber species, k points), each summing
+            // only its absorber's direct records, table rows and MS rows.
             // Direct records (pairs with a displaced atom) first, one thread
             // per k over all of them as the per-k sum does, so that their
             // cost spreads evenly whatever absorbers they belong to; their
@@ -1369,11 +1414,69 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                 }
                 __syncthreads();
             }
-            const int nk2 = (nk + 1) & ~1, npk = nk2 >> 1, npw = (npk + 31) & ~31;
+            // The FP32 rows are read four k points at a time (the FP32
+            // tables' row stride is nk rounded up to a multiple of 4). A lane
+            // pair takes one (absorber, k quad) item: lane h sums half of the
+            // absorber's MS rows for the whole quad, then the pair trades
+            // partial sums, and lane h finishes k points 4 kq + 2 h and
+            // 4 kq + 2 h + 1 (the items of one warp share an absorber).
+            const int nk4 = (nk + 3) & ~3, npq = nk4 >> 2, npq16 = (npq + 15) & ~15;
+            const int h = tid & 1;
+            const float2 z2 = make_float2(0.f, 0.f), o2 = make_float2(1.f, 1.f);
             double e2acc = 0.0;
-            for (int it = tid; it < NSP * npw; it += blockDim.x) {
-                const int sa_ = it / npw, k0 = 2 * (it - sa_ * npw);
-                if (k0 >= nk) continue;
+            for (int it = tid >> 1; it < NSP * npq16; it += blockDim.x >> 1) {
+                const int sa_ = it / npq16, kq = it - sa_ * npq16;
+                // MS rows: the FP32 running sums of this lane's half (k 0-1 in
+                // A, k 2-3 in B) and, for the near-tie model, the sums of
+                // (count x row)^2 (the rows' FP64 -> FP32 rounding) and of the
+                // running sum^2 (the FP32 accumulation's rounding)
+                float2 smA = z2, smB = z2, vqA = z2, vqB = z2;
+                if (kq < npq) {
+                    const int q0 = s_msb[sa_], q1 = s_msb[sa_ + 1], qm = q0 + ((q1 - q0 + 1) >> 1);
+                    const int qa = h ? qm : q0, qb = h ? q1 : qm;
+                    // eight rows' loads in flight per thread: the phase is bound
+                    // by the bytes a CTA keeps in flight from L2
+                    if (tie_terms) {
+#pragma unroll 8
+                        for (int q = qa; q < qb; ++q) {
+                            const int2 ec = l_ms[q];
+                            const float w = (float)ec.y;
+                            const float4 r = __ldcg((const float4 *)&msT32[(long)ec.x * nk4 + 4 * kq]);
+                            const float2 pA = ffma2(make_float2(w, w), make_float2(r.x, r.y), z2);
+                            const float2 pB = ffma2(make_float2(w, w), make_float2(r.z, r.w), z2);
+                            smA = ffma2(pA, o2, smA);
+                            smB = ffma2(pB, o2, smB);
+                            vqA = ffma2(pA, pA, vqA);
+                            vqB = ffma2(pB, pB, vqB);
+                            vqA = ffma2(smA, smA, vqA);
+                            vqB = ffma2(smB, smB, vqB);
+                        }
+                    } else {
+#pragma unroll 8
+                        for (int q = qa; q < qb; ++q) {
+                            const int2 ec = l_ms[q];
+                            const float w = (float)ec.y;
+                            const float4 r = __ldcg((const float4 *)&msT32[(long)ec.x * nk4 + 4 * kq]);
+                            smA = ffma2(make_float2(w, w), make_float2(r.x, r.y), smA);
+                            smB = ffma2(make_float2(w, w), make_float2(r.z, r.w), smB);
+                        }
+                    }
+                }
+                // lane 0 keeps k 0-1 and takes lane 1's half of them, lane 1
+                // keeps k 2-3; the halves are added (half 0's rows first), one
+                // more FP32 accumulation step
+                const float2 sendS = h ? smA : smB, sendV = h ? vqA : vqB;
+                float2 rS, rV;
+                rS.x = __shfl_xor_sync(0xffffffffu, sendS.x, 1);
+                rS.y = __shfl_xor_sync(0xffffffffu, sendS.y, 1);
+                rV.x = __shfl_xor_sync(0xffffffffu, sendV.x, 1);
+                rV.y = __shfl_xor_sync(0xffffffffu, sendV.y, 1);
+                const float2 oS = h ? smB : smA, oV = h ? vqB : vqA;
+                const float2 sm = make_float2(oS.x + rS.x, oS.y + rS.y);
+                float2 vq = make_float2(oV.x + rV.x, oV.y + rV.y);
+                vq = ffma2(sm, sm, vq);
+                const int k0 = 4 * kq + 2 * h;
+                if (kq >= npq || k0 >= nk) continue;
                 const bool k1ok = k0 + 1 < nk;
                 double acc0 = 0.0, acc1 = 0.0;
                 if (ndir) {
@@ -1413,48 +1516,15 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                             const int2 jc = l_dn[q];
                             if ((jc.x % nn) / NSP != sa_) continue;
                             const float2 t =
-                                __ldg((const float2 *)&L.sstab32[(long)jc.x * nk2 + k0]);
+                                __ldg((const float2 *)&L.sstab32[(long)jc.x * nk4 + k0]);
                             acc0 += (double)((float)jc.y * t.x);
                             acc1 += (double)((float)jc.y * t.y);
                         }
                     }
                 }
-                // near-tie model of the MS rows: sum of (count x row)^2 (the
-                // rows' FP64 -> FP32 rounding) and of the running sum^2 (the
-                // FP32 accumulation's rounding)
-                double v0 = 0.0, v1 = 0.0;
-                if (tie_terms) {
-                    const int q0 = s_msb[sa_], q1 = s_msb[sa_ + 1];
-                    const float2 z2 = make_float2(0.f, 0.f), o2 = make_float2(1.f, 1.f);
-                    float2 sm = z2, vq = z2;
-#pragma unroll 8
-                    for (int q = q0; q < q1; ++q) {
-                        const int2 ec = l_ms[q];
-                        const float w = (float)ec.y;
-                        const float2 p = ffma2(make_float2(w, w),
-                                               __ldcg((const float2 *)&msT32[(long)ec.x * nk2 + k0]),
-                                               z2);
-                        sm = ffma2(p, o2, sm);
-                        vq = ffma2(p, p, vq);
-                        vq = ffma2(sm, sm, vq);
-                    }
-                    acc0 += (double)sm.x;
-                    acc1 += (double)sm.y;
-                    v0 = (double)vq.x;
-                    v1 = (double)vq.y;
-                } else {
-                    const int q0 = s_msb[sa_], q1 = s_msb[sa_ + 1];
-                    float2 sm = make_float2(0.f, 0.f);
-#pragma unroll 16
-                    for (int q = q0; q < q1; ++q) {
-                        const int2 ec = l_ms[q];
-                        const float w = (float)ec.y;
-                        sm = ffma2(make_float2(w, w),
-                                   __ldcg((const float2 *)&msT32[(long)ec.x * nk2 + k0]), sm);
-                    }
-                    acc0 += (double)sm.x;
-                    acc1 += (double)sm.y;
-                }
+                acc0 += (double)sm.x;
+                acc1 += (double)sm.y;
+                const double v0 = (double)vq.x, v1 = (double)vq.y;
                 const double inv = fmax(CNT[sa_], 1.0);
                 const int o = sa_ * nk + k0;
                 if (tie_terms) {
@@ -1507,7 +1577,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
                     int2 jc = l_dn[q];
                     add_by_species<NSP>(acc, (jc.x % nn) / NSP,
                                         (double)((float)jc.y *
-                                                 __ldg(&L.sstab32[(long)jc.x * nk + ik])));
+                                                 __ldg(&L.sstab32[(long)jc.x * ((nk + 3) & ~3) + ik])));
                 }
             }
             // MS rows, one run per absorber block: independent loads, no divides
@@ -1527,7 +1597,7 @@ __global__ void __launch_bounds__(NT, MINB) k_step(const chx_ladder_t *__restric
 #pragma unroll 16
                     for (int q = q0; q < q1; ++q) {
                         int2 ec = l_ms[q];
-                        sa = fmaf((float)ec.y, __ldg(&msT32[(long)ec.x * nk + ik]), sa);
+                        sa = fmaf((float)ec.y, __ldg(&msT32[(long)ec.x * ((nk + 3) & ~3) + ik]), sa);
                     }
                     acc[a_] += (double)sa;
                 }
@@ -2247,7 +2317,7 @@ static int plan_ladders(const chx_ladder_t *H, int nladders, int precision, Step
     for (int i = 0; i < nladders; ++i) {
         const chx_ladder_t &L = H[i];
         CHX_REQUIRE(L.nsp == nsp, "sampler: one launch needs one species count");
-        CHX_REQUIRE(!L.ms_nblk || (L.ms_tpl && L.ms_nbr && L.ms_D > 0 && L.ms_D < 0xFE &&
+        CHX_REQUIRE(!L.ms_nblk || (L.ms_tpl && L.ms_nbr && L.ms_D > 0 && L.ms_D < 0xFD &&
                                    L.ms_M > 0 && L.natoms < 65536),
                     "sampler: ladder %d has incomplete multiple-scattering templates", i);
         CHX_REQUIRE(L.ncoord > 0 && L.ncoord <= kMaxCoord && L.nk > 0 && L.nkw >= 1 &&

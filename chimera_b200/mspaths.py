@@ -506,7 +506,7 @@ class SupercellPaths:
             if k not in self._dev:
                 a = getattr(self, k)
                 if k == "tpl":
-                    a = a[self.tpl_order()]
+                    a = self.device_templates()
                 self._dev[k] = N.to_dev(np.ascontiguousarray(a))
         return self._dev
 
@@ -521,6 +521,20 @@ class SupercellPaths:
         start = np.maximum.accumulate(np.where(first, np.arange(len(off)), 0))
         rank = np.arange(len(off)) - start
         return np.lexsort((off, rank))
+
+    def device_templates(self):
+        """The templates as the sampler step reads them: in tpl_order, with
+        the position bytes SELF and NONE replaced by D and D + 1, the two
+        slots the step appends to each site's neighbourhood (the site itself
+        and a zero), so that every position is a plain table index."""
+        if self.D + 1 >= self.SELF:
+            raise ValueError(f"{self.D} neighbourhood sites leave no room for the extra slots")
+        t = np.ascontiguousarray(self.tpl[self.tpl_order()])
+        pos = np.ascontiguousarray(t[:, 1]).view(np.uint8).reshape(-1, 4)  # position p: byte p
+        pos[pos == self.SELF] = self.D
+        pos[pos == self.NONE] = self.D + 1
+        t[:, 1] = pos.reshape(-1).view(np.int32)
+        return t
 
 
 def _host_array(x):

@@ -47,11 +47,11 @@ def _host(x):
 
 def _fp32_rows(t):
     """FP32 copy of a (rows, nk) FP64 table with the row stride rounded up to
-    an even count (a zero column when nk is odd), the layout of the step
-    kernel's FP32 tables: it reads k points in pairs."""
+    a multiple of 4 (zero columns past nk), the layout of the step kernel's
+    FP32 tables: it reads k points in 16-byte groups of four."""
     import torch
     rows, nk = t.shape
-    out = torch.zeros((rows, nk + (nk & 1)), dtype=torch.float32, device=t.device)
+    out = torch.zeros((rows, (nk + 3) & ~3), dtype=torch.float32, device=t.device)
     out[:, :nk] = t
     return out
 

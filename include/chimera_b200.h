@@ -283,8 +283,9 @@ typedef struct {
     double s02;
     const double *sstab;             /* (nshell*nsp*nsp, nk) ideal-shell terms, or NULL */
     const float *sstab32;            /* the same table in FP32 (CHX_FP32C), or NULL;
-                                        row stride nk rounded up to even, the pad
-                                        column zero (k points are read in pairs)   */
+                                        row stride nk rounded up to a multiple of
+                                        4, pad columns zero, rows 16-byte aligned
+                                        (k points are read four at a time)         */
     /* exact multiple scattering, ms_nblk == 0 when off. The paths through a
        site are ms_M shared templates {class entry offset, 4 position bytes:
        neighbourhood index of the absorber and slots 0-2, 0xFE the site itself,
@@ -294,7 +295,7 @@ typedef struct {
     const int *ms_nbr;               /* (natoms, ms_D) neighbourhood site indices */
     const double *ms_T;              /* (nsp*ms_nblk, nk)                         */
     const float *ms_T32;             /* the same table in FP32 (CHX_FP32C), or NULL;
-                                        row stride nk rounded up to even, as sstab32 */
+                                        row stride and alignment as sstab32        */
     /* pair-interaction prior, etab NULL when off (method_a_rmc.py:147-157,310-320) */
     const double *etab;              /* (nshell*nsp*nsp) eV per directed pair     */
     double energy_beta;

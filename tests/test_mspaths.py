@@ -270,3 +270,50 @@ def test_reference_construction_lays_the_same_paths(classes, nsp):
     P_slot = np.vstack([sp.p_slot, -np.ones((1, 3), np.int32)]).astype(np.int32)
     assert digest(P_abs, P_cls, P_slot, sp.inc) == str(g[key + "digest"])
     assert ms.T is None and ms.lib is not None
+
+
+@pytest.mark.parametrize("nsp", [2, 3])
+def test_device_templates_resolve_the_swap_from_packed_words(classes, nsp):
+    """The sampler step's form of the template walk: device templates (class-
+    interleaved, SELF/NONE as neighbourhood slots D and D + 1) against packed
+    neighbourhood words (old entry bits 0-13, new entry 14-27, occurrences of
+    site a 28-31), summed per template, give the oracle's count change."""
+    from oracle import kernels as K
+    cell = L.CrystalSupercell("fcc", (5, 5, 5), 3.59)
+    sp = MP.SupercellPaths(classes, cell.ideal, cell.H, 3.59, nsp)
+    assert sp.nent < 1 << 14
+    t = sp.device_templates()
+    assert np.array_equal(np.sort(t[:, 0]), np.sort(sp.tpl[:, 0]))
+    rng = np.random.default_rng(10 + nsp)
+    species = rng.integers(0, nsp, sp.natoms).astype(np.int32)
+    a, b = 23, int(sp.nbr[23, 5])
+    while species[a] == species[b]:
+        species[b] = (species[b] + 1) % nsp
+    nsa, nsb = int(species[b]), int(species[a])
+    D = sp.D
+    mul = [sp.nblk, 1, nsp, nsp * nsp]
+    words = np.zeros((2, 4, D + 2), np.int64)
+    for half, site in enumerate((a, b)):
+        for d in range(D + 1):
+            s = site if d == D else int(sp.nbr[site, d])
+            so = int(species[s])
+            sn = nsa if s == a else (nsb if s == b else so)
+            fa = int(s == a and d < D)
+            for pp in range(4):
+                words[half, pp, d] = (so | sn << 14) * mul[pp] + (fa << 28)
+    dC = np.zeros(sp.nent)
+    for off, code in t:
+        code = int(code) & 0xFFFFFFFF
+        for half in range(2):
+            acc = int(off) | int(off) << 14
+            for pp in range(4):
+                acc += int(words[half, pp, (code >> 8 * pp) & 0xFF])
+            eo, en, hasa = acc & 0x3FFF, (acc >> 14) & 0x3FFF, acc >> 28
+            if half == 1 and hasa:
+                continue
+            dC[en] += 1
+            dC[eo] -= 1
+    ref = K.ms_delta(species[None], sp.inc, sp.p_abs, sp.p_cls, sp.p_slot, sp.npath,
+                     sp.cls_off, nsp, sp.nblk, np.array([a], np.int32), np.array([b], np.int32),
+                     np.array([nsa], np.int32), np.array([nsb], np.int32))[0]
+    assert np.array_equal(dC, ref)
