@@ -688,7 +688,12 @@ def bench_uneven(args):
                        "species_counts": [g.nsp for g in bs.groups],
                        "ladders": len(specs), "replicas": bs.nslots, "periods": nb},
             "batched": {"attempts_per_s": att / t_batch, "gpu_s": t_batch,
-                        "launch_shapes": [list(t["shape"]) for t in bs.tuning]},
+                        "launch_shapes": [list(t["shape"]) for t in bs.tuning],
+                        "tuning": [{"nsp": g.nsp, "ladders": g.nladders, "replicas": g.nslots,
+                                    "shape": list(t["shape"]),
+                                    "tensor_core_transform": t.get("tensor_core_transform"),
+                                    "us_per_step": t["us_per_step"]}
+                                   for g, t in zip(bs.groups, bs.tuning)]},
             "one_ladder_per_launch": {"attempts_per_s": att / t_sep, "gpu_s": t_sep},
             "learned": {"attempts_per_s": att / t_learned, "gpu_s": t_learned,
                         "surrogates": len(bs.surrogates),
