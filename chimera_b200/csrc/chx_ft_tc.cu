@@ -33,6 +33,7 @@
 #include <cstring>
 #include <cuda_bf16.h>
 #include "chx_common.cuh"
+#include "chx_tc.cuh"
 
 namespace chx {
 
@@ -43,8 +44,6 @@ constexpr int kTcResKp = 256;                          // largest padded nk kept
 constexpr int kTcBox = 32 * 16 * 8;                     // one staged chi(R) box: 32 rows x 16 FP64
 constexpr int kTcAcc = 2;                              // accumulators in tensor memory
 constexpr int kTcThreads = 192;                        // 4 epilogue warps, producer, MMA
-constexpr uint32_t kTcLBO = 128;                        // core matrices along K (bytes)
-constexpr int kTcSpin = 1 << 24;
 constexpr int kTcTmemCols = kTcAcc * kTcN;              // FP32 accumulator columns
 
 // Operand modes: split-BF16 (two BF16 parts of 2 bytes, MMA K = 16, kind::f16
@@ -80,37 +79,6 @@ struct TcMode {
                           (k * esz) % 16);
     }
 };
-
-__device__ __forceinline__ uint32_t tc_smem(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// shared-memory matrix descriptor: start address, leading (K) and stride
-// (row-group) byte offsets, descriptor version 1, no swizzle
-__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t sbo) {
-    return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)(kTcLBO >> 4) << 16) |
-           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
-}
-
-__device__ __forceinline__ void tc_mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem(bar)), "r"(count)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool tc_mbar_wait(uint64_t *bar, uint32_t parity) {
-    const uint32_t a = tc_smem(bar);
-    for (int it = 0; it < kTcSpin; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-            " selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
 
 __device__ __forceinline__ void tc_load_tile(void *dst, const void *src, uint32_t bytes,
                                              uint64_t *bar) {
@@ -154,13 +122,6 @@ __device__ __forceinline__ uint32_t tc_tf32(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return r;
-}
-
-__device__ __forceinline__ void tc_commit(uint64_t *bar) {
-    asm volatile(
-        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            tc_smem(bar))
-        : "memory");
 }
 
 // One operand of the contraction: X (R x C, element (r, c) at X[r*sr + c*sc])

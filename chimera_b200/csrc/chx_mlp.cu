@@ -2,8 +2,8 @@
 // per-CTA code the sampler runs), training forward + loss + gradient, Adam.
 //
 // Training works on a batch of B logged swaps. The two dense layers
-// (B x H x H) run on the tensor cores through one strided BF16 GEMM
-// (mma.sync m16n8k16, FP32 accumulation) that serves the forward (H W), the
+// (B x H x H) run on the tcgen05 tensor cores through one strided BF16 GEMM
+// (FP32 accumulation in tensor memory) that serves the forward (H W), the
 // weight gradients (H^T dZ) and the input gradients (dZ W^T). Layer 1 is a
 // gather-sum of W1 rows (its input is one-hot), and its weight gradient a
 // per-site scatter done as one CTA per input site with no atomics. Every
@@ -11,6 +11,7 @@
 // Rounding: weights BF16; activations and the back-propagated dZ rounded to
 // BF16 before they enter a GEMM; everything else FP32.
 #include "chx_mlp.cuh"
+#include "chx_tc.cuh"
 
 namespace chx {
 
@@ -22,86 +23,163 @@ static inline int64_t mlp_nin(int nsp, int D, int nchain) {
 // C[m][n] = sum_k A(m,k) B(k,n) (+ bias[n]); A(m,k) = A[m*sam + k*sak],
 // B(k,n) = B[k*sbk + n*sbn] (BF16 bit patterns); C FP32 with row stride ldc;
 // with Cb, also BF16(relu(C)) (relu != 0) or BF16(C) into Cb (row stride ldc).
-constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
+//
+// On the tcgen05 tensor cores: one CTA (4 warps) per 128 x 128 tile of C,
+// the FP32 accumulator in 128 columns of tensor memory. K goes in chunks of
+// 32: all threads stage the chunk's A rows and B columns (any strides, so
+// plain loads) into two 8 KB tiles in the no-swizzle K-major core-matrix
+// layout (8 x 16-byte core matrices, 128 B apart along K, 512 B per row
+// group), then one thread issues two 128 x 128 x 16 BF16 MMAs (kind::f16)
+// and commits them to the chunk buffer's mbarrier; two buffers, so the
+// staging of chunk c + 1 overlaps the MMAs of chunk c. The epilogue warp w
+// reads accumulator lanes 32w..32w+31 (one row each) with tcgen05.ld. Every
+// wait is bounded; a wait that runs out makes the tile's outputs NaN after
+// the MMAs the CTA issued have completed.
+constexpr int kGm = 128, kGn = 128, kGk = 32;
+constexpr uint32_t kGsbo = (kGk * 2 / 16) * 128;          // row-group stride of a tile
+constexpr uint32_t kGtile = kGm * kGk * 2;                 // one 128 x 32 BF16 tile
+constexpr uint32_t kGidesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                             ((uint32_t)(kGn >> 3) << 17) | ((uint32_t)(kGm >> 4) << 24);
+// two buffers of two tiles and alignment slack, rounded up so that at most
+// four CTAs (4 x 128 tensor-memory columns of 512) share an SM
+constexpr size_t kGsmem = 57 * 1024;
+static_assert(4 * kGtile + 1024 <= kGsmem && 5 * (kGsmem + 1024) > 228 * 1024,
+              "GEMM shared memory must hold the buffers and cap the CTAs per SM at four");
 
-__device__ __forceinline__ uint32_t pack2(uint16_t lo, uint16_t hi) {
-    return (uint32_t)lo | ((uint32_t)hi << 16);
+// byte offset of element (r, k) in a 128 x 32 BF16 tile
+__device__ __forceinline__ uint32_t g_off(int r, int k) {
+    return (uint32_t)((r >> 3) * kGsbo + (k >> 3) * kTcLBO + (r & 7) * 16 + (k & 7) * 2);
 }
 
-__global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t *__restrict__ A, long sam,
-                                                   long sak, const uint16_t *__restrict__ B,
-                                                   long sbk, long sbn, float *__restrict__ C,
-                                                   long ldc, uint16_t *__restrict__ Cb,
-                                                   const float *__restrict__ bias, int M, int N,
-                                                   int K, int relu) {
-    __shared__ uint16_t sa[GT_M][GT_K + 2];
-    __shared__ uint16_t sb[GT_K][GT_N + 2];
+__device__ __forceinline__ void g_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+            tmem),
+        "l"(da), "l"(db), "r"(kGidesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A, long sam,
+                                                 long sak, const uint16_t *__restrict__ B,
+                                                 long sbk, long sbn, float *__restrict__ C,
+                                                 long ldc, uint16_t *__restrict__ Cb,
+                                                 const float *__restrict__ bias, int M, int N,
+                                                 int K, int relu) {
+    extern __shared__ uint8_t g_raw[];
+    __shared__ __align__(8) uint64_t buf_bar[2], done_bar;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    uint8_t *sm = (uint8_t *)(((uintptr_t)g_raw + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g = lane >> 2, t = lane & 3;
-    const int m0 = blockIdx.y * GT_M, n0 = blockIdx.x * GT_N;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;   // the warp's 32 x 32 sub-tile
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
-    for (int k0 = 0; k0 < K; k0 += GT_K) {
-        for (int q = tid; q < GT_M * GT_K; q += blockDim.x) {
-            int mm = q / GT_K, kk = q % GT_K, gm = m0 + mm, gk = k0 + kk;
-            sa[mm][kk] = (gm < M && gk < K) ? A[gm * sam + gk * sak] : (uint16_t)0;
-        }
-        for (int q = tid; q < GT_K * GT_N; q += blockDim.x) {
-            int kk = q / GT_N, nn = q % GT_N, gk = k0 + kk, gn = n0 + nn;
-            sb[kk][nn] = (gk < K && gn < N) ? B[gk * sbk + gn * sbn] : (uint16_t)0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int r = wm + i * 16;
-            uint32_t a0 = pack2(sa[r + g][2 * t], sa[r + g][2 * t + 1]);
-            uint32_t a1 = pack2(sa[r + g + 8][2 * t], sa[r + g + 8][2 * t + 1]);
-            uint32_t a2 = pack2(sa[r + g][2 * t + 8], sa[r + g][2 * t + 9]);
-            uint32_t a3 = pack2(sa[r + g + 8][2 * t + 8], sa[r + g + 8][2 * t + 9]);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int cc = wn + j * 8 + g;
-                uint32_t b0 = pack2(sb[2 * t][cc], sb[2 * t + 1][cc]);
-                uint32_t b1 = pack2(sb[2 * t + 8][cc], sb[2 * t + 9][cc]);
-                asm volatile(
-                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-                    "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                    : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]),
-                      "+f"(acc[i][j][3])
-                    : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-            }
-        }
-        __syncthreads();
+    const int m0 = blockIdx.y * kGm, n0 = blockIdx.x * kGn;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         tc_smem(&s_tmem)),
+                     "r"(kGn)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    if (tid == 0) {
+        tc_mbar_init(&buf_bar[0], 1);
+        tc_mbar_init(&buf_bar[1], 1);
+        tc_mbar_init(&done_bar, 1);
+        s_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const int nkc = (K + kGk - 1) / kGk;
+    for (int kc = 0; kc < nkc; ++kc) {
+        const int b = kc & 1;
+        uint8_t *sa = sm + (size_t)b * 2 * kGtile, *sb = sa + kGtile;
+        // the buffer's previous chunk (kc - 2) has been read by its MMAs
+        if (kc >= 2 && !tc_mbar_wait(&buf_bar[b], (uint32_t)((kc / 2 - 1) & 1))) s_fail = 1;
+        __syncthreads();
+        if (s_fail) break;
+        // one item: 8 consecutive k of one row of A and of one column of B
+        for (int q = tid; q < kGm * (kGk / 8); q += blockDim.x) {
+            const int r = q >> 2, kg = (q & 3) * 8, k0 = kc * kGk + kg;
+            const int gm = m0 + r, gn = n0 + r;
+            __align__(16) uint16_t va[8], vb[8];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int gm = m0 + wm + i * 16 + g + ((q & 2) ? 8 : 0);
-                const int gn = n0 + wn + j * 8 + 2 * t + (q & 1);
-                if (gm >= M || gn >= N) continue;
-                float v = acc[i][j][q];
-                if (bias) v += bias[gn];
-                C[gm * ldc + gn] = v;
-                if (Cb)
-                    Cb[gm * ldc + gn] =
-                        __bfloat16_as_ushort(__float2bfloat16_rn(relu ? fmaxf(v, 0.f) : v));
+            for (int j = 0; j < 8; ++j) {
+                const bool kin = k0 + j < K;
+                va[j] = (gm < M && kin) ? A[gm * sam + (long)(k0 + j) * sak] : (uint16_t)0;
+                vb[j] = (gn < N && kin) ? B[(long)(k0 + j) * sbk + gn * sbn] : (uint16_t)0;
             }
+            *(uint4 *)(sa + g_off(r, kg)) = *(const uint4 *)va;
+            *(uint4 *)(sb + g_off(r, kg)) = *(const uint4 *)vb;
+        }
+        // the staged tiles, written through the generic proxy, become visible
+        // to the tensor cores' reads
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int kk = 0; kk < kGk / 16; ++kk) {
+                const uint32_t ko = kk * 2 * kTcLBO;    // one MMA's K = two core matrices
+                g_mma(tmem, tc_desc(tc_smem(sa) + ko, kGsbo), tc_desc(tc_smem(sb) + ko, kGsbo),
+                      (kc | kk) != 0);
+            }
+            tc_commit(&buf_bar[b]);
+        }
+    }
+    // every MMA issued by this CTA has completed (also after a failed wait)
+    if (tid == 0) tc_commit(&done_bar);
+    if (!tc_mbar_wait(&done_bar, 0)) s_fail = 1;
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool fail = s_fail != 0;
+    const int gm = m0 + warp * 32 + lane;
+    for (int q = 0; q < kGn / 32; ++q) {
+        uint32_t v[32];
+        const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * 32);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, "
+            "%26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]),
+              "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+              "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+              "=r"(v[30]), "=r"(v[31])
+            : "r"(ta)
+            : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (gm >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const int gn = n0 + q * 32 + j;
+            if (gn >= N) continue;
+            float x = fail ? __int_as_float(0x7fc00000) : (nkc ? __uint_as_float(v[j]) : 0.f);
+            if (bias) x += bias[gn];
+            C[gm * ldc + gn] = x;
+            if (Cb)
+                Cb[gm * ldc + gn] =
+                    __bfloat16_as_ushort(__float2bfloat16_rn(relu ? fmaxf(x, 0.f) : x));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kGn)
+                     : "memory");
 }
 
 static void gemm(const uint16_t *A, long sam, long sak, const uint16_t *B, long sbk, long sbn,
                  float *C, long ldc, uint16_t *Cb, const float *bias, int M, int N, int K,
                  int relu, cudaStream_t st) {
-    dim3 grid((N + GT_N - 1) / GT_N, (M + GT_M - 1) / GT_M);
-    k_gemm_bf16<<<grid, 128, 0, st>>>(A, sam, sak, B, sbk, sbn, C, ldc, Cb, bias, M, N, K, relu);
+    cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGsmem);
+    dim3 grid((N + kGn - 1) / kGn, (M + kGm - 1) / kGm);
+    k_gemm_tc<<<grid, 128, kGsmem, st>>>(A, sam, sak, B, sbk, sbn, C, ldc, Cb, bias, M, N, K,
+                                         relu);
 }
 
 // ---------------------------------------------------------------- forward
