@@ -251,17 +251,7 @@ struct TcSums {
     double *part;        // (rows, ntn, kSums)
     int nR;
     double s0;
-    const float2 *tgt32; // FP32 copies of tgt and wgt (in the scratch)
-    const float *wgt32;
 };
-
-__global__ void k_tc_sums_prep(const double *__restrict__ tgt, const double *__restrict__ wgt,
-                               int nR, float2 *__restrict__ t32, float *__restrict__ w32) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nR) return;
-    t32[b] = make_float2((float)tgt[2 * b], (float)tgt[2 * b + 1]);
-    w32[b] = (float)wgt[b];
-}
 
 template <bool TF32, bool RES, bool SUMS>
 __global__ void __launch_bounds__(kTcThreads, 1) k_ft_tc(const uint8_t *__restrict__ Ahi,
@@ -455,25 +445,38 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_ft_tc(const uint8_t *__restri
                 float nu = 0.f, dn = 0.f, R = 0.f, Q = 0.f, P = 0.f, Ru = 0.f, Qu = 0.f;
                 const float s0 = (float)sums.s0;
                 const int b0 = (nt * kTcN) >> 1;
+                // the tile's 64 bins {target re, im, weight, in window}, in
+                // FP32, staged once per warp in its (here unused) store boxes;
+                // a bin off the window carries zeros, so it adds nothing
+                float4 *bw = (float4 *)stg;
+                __syncwarp();
+                for (int j = lane; j < 64; j += 32) {
+                    const int bin = b0 + j;
+                    float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (bin < sums.nR) {
+                        const double w = sums.wgt[bin];
+                        if (w != 0.0)
+                            f = make_float4((float)sums.tgt[2 * bin], (float)sums.tgt[2 * bin + 1],
+                                            (float)w, 1.f);
+                    }
+                    bw[j] = f;
+                }
+                __syncwarp();
 #pragma unroll
                 for (int j = 0; j < 64; ++j) {
-                    const int bin = b0 + j;
-                    const float w = bin < sums.nR ? sums.wgt32[bin] : 0.f;
-                    if (w != 0.f) {
-                        const float mr = __uint_as_float(v[j >> 4][(j & 15) * 2]);
-                        const float mi = __uint_as_float(v[j >> 4][(j & 15) * 2 + 1]);
-                        const float2 t = sums.tgt32[bin];
-                        const float rr = fmaf(s0, mr, -t.x), ri = fmaf(s0, mi, -t.y);
-                        const float mm = fmaf(mr, mr, mi * mi);
-                        const float r2 = fmaf(rr, rr, ri * ri), q2 = fmaf(mr, rr, mi * ri);
-                        nu = fmaf(mr, t.x, fmaf(mi, t.y, nu));
-                        dn += mm;
-                        R = fmaf(w, r2, R);
-                        Q = fmaf(w, q2, Q);
-                        P = fmaf(w, mm, P);
-                        Ru += r2;
-                        Qu += q2;
-                    }
+                    const float4 f = bw[j];
+                    const float mr = __uint_as_float(v[j >> 4][(j & 15) * 2]);
+                    const float mi = __uint_as_float(v[j >> 4][(j & 15) * 2 + 1]);
+                    const float rr = fmaf(s0, mr, -f.x), ri = fmaf(s0, mi, -f.y);
+                    const float mm = fmaf(mr, mr, mi * mi);
+                    const float r2 = fmaf(rr, rr, ri * ri), q2 = fmaf(mr, rr, mi * ri);
+                    nu = fmaf(mr, f.x, fmaf(mi, f.y, nu));
+                    dn = fmaf(f.w, mm, dn);
+                    R = fmaf(f.z, r2, R);
+                    Q = fmaf(f.z, q2, Q);
+                    P = fmaf(f.z, mm, P);
+                    Ru = fmaf(f.w, r2, Ru);
+                    Qu = fmaf(f.w, q2, Qu);
                 }
                 const int row = y + lane;
                 if (row < rows) {
@@ -598,21 +601,20 @@ static cudaError_t tc_launch(int grid, size_t smem, cudaStream_t st, const uint8
 // rows x ntn partial window sums after the operand scratch (the fused form)
 static size_t tc_sums_bytes(int rows, int nR) {
     const int ntn = (2 * nR + kTcN - 1) / kTcN;
-    return ((size_t)rows * ntn * kSums * sizeof(double) + 255) / 256 * 256 +
-           ((size_t)nR * 12 + 255) / 256 * 256;
+    return ((size_t)rows * ntn * kSums * sizeof(double) + 255) / 256 * 256;
 }
 
-// row r of out = the sum over column tiles (in order) of its partials
+// sum q of row r of out = the sum over column tiles (in order) of its
+// partials; one thread per (row, sum)
 __global__ void k_tc_sums_reduce(const double *__restrict__ part, int rows, int ntn,
                                  double *__restrict__ out) {
-    const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rows) return;
-    double a[kSums] = {};
-    for (int t = 0; t < ntn; ++t)
-#pragma unroll
-        for (int q = 0; q < kSums; ++q) a[q] += part[(r * ntn + t) * kSums + q];
-#pragma unroll
-    for (int q = 0; q < kSums; ++q) out[r * kSums + q] = a[q];
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)rows * kSums) return;
+    const long r = i / kSums;
+    const int q = (int)(i - r * kSums);
+    double a = 0.0;
+    for (int t = 0; t < ntn; ++t) a += part[(r * ntn + t) * kSums + q];
+    out[i] = a;
 }
 
 // out: chi(R) (sums NULL), or with sums the (rows, 4) window sums
@@ -676,26 +678,18 @@ static int ft_batch_tc_mode(const double *chi, int rows, int nk, const double *b
     if (sums) {
         TcSums sm = *sums;
         sm.part = (double *)(base + p.total);
-        const int ntn_ = (2 * nR + kTcN - 1) / kTcN;
-        uint8_t *f32 = base + p.total +
-                       ((size_t)rows * ntn_ * kSums * sizeof(double) + 255) / 256 * 256;
-        sm.tgt32 = (const float2 *)f32;
-        sm.wgt32 = (const float *)(f32 + (size_t)nR * 8);
-        k_tc_sums_prep<<<(nR + 255) / 256, 256, 0, st>>>(sums->tgt, sums->wgt, nR,
-                                                          (float2 *)f32,
-                                                          (float *)(f32 + (size_t)nR * 8));
-        CHX_CHECK_LAUNCH("ft_sums prep");
         e = res ? tc_launch<TF32, true, true>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol,
                                               ntn, mtiles, tm, sm, err)
                 : tc_launch<TF32, false, true>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol,
                                                ntn, mtiles, tm, sm, err);
         if (e != cudaSuccess) return cuda_fail(e, "ft_sums tc launch");
         CHX_CHECK_LAUNCH("ft_sums tc");
-        k_tc_sums_reduce<<<(rows + 255) / 256, 256, 0, st>>>(sm.part, rows, ntn, out);
+        k_tc_sums_reduce<<<(unsigned)(((long)rows * kSums + 255) / 256), 256, 0, st>>>(
+            sm.part, rows, ntn, out);
         CHX_CHECK_LAUNCH("ft_sums reduce");
         return CHX_OK;
     }
-    const TcSums none = {nullptr, nullptr, nullptr, 0, 1.0, nullptr, nullptr};
+    const TcSums none = {nullptr, nullptr, nullptr, 0, 1.0};
     e = res ? tc_launch<TF32, true, false>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol, ntn,
                                            mtiles, tm, none, err)
             : tc_launch<TF32, false, false>(grid, smem, st, ahi, al, rows, bhi, bl, nkt, ncol,
@@ -712,7 +706,7 @@ int64_t ft_sums_tc_scratch(int rows, int nk, int nR, bool tf32) {
 int ft_sums_tc(const double *chi, int rows, int nk, const double *basis, int nR,
                const double *target, const double *weight, double s0, double *out4,
                void *scratch, int64_t scratch_bytes, cudaStream_t st, bool tf32) {
-    const TcSums sums = {target, weight, nullptr, nR, s0, nullptr, nullptr};
+    const TcSums sums = {target, weight, nullptr, nR, s0};
     return tf32 ? ft_batch_tc_mode<true>(chi, rows, nk, basis, nR, out4, scratch, scratch_bytes,
                                          st, &sums)
                 : ft_batch_tc_mode<false>(chi, rows, nk, basis, nR, out4, scratch, scratch_bytes,
