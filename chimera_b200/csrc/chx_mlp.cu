@@ -51,6 +51,57 @@ __device__ __forceinline__ uint32_t g_off(int r, int k) {
     return (uint32_t)((r >> 3) * kGsbo + (k >> 3) * kTcLBO + (r & 7) * 16 + (k & 7) * 2);
 }
 
+// Stage one 128 x 32 chunk of an operand X(r, k) = X[r*sr + k*sk] (rows
+// r0.., K columns k0..) into the core-matrix tile, zero past R and K. mode 1:
+// k contiguous (sk == 1), a 16-byte load per 8 k of one row; mode 2: rows
+// contiguous (sr == 1), a 16-byte load per 8 rows of one k, scattered into
+// the 8 rows' core matrices; mode 0: one element at a time. The vector modes
+// need the base 16-byte aligned and the other stride a multiple of 8.
+__device__ __forceinline__ void g_stage(uint8_t *tile, const uint16_t *__restrict__ X, long sr,
+                                        long sk, int r0, int R, int k0, int K, int mode) {
+    const int tid = threadIdx.x;
+    if (mode == 1) {
+        for (int q = tid; q < kGm * (kGk / 8); q += blockDim.x) {
+            const int r = q >> 2, kg = (q & 3) * 8, gr = r0 + r, gk = k0 + kg;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (gr < R) {
+                if (gk + 8 <= K) {
+                    v = __ldg((const uint4 *)(X + gr * sr + gk));
+                } else {
+                    __align__(16) uint16_t e[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) e[j] = gk + j < K ? X[gr * sr + gk + j] : (uint16_t)0;
+                    v = *(const uint4 *)e;
+                }
+            }
+            *(uint4 *)(tile + g_off(r, kg)) = v;
+        }
+    } else if (mode == 2) {
+        for (int q = tid; q < kGk * (kGm / 8); q += blockDim.x) {
+            const int k = q >> 4, rg = (q & 15) * 8, gr = r0 + rg, gk = k0 + k;
+            __align__(16) uint16_t e[8];
+            if (gk < K && gr + 8 <= R) {
+                *(uint4 *)e = __ldg((const uint4 *)(X + (long)gk * sk + gr));
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    e[j] = (gk < K && gr + j < R) ? X[(long)gk * sk + gr + j] : (uint16_t)0;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) *(uint16_t *)(tile + g_off(rg + j, k)) = e[j];
+        }
+    } else {
+        for (int q = tid; q < kGm * (kGk / 8); q += blockDim.x) {
+            const int r = q >> 2, kg = (q & 3) * 8, gr = r0 + r, gk = k0 + kg;
+            __align__(16) uint16_t e[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                e[j] = (gr < R && gk + j < K) ? X[gr * sr + (long)(gk + j) * sk] : (uint16_t)0;
+            *(uint4 *)(tile + g_off(r, kg)) = *(const uint4 *)e;
+        }
+    }
+}
+
 __device__ __forceinline__ void g_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -93,6 +144,13 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A,
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
     const int nkc = (K + kGk - 1) / kGk;
+    auto mode_of = [](const uint16_t *X, long sr, long sk) {
+        if (((uintptr_t)X & 15) != 0) return 0;
+        if (sk == 1 && sr % 8 == 0) return 1;
+        if (sr == 1 && sk % 8 == 0) return 2;
+        return 0;
+    };
+    const int va_mode = mode_of(A, sam, sak), vb_mode = mode_of(B, sbn, sbk);
     for (int kc = 0; kc < nkc; ++kc) {
         const int b = kc & 1;
         uint8_t *sa = sm + (size_t)b * 2 * kGtile, *sb = sa + kGtile;
@@ -100,20 +158,8 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A,
         if (kc >= 2 && !tc_mbar_wait(&buf_bar[b], (uint32_t)((kc / 2 - 1) & 1))) s_fail = 1;
         __syncthreads();
         if (s_fail) break;
-        // one item: 8 consecutive k of one row of A and of one column of B
-        for (int q = tid; q < kGm * (kGk / 8); q += blockDim.x) {
-            const int r = q >> 2, kg = (q & 3) * 8, k0 = kc * kGk + kg;
-            const int gm = m0 + r, gn = n0 + r;
-            __align__(16) uint16_t va[8], vb[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const bool kin = k0 + j < K;
-                va[j] = (gm < M && kin) ? A[gm * sam + (long)(k0 + j) * sak] : (uint16_t)0;
-                vb[j] = (gn < N && kin) ? B[(long)(k0 + j) * sbk + gn * sbn] : (uint16_t)0;
-            }
-            *(uint4 *)(sa + g_off(r, kg)) = *(const uint4 *)va;
-            *(uint4 *)(sb + g_off(r, kg)) = *(const uint4 *)vb;
-        }
+        g_stage(sa, A, sam, sak, m0, M, kc * kGk, K, va_mode);
+        g_stage(sb, B, sbn, sbk, n0, N, kc * kGk, K, vb_mode);
         // the staged tiles, written through the generic proxy, become visible
         // to the tensor cores' reads
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -135,7 +181,10 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A,
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const bool fail = s_fail != 0;
-    const int gm = m0 + warp * 32 + lane;
+    // accumulator lane = row: each 32-column block goes through shared memory
+    // (the operand tiles are free now, rows padded to 33 words) so that the
+    // warp writes each row's 32 columns with one coalesced store
+    float *tp = (float *)(sm + (size_t)warp * 32 * 33 * 4);
     for (int q = 0; q < kGn / 32; ++q) {
         uint32_t v[32];
         const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(q * 32);
@@ -152,13 +201,17 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A,
             : "r"(ta)
             : "memory");
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (gm >= M) continue;
+        __syncwarp();
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            const int gn = n0 + q * 32 + j;
-            if (gn >= N) continue;
-            float x = fail ? __int_as_float(0x7fc00000) : (nkc ? __uint_as_float(v[j]) : 0.f);
-            if (bias) x += bias[gn];
+        for (int j = 0; j < 32; ++j) tp[lane * 33 + j] = __uint_as_float(v[j]);
+        __syncwarp();
+        const int gn = n0 + q * 32 + lane;
+        const float bv = (bias && gn < N) ? bias[gn] : 0.f;
+        for (int r = 0; r < 32; ++r) {
+            const int gm = m0 + warp * 32 + r;
+            if (gm >= M || gn >= N) continue;
+            float x = fail ? __int_as_float(0x7fc00000) : (nkc ? tp[r * 33 + lane] : 0.f);
+            x += bv;
             C[gm * ldc + gn] = x;
             if (Cb)
                 Cb[gm * ldc + gn] =
