@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A,
                                                  long sbk, long sbn, float *__restrict__ C,
                                                  long ldc, uint16_t *__restrict__ Cb,
                                                  const float *__restrict__ bias, int M, int N,
-                                                 int K, int relu) {
+                                                 int K, int relu, int kslice) {
     extern __shared__ uint8_t g_raw[];
     __shared__ __align__(8) uint64_t buf_bar[2], done_bar;
     __shared__ uint32_t s_tmem;
@@ -143,7 +143,11 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A,
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    const int nkc = (K + kGk - 1) / kGk;
+    // split K: block z takes K range [z kslice, (z + 1) kslice) and writes its
+    // partial product to the z-th M x ldc slab of C
+    const int kbeg = blockIdx.z * kslice, kend = min(K, kbeg + kslice);
+    const int nkc = kend > kbeg ? (kend - kbeg + kGk - 1) / kGk : 0;
+    C += (long)blockIdx.z * M * ldc;
     auto mode_of = [](const uint16_t *X, long sr, long sk) {
         if (((uintptr_t)X & 15) != 0) return 0;
         if (sk == 1 && sr % 8 == 0) return 1;
@@ -158,8 +162,8 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A,
         if (kc >= 2 && !tc_mbar_wait(&buf_bar[b], (uint32_t)((kc / 2 - 1) & 1))) s_fail = 1;
         __syncthreads();
         if (s_fail) break;
-        g_stage(sa, A, sam, sak, m0, M, kc * kGk, K, va_mode);
-        g_stage(sb, B, sbn, sbk, n0, N, kc * kGk, K, vb_mode);
+        g_stage(sa, A, sam, sak, m0, M, kbeg + kc * kGk, kend, va_mode);
+        g_stage(sb, B, sbn, sbk, n0, N, kbeg + kc * kGk, kend, vb_mode);
         // the staged tiles, written through the generic proxy, become visible
         // to the tensor cores' reads
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -226,13 +230,51 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const uint16_t *__restrict__ A,
                      : "memory");
 }
 
+// the split-K partials summed in slice order (fixed, so the result is the same
+// on every run), then the bias and the BF16 copy as the GEMM's own epilogue
+__global__ void k_gemm_splitk_sum(const float *__restrict__ part, int S, int M, int N,
+                                  float *__restrict__ C, long ldc, uint16_t *__restrict__ Cb,
+                                  const float *__restrict__ bias, int relu) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)M * N) return;
+    const int m = (int)(i / N), n = (int)(i - (long)m * N);
+    float x = 0.f;
+    for (int z = 0; z < S; ++z) x += part[(long)z * M * N + i];
+    if (bias) x += bias[n];
+    C[m * ldc + n] = x;
+    if (Cb) Cb[m * ldc + n] = __bfloat16_as_ushort(__float2bfloat16_rn(relu ? fmaxf(x, 0.f) : x));
+}
+
+// Slices of K for a product of few output tiles and a long K (the weight
+// gradients, K = batch): at least 256 of K per slice, at most kGsplit slices,
+// enough to give the GPU about 64 CTAs; partials need kGsplit M N floats.
+constexpr int kGsplit = 16;
+
+static int gemm_slices(int M, int N, int K) {
+    const int tiles = ((M + kGm - 1) / kGm) * ((N + kGn - 1) / kGn);
+    int S = 1;
+    while (S < kGsplit && tiles * S < 64 && K / (2 * S) >= 256) S *= 2;
+    return S;
+}
+
 static void gemm(const uint16_t *A, long sam, long sak, const uint16_t *B, long sbk, long sbn,
                  float *C, long ldc, uint16_t *Cb, const float *bias, int M, int N, int K,
-                 int relu, cudaStream_t st) {
+                 int relu, cudaStream_t st, float *part = nullptr) {
     cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGsmem);
-    dim3 grid((N + kGn - 1) / kGn, (M + kGm - 1) / kGm);
-    k_gemm_tc<<<grid, 128, kGsmem, st>>>(A, sam, sak, B, sbk, sbn, C, ldc, Cb, bias, M, N, K,
-                                         relu);
+    const int S = part ? gemm_slices(M, N, K) : 1;
+    if (S == 1) {
+        dim3 grid((N + kGn - 1) / kGn, (M + kGm - 1) / kGm, 1);
+        k_gemm_tc<<<grid, 128, kGsmem, st>>>(A, sam, sak, B, sbk, sbn, C, ldc, Cb, bias, M, N, K,
+                                             relu, K);
+        return;
+    }
+    // K slices a multiple of the 32-wide chunk
+    const int kslice = ((K + S - 1) / S + kGk - 1) / kGk * kGk;
+    dim3 grid((N + kGn - 1) / kGn, (M + kGm - 1) / kGm, S);
+    k_gemm_tc<<<grid, 128, kGsmem, st>>>(A, sam, sak, B, sbk, sbn, part, N, nullptr, nullptr, M,
+                                         N, K, 0, kslice);
+    k_gemm_splitk_sum<<<(unsigned)(((long)M * N + 255) / 256), 256, 0, st>>>(part, S, M, N, C,
+                                                                           ldc, Cb, bias, relu);
 }
 
 // ---------------------------------------------------------------- forward
@@ -515,7 +557,7 @@ int chx_mlp_predict(const chx_mlp_t *P, const uint8_t *codes, const float *lnbet
 int64_t chx_mlp_work_bytes(int B, int H) {
     if (B <= 0 || H <= 0) return -1;
     const int64_t bh = (int64_t)B * H;
-    return bh * (4 * 4 + 5 * 2) + (int64_t)B * 8 + 12 * 256;
+    return bh * (4 * 4 + 5 * 2) + (int64_t)B * 8 + (int64_t)kGsplit * H * H * 4 + 13 * 256;
 }
 
 int chx_mlp_grad(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
@@ -540,6 +582,7 @@ int chx_mlp_grad(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
              *H3b = (uint16_t *)take(p, bh * 2);
     uint16_t *dZa = (uint16_t *)take(p, bh * 2), *dZb = (uint16_t *)take(p, bh * 2);
     float *dy = (float *)take(p, (size_t)B * 4), *f = (float *)take(p, (size_t)B * 4);
+    float *part = (float *)take(p, (size_t)kGsplit * H * H * 4);   // split-K partials
     if ((int64_t)(p - (char *)work) > chx_mlp_work_bytes(B, H)) {
         set_error("mlp_grad: work carve-up exceeds chx_mlp_work_bytes");
         return CHX_ERR_SCRATCH;
@@ -556,12 +599,12 @@ int chx_mlp_grad(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
     const int cs = (H + 31) / 32;
     k_colsum<<<cs, 256, 0, st>>>(H3b, dy, B, H, grad + of.w4);
     // layer 3: gW3 = H2^T dZ3, gb3, dH2 = dZ3 W3^T
-    gemm(H2b, 1, H, dZa, H, 1, grad + of.W3, H, nullptr, nullptr, H, H, B, 0, st);
+    gemm(H2b, 1, H, dZa, H, 1, grad + of.W3, H, nullptr, nullptr, H, H, B, 0, st, part);
     k_colsum<<<cs, 256, 0, st>>>(dZa, nullptr, B, H, grad + of.b3);
     gemm(dZa, H, 1, P->W3, 1, H, dH, H, nullptr, nullptr, B, H, H, 0, st);
     k_relu_back<<<(unsigned)((bh + 255) / 256), 256, 0, st>>>(dH, Z2, bh, dZb);
     // layer 2
-    gemm(H1b, 1, H, dZb, H, 1, grad + of.W2, H, nullptr, nullptr, H, H, B, 0, st);
+    gemm(H1b, 1, H, dZb, H, 1, grad + of.W2, H, nullptr, nullptr, H, H, B, 0, st, part);
     k_colsum<<<cs, 256, 0, st>>>(dZb, nullptr, B, H, grad + of.b2);
     gemm(dZb, H, 1, P->W2, 1, H, dH, H, nullptr, nullptr, B, H, H, 0, st);
     k_relu_back<<<(unsigned)((bh + 255) / 256), 256, 0, st>>>(dH, Z1, bh, dZa);
