@@ -255,11 +255,13 @@ CHX_API int chx_mlp_bind(chx_mlp_t *P, int nsp, int D, int nchain, int H, const 
  * out_scale). P is a device pointer. */
 CHX_API int chx_mlp_predict(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
                             const int *chain, int B, float *out, void *stream);
-/* Training forward (tensor-core GEMMs over the batch), loss and gradient:
+/* Training forward (tcgen05 GEMMs over the batch), loss and gradient:
  * loss = mean (net - target)^2; grad (nparam, FP32) overwritten; y (B) the
  * batch outputs; chain (B) sorted ascending (the chain rows' gradient is
  * summed per run of equal chains, in order), or NULL; work:
- * chx_mlp_work_bytes(B, H). P is a HOST descriptor. */
+ * chx_mlp_work_bytes(B, H), which includes the split-K partials of the
+ * weight gradients (summed in a fixed order: the gradient is the same on
+ * every run). P is a HOST descriptor. */
 CHX_API int64_t chx_mlp_work_bytes(int B, int H);
 CHX_API int chx_mlp_grad(const chx_mlp_t *P, const uint8_t *codes, const float *lnbeta,
                          const int *chain, const float *target, int B, float *y, float *grad,
